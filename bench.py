@@ -1,0 +1,411 @@
+#!/usr/bin/env python
+"""bench.py -- seconds per self-energy (Sigma) evaluation on B200.
+
+Workload (N=1): the GPP plain-FP64 benchmark configuration -- 512 bands,
+nvband 2, ncouls 32768, nodes_per_group 20 (ngpown 1638), 3 frequencies,
+seeded inputs with the benchmark distributions (bgwsigma.inputs.gpp_seeded),
+evaluated by the band-loop kernel (every (band, G', G, frequency) quotient, as
+the reference loop nest GPP/gpp.cpp:343-390).  One step = one Sigma
+evaluation through the C ABI with inputs resident in HBM (2.25 GB, larger than
+the 126 MB L2, so no flush is needed).  With --gpus N each rank evaluates its
+own instance (seed + rank); no data-path collective; value = max-over-ranks
+time / (N * steps).
+
+Extra lines in the JSON: the factored GPP path, the FF sums at 512 bands /
+nvband 2 / ncouls 8192 / ngpown 512 / nFreq 15 / nfreqeval 10, the end-to-end
+time through host (pinned) buffers, the FP64 roofline of the dominant kernel
+against the in-run measured DFMA/DMMA peaks, and the reference's own OpenMP
+CPU build timed on this host's cores.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "berkeleygw-kernels-cpp_b200"))
+sys.path.insert(0, str(REPO))
+
+import numpy as np  # noqa: E402
+
+METRIC = "GPP/FF sec per Sigma & % of FP64/TC peak; mixed vs plain FP64 speedup @ rel err"
+GPP_DIMS = dict(number_bands=512, nvband=2, ncouls=32768, nodes_per_group=20)
+FF_DIMS = dict(number_bands=512, nvband=2, ncouls=8192, ngpown=512, nFreq=15, nfreqeval=10)
+WORKLOAD = ("GPP plain FP64 band loop: number_bands 512, nvband 2, ncouls 32768, nodes_per_group 20 "
+            "(ngpown 1638), 3 frequencies")
+
+
+# ----------------------------------------------------------------- helpers --
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+        return self.summary()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def rel_err(got, ref) -> float:
+    got = np.atleast_1d(np.asarray(got, dtype=np.complex128))
+    ref = np.atleast_1d(np.asarray(ref, dtype=np.complex128))
+    return float(np.max(np.abs(got - ref)) / np.max(np.abs(ref)))
+
+
+def traffic_from_profiles(kernel: str):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summaries
+    (a line `TRAFFIC <kernel> <bytes_per_launch>` in profiles/*.md)."""
+    for p in sorted((REPO / "profiles").glob("*.md")):
+        for line in p.read_text().splitlines():
+            parts = line.strip().strip("`").split()
+            if len(parts) == 3 and parts[0] == "TRAFFIC" and parts[1] == kernel:
+                try:
+                    return float(parts[2])
+                except ValueError:
+                    pass
+    return None
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ------------------------------------------------------- reference (CPU) --
+
+def cpu_reference_gpp(g_full, target_s: float, threads_note: bool = True):
+    """Times the reference's OpenMP build (oracle/_ref) -- or, where it was not
+    built, the oracle port -- on the first nb_s bands of the workload, sized
+    to about target_s seconds; returns (seconds per full Sigma, descriptor)."""
+    from bgwsigma import inputs as I
+    from oracle.oracle import Oracle, Reference
+    if Reference.available():
+        impl, kind, cores = Reference(), "reference", None
+        cores = impl.num_threads()
+    else:
+        impl, kind, cores = Oracle(), "port", os.cpu_count()
+
+    def sample(nb_s):
+        g = I.GppInputs(**{**g_full.__dict__, "number_bands": nb_s,
+                            "aqsmtemp": np.ascontiguousarray(g_full.aqsmtemp[:nb_s]),
+                            "aqsntemp": np.ascontiguousarray(g_full.aqsntemp[:nb_s])})
+        t0 = time.perf_counter()
+        impl.gpp(g)
+        return time.perf_counter() - t0
+
+    nb = g_full.number_bands
+    t4 = sample(4)
+    nb_s = int(min(nb, max(4, round(4 * target_s / max(t4, 1e-6)))))
+    t = sample(nb_s)
+    per_sigma = t * nb / nb_s
+    desc = {"kind": kind, "cores": cores,
+            "sample": f"first {nb_s} of {nb} bands of the same workload ({t:.2f} s), scaled by {nb}/{nb_s} "
+                      f"(the reference's work is linear in bands)",
+            "nb_sample": nb_s, "sample_s": t}
+    return per_sigma, desc
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return 0
+    from bgwsigma import inputs as I
+    g = I.gpp_seeded(**GPP_DIMS, seed=1234)
+    budget = 150.0  # seconds for the whole run
+    per_step_target = max(1.0, budget / (args.steps + args.warmup))
+    vals = []
+    desc = None
+    for i in range(args.warmup + args.steps):
+        v, desc = cpu_reference_gpp(g, per_step_target)
+        if i >= args.warmup:
+            vals.append(v)
+    value = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded PCG64)",
+            "config": {"workload": WORKLOAD, "parallelism": "OpenMP 3.0 on the host cores"},
+            "cpu_baseline": {"value": value, "unit": "s", "cores": desc["cores"], "kind": desc["kind"],
+                             "sample": desc["sample"]},
+            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ ours --
+
+def run_ours(args, world, rank, local):
+    import torch
+    import bgwsigma as bgw
+    from bgwsigma import inputs as I
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+        pg = dist
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if pg is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    bgw.load()
+    dfma_peak, dmma_peak = bgw.measure_fp64_peak(local)
+
+    g = I.gpp_seeded(**GPP_DIMS, seed=1234 + rank)
+    d = bgw.to_device(g, dev)
+    stream = torch.cuda.Stream(device=dev)
+    sh = stream.cuda_stream
+    out = torch.zeros(3, dtype=torch.complex128, device=dev)
+
+    # Warm-up.
+    for _ in range(args.warmup):
+        bgw.noflagOCC_solver(d, stream=sh, out=out, flags=bgw.FLAG_PROFILE)
+    torch.cuda.synchronize(dev)
+    barrier()
+    torch.cuda.synchronize(dev)
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    n0 = bgw.launch_count()
+    main_ms = []
+    e0.record(stream)
+    for _ in range(args.steps):
+        bgw.noflagOCC_solver(d, stream=sh, out=out, flags=bgw.FLAG_PROFILE)
+        main_ms.append(bgw.last_profile()["main_kernel_ms"])
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    launches = bgw.launch_count() - n0
+    clk = clocks.stop()
+    barrier()
+    torch.cuda.synchronize(dev)
+    elapsed_ms = max_over_ranks(e0.elapsed_time(e1))
+    prof = bgw.last_profile()
+    ms_per_step = elapsed_ms / args.steps
+    value = elapsed_ms / 1e3 / (args.steps * world)
+    result = out.cpu().numpy()
+
+    kernel_ms = statistics.mean(main_ms)
+    achieved = prof["flops"] / (kernel_ms * 1e-3) / 1e12
+    roofline = {"bound": "fp64", "achieved": achieved, "peak": dfma_peak, "unit": "TFLOP/s",
+                "frac": achieved / dfma_peak, "traffic": traffic_from_profiles("gpp_bandloop_kernel"),
+                "kernel": prof["main_kernel"], "kernel_ms": kernel_ms,
+                "algorithmic_flops_per_launch": prof["flops"], "algorithmic_bytes_per_launch": prof["main_bytes"],
+                "peak_source": "in-run DFMA microkernel (bgw_measure_fp64_peak); MEASURED_PEAKS.json has no FP64 "
+                               "entry", "peak_dmma": dmma_peak,
+                "flop_convention": "21 flops per (band, G', G, frequency) term, 63 per triple (gpp.cpp:374-383)"}
+
+    extra = {}
+    # End to end: host (pinned) inputs, H2D + kernels + D2H inside the timed region.
+    gp = bgw.to_pinned(g)
+    bgw.noflagOCC_solver(gp, stream=sh)
+    torch.cuda.synchronize(dev)
+    barrier()
+    h0 = torch.cuda.Event(enable_timing=True)
+    h1 = torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(3, min(args.steps, 10))
+    h0.record(stream)
+    for _ in range(e2e_steps):
+        host_res = bgw.noflagOCC_solver(gp, stream=sh)
+    h1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = max_over_ranks(h0.elapsed_time(h1))
+    e2e = {"value": e2e_ms / 1e3 / (e2e_steps * world), "unit": "s", "h2d_bytes_per_step": int(g.nbytes()),
+           "d2h_bytes_per_step": 48, "steps": e2e_steps,
+           "note": "bgw_noflagOCC_solver with BGW_MEMORY_HOST on pinned buffers (the drop-in path)"}
+    del gp
+
+    # Factored GPP path (band-independent wx): HBM-bound stream.
+    if not args.quick:
+        for _ in range(2):
+            bgw.noflagOCC_solver(d, stream=sh, algorithm="factored", flags=bgw.FLAG_PROFILE)
+        fms, fdev = [], []
+        for _ in range(args.steps):
+            fres = bgw.noflagOCC_solver(d, stream=sh, algorithm="factored", flags=bgw.FLAG_PROFILE)
+            p = bgw.last_profile()
+            fms.append(p["main_kernel_ms"])
+            fdev.append(p["device_ms"])
+        fk = statistics.mean(fms)
+        extra["gpp_factored"] = {
+            "s_per_sigma": statistics.mean(fdev) / 1e3, "kernel": p["main_kernel"], "kernel_ms": fk,
+            "roofline": {"bound": "hbm", "achieved": p["main_bytes"] / (fk * 1e-3) / 1e9, "unit": "GB/s",
+                         "peak": _hbm_peak(), "frac": p["main_bytes"] / (fk * 1e-3) / 1e9 / _hbm_peak(),
+                         "algorithmic_bytes_per_launch": p["main_bytes"],
+                         "traffic": traffic_from_profiles("gpp_factored_kernel")},
+            "rel_err_vs_bandloop": rel_err(fres.cpu().numpy(), result)}
+    del d
+    torch.cuda.empty_cache()
+
+    # FF sums.
+    if not args.quick:
+        f = I.ff_seeded(**FF_DIMS, seed=1234 + rank)
+        fd = bgw.to_device(f, dev)
+        for _ in range(2):
+            bgw.ff_sigma(fd, stream=sh, flags=bgw.FLAG_PROFILE)
+        kms, dms = [], []
+        for _ in range(args.steps):
+            ff_out = bgw.ff_sigma(fd, stream=sh, flags=bgw.FLAG_PROFILE)
+            p = bgw.last_profile()
+            kms.append(p["main_kernel_ms"])
+            dms.append(p["device_ms"])
+        fk = statistics.mean(kms)
+        ach = p["flops"] / (fk * 1e-3) / 1e12
+        extra["ff"] = {
+            "workload": "FF: number_bands 512, nvband 2, ncouls 8192, ngpown 512, nFreq 15, nfreqeval 10 "
+                        "(achsDtemp + asxDtemp + achDtemp_cor in one call)",
+            "s_per_sigma": statistics.mean(dms) / 1e3, "kernel": p["main_kernel"], "kernel_ms": fk,
+            "roofline": {"bound": "fp64_tensor", "achieved": ach, "unit": "TFLOP/s", "peak": dmma_peak,
+                         "frac": ach / dmma_peak, "algorithmic_flops_per_launch": p["flops"],
+                         "algorithmic_bytes_per_launch": p["main_bytes"],
+                         "achieved_GBps": p["main_bytes"] / (fk * 1e-3) / 1e9,
+                         "traffic": traffic_from_profiles("ff_contract_kernel")}}
+        if rank == 0 and not args.no_cpu:
+            from oracle.oracle import Reference
+            if Reference.available():
+                ref = Reference()
+                t0 = time.perf_counter()
+                ra = ref.achs(f)
+                t1 = time.perf_counter()
+                rs = ref.asx(f)
+                t2 = time.perf_counter()
+                rc = ref.cor(f)
+                t3 = time.perf_counter()
+                extra["ff"]["cpu_baseline"] = {
+                    "kind": "reference", "cores": ref.num_threads(), "unit": "s",
+                    "achsDtemp_s": t1 - t0, "asxDtemp_s": t2 - t1, "achDtemp_cor_s": t3 - t2, "value": t3 - t0,
+                    "sample": "full FF workload, one run"}
+                extra["ff"]["rel_err_vs_reference"] = {
+                    "achsDtemp": rel_err(ff_out[0].cpu().numpy(), ra),
+                    "asxDtemp": rel_err(ff_out[1].cpu().numpy(), rs),
+                    "achDtemp_cor": rel_err(ff_out[2].cpu().numpy(), rc)}
+        del fd
+
+    # Accuracy against the long-double oracle (exact factored identity).
+    cpu_baseline = None
+    if rank == 0 and not args.no_cpu:
+        from oracle.oracle import Oracle
+        ref = Oracle().gpp(g, factored=True)
+        extra["rel_err_vs_oracle"] = {"bandloop": rel_err(result, ref), "e2e_host_path": rel_err(host_res, ref)}
+        if world == 1:
+            per_sigma, desc = cpu_reference_gpp(g, args.cpu_seconds)
+            cpu_baseline = {"value": per_sigma, "unit": "s", "cores": desc["cores"], "kind": desc["kind"],
+                            "sample": desc["sample"]}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded PCG64, benchmark distributions)",
+                "config": {"workload": WORKLOAD, "global_batch": world, "l2": "inputs 2.25 GB resident in HBM per "
+                           "GPU (> 126 MB L2); no flush", "parallelism": f"{world} independent instance(s), one "
+                           "per GPU"},
+                "roofline": roofline, "cpu_baseline": cpu_baseline, "e2e": e2e, "gpu_launches": int(launches),
+                "clocks": clk, "extra": extra}
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+def _hbm_peak() -> float:
+    p = REPO / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"])
+    except (OSError, ValueError, KeyError):
+        return 6650.0  # fallback measurement of this pool
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--quick", action="store_true", help="GPP band loop + e2e only")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and oracle check")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        return run_reference_arm(args, world, rank)
+    return run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

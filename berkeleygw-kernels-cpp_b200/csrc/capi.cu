@@ -1,0 +1,256 @@
+// capi.cu -- the extern "C" entry points of libbgwsigma.so (include/bgw_sigma.h).
+//
+// Each entry point validates its arguments on the host (no launch on a bad
+// size or pointer), stages host inputs to the device when asked, enqueues
+// the kernels of gpp.cu / ff.cu on the caller's stream and, unless
+// BGW_FLAG_ASYNC, synchronises and returns the device-side status.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "bgw_internal.cuh"
+
+namespace bgw {
+
+struct FFPlan;
+int gpp_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *inv, const int32_t *indinv,
+                int64_t indinv_len, const double *wx, int64_t wx_stride, const double2 *wt, const double2 *am,
+                const double2 *an, const double2 *ie, const double *vc, double *achtemp_dev);
+
+}  // namespace bgw
+
+#include "ff_plan.cuh"
+
+namespace bgw {
+namespace {
+
+// Guards against products that overflow the 64-bit byte counts.
+bool dims_ok(int64_t a, int64_t b) { return a >= 0 && b >= 0 && (a == 0 || b <= (int64_t(1) << 40) / a); }
+
+// Common prologue: begin_call + lock + status reset.
+struct Call {
+  CallEnv env;
+  std::unique_lock<std::mutex> lock;
+  int st = BGW_OK;
+  explicit Call(const bgw_options *opt) {
+    st = begin_call(opt, &env);
+    if (st != BGW_OK) return;
+    lock = std::unique_lock<std::mutex>(env.ws->mu);
+    st = ws_acquire(env.ws, env.stream);
+    if (st != BGW_OK) return;
+    void *s = nullptr;
+    st = ws_reserve(env.ws, SLOT_STATUS, sizeof(int32_t) * STATUS_WORDS, &s);
+    if (st != BGW_OK) return;
+    env.d_status = static_cast<int *>(s);
+    st = prof_mark(&env, 0);
+    if (st != BGW_OK) return;
+    if (cudaMemsetAsync(s, 0, sizeof(int32_t) * STATUS_WORDS, env.stream) != cudaSuccess) st = BGW_ERR_CUDA;
+  }
+};
+
+int out_buffer(CallEnv *env, double *user, size_t bytes, double **dev) {
+  if (!env->host) {
+    *dev = user;
+    return BGW_OK;
+  }
+  void *d = nullptr;
+  BGW_TRY(ws_reserve(env->ws, SLOT_OUT, bytes, &d));
+  *dev = static_cast<double *>(d);
+  return BGW_OK;
+}
+
+}  // namespace
+}  // namespace bgw
+
+using namespace bgw;
+
+extern "C" int bgw_noflagOCC_solver(int64_t number_bands, int64_t ngpown, int64_t ncouls,
+                                    const int32_t *inv_igp_index, const int32_t *indinv, int64_t indinv_len,
+                                    const double *wx_array, const double *wtilde_array, const double *aqsmtemp,
+                                    const double *aqsntemp, const double *I_eps_array, const double *vcoul,
+                                    double *achtemp, const bgw_options *opt) {
+  const int64_t nb = number_bands, P = ngpown, G = ncouls;
+  if (nb < 0 || P < 0 || G <= 0 || G > INT32_MAX || nb > INT32_MAX || P > INT32_MAX) return BGW_ERR_INVALID_ARG;
+  if (!dims_ok(nb, G) || !dims_ok(P, G) || indinv_len <= 0 || indinv_len > INT32_MAX) return BGW_ERR_INVALID_ARG;
+  if (!achtemp || !wx_array || !vcoul || !indinv) return BGW_ERR_INVALID_ARG;
+  if (P > 0 && (!inv_igp_index || !wtilde_array || !I_eps_array)) return BGW_ERR_INVALID_ARG;
+  if (nb > 0 && P > 0 && (!aqsmtemp || !aqsntemp)) return BGW_ERR_INVALID_ARG;
+  Call c(opt);
+  if (c.st != BGW_OK) return c.st;
+  CallEnv *env = &c.env;
+  const int64_t stride = env->opt.wx_band_stride;
+  if (stride != 0 && stride < 3) return BGW_ERR_INVALID_ARG;
+  if (env->opt.precision != BGW_PRECISION_FP64) return BGW_ERR_UNSUPPORTED;
+  const size_t wx_n = stride == 0 ? 3 : (size_t)(nb > 0 ? (nb - 1) * stride + 3 : 3);
+  const void *inv = nullptr, *ind = nullptr, *wx = nullptr, *wt = nullptr, *am = nullptr, *an = nullptr,
+             *ie = nullptr, *vc = nullptr;
+  const size_t pg = (size_t)P * (size_t)G * 16, ng = (size_t)nb * (size_t)G * 16;
+  BGW_TRY(stage_input(env, SLOT_IN0, inv_igp_index, sizeof(int32_t) * (size_t)P, &inv));
+  BGW_TRY(stage_input(env, SLOT_IN1, indinv, sizeof(int32_t) * (size_t)indinv_len, &ind));
+  BGW_TRY(stage_input(env, SLOT_IN2, wx_array, sizeof(double) * wx_n, &wx));
+  BGW_TRY(stage_input(env, SLOT_IN3, wtilde_array, pg, &wt));
+  BGW_TRY(stage_input(env, SLOT_IN4, aqsmtemp, ng, &am));
+  BGW_TRY(stage_input(env, SLOT_IN5, aqsntemp, ng, &an));
+  BGW_TRY(stage_input(env, SLOT_IN6, I_eps_array, pg, &ie));
+  BGW_TRY(stage_input(env, SLOT_IN7, vcoul, sizeof(double) * (size_t)G, &vc));
+  double *out = nullptr;
+  BGW_TRY(out_buffer(env, achtemp, 6 * sizeof(double), &out));
+  BGW_TRY(gpp_enqueue(env, nb, P, G, (const int32_t *)inv, (const int32_t *)ind, indinv_len, (const double *)wx,
+                      stride, (const double2 *)wt, (const double2 *)am, (const double2 *)an, (const double2 *)ie,
+                      (const double *)vc, out));
+  if (env->host) BGW_CUDA_TRY(cudaMemcpyAsync(achtemp, out, 6 * sizeof(double), cudaMemcpyDeviceToHost, env->stream));
+  env->prof.flops = 63.0 * (double)nb * (double)P * (double)G;
+  return finish_call(env);
+}
+
+namespace {
+
+// Shared body of the three FF entry points and bgw_ff_sigma.
+int ff_call(int64_t nb, int64_t nvband, int64_t nE, int64_t G, int64_t P, int64_t nFreq, double fmin, double fstep,
+            double occ, const double *ekq, const double *grid, const int32_t *inv, const int32_t *indinv,
+            int64_t indinv_len, const double *aqsm, const double *aqsn, const double *vcoul, const double *R,
+            const double *A, double *achs, double *asx, double *cor, const bgw_options *opt) {
+  if (nb < 0 || nvband < 0 || nE < 0 || P < 0 || G <= 0 || nFreq < 2) return BGW_ERR_INVALID_ARG;
+  if (nb > INT32_MAX || P > INT32_MAX || G > INT32_MAX || nFreq > INT32_MAX || nE > INT32_MAX)
+    return BGW_ERR_INVALID_ARG;
+  if (P > G) return BGW_ERR_INVALID_ARG;  // the reference driver's guard, ff.cpp:492-499
+  if ((asx || cor) && nvband > nb) return BGW_ERR_INVALID_ARG;
+  if (!dims_ok(nb, G) || !dims_ok(nFreq, P) || !dims_ok(nFreq * P, G) || indinv_len <= 0 ||
+      indinv_len > INT32_MAX)
+    return BGW_ERR_INVALID_ARG;
+  const bool want_achs = achs != nullptr, want_asx = asx != nullptr, want_cor = cor != nullptr;
+  if (!want_achs && !want_asx && !want_cor) return BGW_ERR_INVALID_ARG;
+  if (!indinv || !vcoul || (P > 0 && !inv)) return BGW_ERR_INVALID_ARG;
+  if (nb > 0 && (!aqsm || !aqsn)) return BGW_ERR_INVALID_ARG;
+  if ((want_asx || want_cor) && (!ekq || !grid || !R || !A)) return BGW_ERR_INVALID_ARG;
+  if (want_achs && !R) return BGW_ERR_INVALID_ARG;
+
+  Call c(opt);
+  if (c.st != BGW_OK) return c.st;
+  CallEnv *env = &c.env;
+  if (env->opt.precision != BGW_PRECISION_FP64) return BGW_ERR_UNSUPPORTED;
+
+  // Band classification needs ekq and dFreqGrid on the host.
+  const int64_t ne = (want_asx || want_cor) ? nb : 0;
+  std::vector<double> ekq_h((size_t)std::max<int64_t>(ne, 1)), grid_h((size_t)nFreq);
+  if (ne > 0 || want_asx || want_cor) {
+    if (env->host) {
+      if (ne) std::memcpy(ekq_h.data(), ekq, sizeof(double) * (size_t)ne);
+      std::memcpy(grid_h.data(), grid, sizeof(double) * (size_t)nFreq);
+    } else {
+      if (ne)
+        BGW_CUDA_TRY(cudaMemcpyAsync(ekq_h.data(), ekq, sizeof(double) * (size_t)ne, cudaMemcpyDeviceToHost,
+                                     env->stream));
+      BGW_CUDA_TRY(cudaMemcpyAsync(grid_h.data(), grid, sizeof(double) * (size_t)nFreq, cudaMemcpyDeviceToHost,
+                                   env->stream));
+      BGW_CUDA_TRY(cudaStreamSynchronize(env->stream));
+    }
+  }
+  FFPlan plan;
+  BGW_TRY(ff_make_plan(env, nb, nvband, P, G, nFreq, fmin, fstep, occ, ekq_h.data(), grid_h.data(), want_achs,
+                       want_asx, want_cor, &plan));
+
+  const size_t slice = (size_t)P * (size_t)G * 16;
+  const size_t ng = (size_t)nb * (size_t)G * 16;
+  const void *d_inv = nullptr, *d_ind = nullptr, *d_am = nullptr, *d_an = nullptr, *d_vc = nullptr;
+  const void *d_R = nullptr, *d_A = nullptr;
+  int r_f0 = 0, a_f0 = 0;
+  BGW_TRY(stage_input(env, SLOT_IN0, inv, sizeof(int32_t) * (size_t)P, &d_inv));
+  BGW_TRY(stage_input(env, SLOT_IN1, indinv, sizeof(int32_t) * (size_t)indinv_len, &d_ind));
+  BGW_TRY(stage_input(env, SLOT_IN2, aqsm, ng, &d_am));
+  BGW_TRY(stage_input(env, SLOT_IN3, aqsn, ng, &d_an));
+  BGW_TRY(stage_input(env, SLOT_IN4, vcoul, sizeof(double) * (size_t)G, &d_vc));
+  if (plan.r_hi >= plan.r_lo) {
+    if (env->host) {
+      r_f0 = plan.r_lo;
+      BGW_TRY(stage_input(env, SLOT_IN5, R + (size_t)plan.r_lo * slice / 8,
+                          slice * (size_t)(plan.r_hi - plan.r_lo + 1), &d_R));
+    } else {
+      BGW_TRY(stage_input(env, SLOT_IN5, R, slice, &d_R));
+    }
+  }
+  if (plan.a_hi >= plan.a_lo) {
+    if (env->host) {
+      a_f0 = plan.a_lo;
+      BGW_TRY(stage_input(env, SLOT_IN6, A + (size_t)plan.a_lo * slice / 8,
+                          slice * (size_t)(plan.a_hi - plan.a_lo + 1), &d_A));
+    } else {
+      BGW_TRY(stage_input(env, SLOT_IN6, A, slice, &d_A));
+    }
+  }
+  // Outputs: achs (2) | asx (2 nE) | cor (2 nE) doubles.
+  double *o_achs = nullptr, *o_asx = nullptr, *o_cor = nullptr;
+  if (env->host) {
+    double *o = nullptr;
+    BGW_TRY(out_buffer(env, nullptr, sizeof(double) * (2 + 4 * (size_t)nE), &o));
+    o_achs = want_achs ? o : nullptr;
+    o_asx = want_asx ? o + 2 : nullptr;
+    o_cor = want_cor ? o + 2 + 2 * nE : nullptr;
+  } else {
+    o_achs = achs;
+    o_asx = asx;
+    o_cor = cor;
+  }
+  const int64_t nb_w = (want_achs || want_cor) ? nb : nvband;
+  BGW_TRY(ff_launch(env, plan, nb_w, nE, G, P, (const int32_t *)d_inv, (const int32_t *)d_ind, indinv_len,
+                    (const double2 *)d_am, (const double2 *)d_an, (const double *)d_vc, (const double2 *)d_R, r_f0,
+                    (const double2 *)d_A, a_f0, o_achs, o_asx, o_cor));
+  if (env->host) {
+    if (want_achs)
+      BGW_CUDA_TRY(cudaMemcpyAsync(achs, o_achs, 2 * sizeof(double), cudaMemcpyDeviceToHost, env->stream));
+    if (want_asx && nE)
+      BGW_CUDA_TRY(cudaMemcpyAsync(asx, o_asx, 2 * sizeof(double) * nE, cudaMemcpyDeviceToHost, env->stream));
+    if (want_cor && nE)
+      BGW_CUDA_TRY(cudaMemcpyAsync(cor, o_cor, 2 * sizeof(double) * nE, cudaMemcpyDeviceToHost, env->stream));
+  }
+  return finish_call(env);
+}
+
+}  // namespace
+
+extern "C" int bgw_achsDtemp_Kernel(int64_t number_bands, int64_t ngpown, int64_t ncouls,
+                                    const int32_t *inv_igp_index, const int32_t *indinv, int64_t indinv_len,
+                                    const double *aqsntemp, const double *aqsmtemp, const double *I_epsR_array,
+                                    int64_t nFreq, const double *vcoul, double *achsDtemp, const bgw_options *opt) {
+  if (!achsDtemp) return BGW_ERR_INVALID_ARG;
+  return ff_call(number_bands, 0, 0, ncouls, ngpown, nFreq, 0.0, 0.0, 0.0, nullptr, nullptr, inv_igp_index, indinv,
+                 indinv_len, aqsmtemp, aqsntemp, vcoul, I_epsR_array, nullptr, achsDtemp, nullptr, nullptr, opt);
+}
+
+extern "C" int bgw_asxDtemp_Kernel(int64_t nvband, int64_t nfreqeval, int64_t ncouls, int64_t ngpown,
+                                   int64_t nFreq, double freqevalmin, double freqevalstep, double occ,
+                                   const double *ekq, const double *dFreqGrid, const int32_t *inv_igp_index,
+                                   const int32_t *indinv, int64_t indinv_len, const double *aqsmtemp,
+                                   const double *aqsntemp, int64_t number_bands, const double *vcoul,
+                                   const double *I_epsR_array, const double *I_epsA_array, double *asxDtemp,
+                                   const bgw_options *opt) {
+  if (!asxDtemp && nfreqeval > 0) return BGW_ERR_INVALID_ARG;
+  double dummy[2];
+  return ff_call(number_bands, nvband, nfreqeval, ncouls, ngpown, nFreq, freqevalmin, freqevalstep, occ, ekq,
+                 dFreqGrid, inv_igp_index, indinv, indinv_len, aqsmtemp, aqsntemp, vcoul, I_epsR_array,
+                 I_epsA_array, nullptr, nfreqeval > 0 ? asxDtemp : dummy, nullptr, opt);
+}
+
+extern "C" int bgw_achDtemp_cor_Kernel(int64_t number_bands, int64_t nvband, int64_t nfreqeval, int64_t ncouls,
+                                       int64_t ngpown, int64_t nFreq, double freqevalmin, double freqevalstep,
+                                       const double *ekq, const double *dFreqGrid, const int32_t *inv_igp_index,
+                                       const int32_t *indinv, int64_t indinv_len, const double *aqsmtemp,
+                                       const double *aqsntemp, const double *vcoul, const double *I_epsR_array,
+                                       const double *I_epsA_array, double *achDtemp_cor, const bgw_options *opt) {
+  if (!achDtemp_cor && nfreqeval > 0) return BGW_ERR_INVALID_ARG;
+  double dummy[2];
+  return ff_call(number_bands, nvband, nfreqeval, ncouls, ngpown, nFreq, freqevalmin, freqevalstep, 1.0, ekq,
+                 dFreqGrid, inv_igp_index, indinv, indinv_len, aqsmtemp, aqsntemp, vcoul, I_epsR_array,
+                 I_epsA_array, nullptr, nullptr, nfreqeval > 0 ? achDtemp_cor : dummy, opt);
+}
+
+extern "C" int bgw_ff_sigma(int64_t number_bands, int64_t nvband, int64_t nfreqeval, int64_t ncouls, int64_t ngpown,
+                            int64_t nFreq, double freqevalmin, double freqevalstep, double occ, const double *ekq,
+                            const double *dFreqGrid, const int32_t *inv_igp_index, const int32_t *indinv,
+                            int64_t indinv_len, const double *aqsmtemp, const double *aqsntemp, const double *vcoul,
+                            const double *I_epsR_array, const double *I_epsA_array, double *achsDtemp,
+                            double *asxDtemp, double *achDtemp_cor, const bgw_options *opt) {
+  return ff_call(number_bands, nvband, nfreqeval, ncouls, ngpown, nFreq, freqevalmin, freqevalstep, occ, ekq,
+                 dFreqGrid, inv_igp_index, indinv, indinv_len, aqsmtemp, aqsntemp, vcoul, I_epsR_array,
+                 I_epsA_array, achsDtemp, asxDtemp, achDtemp_cor, opt);
+}

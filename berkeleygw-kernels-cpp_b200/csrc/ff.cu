@@ -1,0 +1,492 @@
+// ff.cu -- full-frequency self-energy sums (FF/ff.cpp:103-451) on sm_100a.
+//
+// All three FF sums are weighted complex contractions over (band, G', G):
+//   sum_{rows r} coef(r) sum_p W(band(r), p) C(r, p),
+//   C(r, p)  = sum_ig aqsn[band(r)][ig] * X_f[p][ig],
+//   W(n1, p) = conj(aqsm[n1][igp(p)]) * vcoul[igp(p)],
+// with X_f one frequency slice of I_epsR (achsDtemp, and asxDtemp when
+// wx > 0), of I_epsA (asxDtemp when wx <= 0) or of I_epsR - I_epsA
+// (achDtemp_cor).  The reference evaluates (f1 X_i + f2 X_{i+1}) per band
+// (ff.cpp:161-164, 396-403, 432-437); by linearity this equals f1 C_i + f2
+// C_{i+1}, so a band contributes one row with coefficient f1 to the group of
+// slice i and one with f2 to the group of slice i+1.  Grouping bands by slice
+// turns every sum into a dense complex GEMM per group (rows x G' x G), which
+// runs on the FP64 tensor cores (mma.sync m8n8k4 f64, the only FP64 MMA on
+// sm_100a) with a fused epilogue that applies W and coef and reduces to one
+// complex partial per tile.  The reference's iw loop recomputes an
+// iw-independent value (wx has no iw term, ff.cpp:245, 337); it is computed
+// once and written to every iw.
+//
+// Reductions are deterministic: per-tile partials in a fixed slot, summed in
+// tile order by one block.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <tuple>
+#include <vector>
+
+#include "bgw_internal.cuh"
+#include "ff_plan.cuh"
+#include "reduce.cuh"
+
+namespace bgw {
+
+// --------------------------------------------------------------- planning --
+
+// compute_fact (FF/ff.cpp:103-152), quirks included: loop 1 maps a found
+// ifreq == 0 to nFreq - 2; loop 2 with wx > 0 keeps ifreq == 0 (its `== -1`
+// test never fires) and scales both weights by -0.5; loop 2 with wx <= 0 and
+// an occupied band searches -wx and maps 0 to nFreq - 2; otherwise the
+// outputs keep their initial values (0, 0, 0).
+struct Fact {
+  int ifreq = 0;
+  double f1 = 0.0, f2 = 0.0;
+};
+
+static int bracket_last(double x, int nFreq, const double *g, int init) {
+  int r = init;
+  for (int j = 0; j + 1 < nFreq; ++j)
+    if (x > g[j] && x < g[j + 1]) r = j;
+  return r;
+}
+
+Fact compute_fact_host(double wx, int nFreq, const double *g, int loop, bool flag_occ) {
+  Fact o;
+  if (loop == 1) {
+    const double x = wx > 0.0 ? wx : -wx;
+    int i = bracket_last(x, nFreq, g, 0);
+    if (i == 0) i = nFreq - 2;
+    const double span = g[i + 1] - g[i];
+    if (wx > 0.0) {
+      o.f1 = (g[i + 1] - wx) / span;
+      o.f2 = (wx - g[i]) / span;
+    } else {
+      o.f1 = (g[i + 1] + wx) / span;
+      o.f2 = (-g[i] - wx) / span;
+    }
+    o.ifreq = i;
+  } else if (wx > 0.0) {
+    const int i = bracket_last(wx, nFreq, g, 0);
+    const double span = g[i + 1] - g[i];
+    o.f1 = -0.5 * (g[i + 1] - wx) / span;
+    o.f2 = -0.5 * (wx - g[i]) / span;
+    o.ifreq = i;
+  } else if (flag_occ) {
+    const double x = -wx;
+    int i = bracket_last(x, nFreq, g, 0);
+    if (i == 0) i = nFreq - 2;
+    const double span = g[i + 1] - g[i];
+    o.f1 = (g[i + 1] - x) / span;
+    o.f2 = (x - g[i]) / span;
+    o.ifreq = i;
+  }
+  return o;
+}
+
+namespace {
+
+constexpr int kTM = 32;       // rows (bands) per tile
+constexpr int kTN = 64;       // G' columns per tile
+constexpr int kBK = 16;       // complex k per stage
+constexpr int kLds = kBK + 4;  // padded row stride (double2): 320 B
+constexpr int kFFThreads = 128;
+
+struct GroupKey {
+  int out, src, f;
+  bool operator<(const GroupKey &o) const { return std::tie(out, src, f) < std::tie(o.out, o.src, o.f); }
+};
+
+// Builds rows and tiles.  ekq/grid are host copies.
+int build_plan(int64_t nb, int64_t nvband, int64_t P, int64_t G, int64_t nFreq, double fmin, double fstep,
+               double occ, const double *ekq, const double *grid, bool want_achs, bool want_asx, bool want_cor,
+               int target_ctas, FFPlan *plan) {
+  std::map<GroupKey, std::vector<FFRow>> groups;
+  if (want_achs) {
+    auto &g = groups[{OUT_ACHS, SRC_R, 1}];
+    for (int64_t n1 = 0; n1 < nb; ++n1) g.push_back({(int32_t)n1, 0, -0.5});
+  }
+  if (want_asx) {
+    for (int64_t n1 = 0; n1 < nvband; ++n1) {
+      const double wx = fmin - ekq[n1] + fstep;
+      const Fact fc = compute_fact_host(wx, (int)nFreq, grid, 1, false);
+      const int src = wx > 0 ? SRC_R : SRC_A;
+      groups[{OUT_ASX, src, fc.ifreq}].push_back({(int32_t)n1, 0, fc.f1 * occ});
+      groups[{OUT_ASX, src, fc.ifreq + 1}].push_back({(int32_t)n1, 0, fc.f2 * occ});
+    }
+  }
+  if (want_cor) {
+    for (int64_t n1 = 0; n1 < nb; ++n1) {
+      const bool flag_occ = n1 < nvband;
+      const double wx = fmin - ekq[n1] + fstep;
+      const Fact fc = compute_fact_host(wx, (int)nFreq, grid, 2, flag_occ);
+      double s;
+      if (wx > 0) {
+        if (flag_occ) continue;  // schDttt_corKernel1 only for unoccupied bands
+        s = 1.0;
+      } else if (flag_occ) {
+        s = -0.5;  // schDttt_corKernel2 (ff.cpp:437-444)
+      } else {
+        continue;
+      }
+      groups[{OUT_COR, SRC_RA, fc.ifreq}].push_back({(int32_t)n1, 0, fc.f1 * s});
+      groups[{OUT_COR, SRC_RA, fc.ifreq + 1}].push_back({(int32_t)n1, 0, fc.f2 * s});
+    }
+  }
+  // Base tiles (no k split), then a k split that fills the GPU.
+  const int64_t ptiles = (P + kTN - 1) / kTN;
+  int64_t base = 0;
+  for (auto &kv : groups) base += ((int64_t)kv.second.size() + kTM - 1) / kTM * ptiles;
+  const int64_t kblocks = (G + kBK - 1) / kBK;
+  int64_t ksplit = base > 0 ? (target_ctas + base - 1) / base : 1;
+  ksplit = std::max<int64_t>(1, std::min<int64_t>(ksplit, std::max<int64_t>(1, kblocks / 8)));
+  const int64_t kb_per = (kblocks + ksplit - 1) / ksplit;
+  ksplit = (kblocks + kb_per - 1) / kb_per;
+
+  plan->rows.clear();
+  plan->tiles.clear();
+  plan->useful_cmacs = 0.0;
+  int cur_out = 0;
+  plan->seg[0] = 0;
+  for (auto &kv : groups) {
+    const GroupKey &key = kv.first;
+    while (cur_out < key.out) plan->seg[++cur_out] = (int)plan->tiles.size();
+    const int32_t rb = (int32_t)plan->rows.size();
+    const int64_t nrows = (int64_t)kv.second.size();
+    plan->rows.insert(plan->rows.end(), kv.second.begin(), kv.second.end());
+    plan->useful_cmacs += (double)nrows * (double)P * (double)G;
+    for (int64_t r0 = 0; r0 < nrows; r0 += kTM)
+      for (int64_t p0 = 0; p0 < P; p0 += kTN)
+        for (int64_t ks = 0; ks < ksplit; ++ks) {
+          FFTile t;
+          t.src = key.src;
+          t.f = key.f;
+          t.row_begin = rb + (int32_t)r0;
+          t.row_count = (int32_t)std::min<int64_t>(kTM, nrows - r0);
+          t.p_begin = (int32_t)p0;
+          t.k_begin = (int32_t)(ks * kb_per * kBK);
+          const int64_t kend = std::min<int64_t>(G, (ks + 1) * kb_per * kBK);
+          t.k_count = (int32_t)std::max<int64_t>(0, kend - t.k_begin);
+          t.out = key.out;
+          plan->tiles.push_back(t);
+        }
+  }
+  while (cur_out < OUT_COUNT) plan->seg[++cur_out] = (int)plan->tiles.size();
+  // Distinct (array, slice) pairs read: 1 per R or A slice, 2 per R - A slice.
+  {
+    std::map<std::pair<int, int>, int> seen;
+    for (auto &kv : groups) {
+      if (kv.first.src != SRC_A) seen[{0, kv.first.f}] = 1;
+      if (kv.first.src != SRC_R) seen[{1, kv.first.f}] = 1;
+    }
+    plan->slice_reads.assign(1, (double)seen.size());
+  }
+  for (auto &kv : groups) {
+    const int f = kv.first.f;
+    if (kv.first.src == SRC_R || kv.first.src == SRC_RA) {
+      plan->r_lo = std::min(plan->r_lo, f);
+      plan->r_hi = std::max(plan->r_hi, f);
+    }
+    if (kv.first.src == SRC_A || kv.first.src == SRC_RA) {
+      plan->a_lo = std::min(plan->a_lo, f);
+      plan->a_hi = std::max(plan->a_hi, f);
+    }
+  }
+  return BGW_OK;
+}
+
+// ------------------------------------------------------------------ prep --
+// W[n1][p] = conj(aqsm[n1][igp]) * vcoul[igp], igp = indinv[inv[p]] (checked).
+__global__ void ff_w_kernel(int nb, int P, int G, const int *__restrict__ inv, const int *__restrict__ indinv,
+                            long long indinv_len, const double2 *__restrict__ am, const double *__restrict__ vc,
+                            double2 *__restrict__ W, int *status) {
+  const long long total = (long long)nb * P;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int n1 = (int)(idx / P), p = (int)(idx % P);
+    const int a = inv[p];
+    double2 w = make_double2(0.0, 0.0);
+    if (a < 0 || (long long)a >= indinv_len) {
+      raise_status(status, BGW_ERR_INDEX, p);
+    } else {
+      const int g = indinv[a];
+      if (g < 0 || g >= G) {
+        raise_status(status, BGW_ERR_INDEX, p);
+      } else {
+        const double2 m = am[(size_t)n1 * G + g];
+        const double v = vc[g];
+        w = make_double2(m.x * v, -m.y * v);
+      }
+    }
+    W[idx] = w;
+  }
+}
+
+// ------------------------------------------------------- DMMA contraction --
+__device__ __forceinline__ void dmma_f64(double &c0, double &c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+struct FFSmem {
+  double2 a[2][kTM * kLds];
+  double2 b[2][kTN * kLds];
+  double red[(kFFThreads / 32) * 2];
+};
+
+// One CTA per tile.  4 warps; warp w owns G' columns [16w, 16w + 16) of the
+// tile and all 32 rows: 4 x 2 m8n8 blocks, each a complex accumulator kept
+// as separate real and imaginary DMMA accumulators (4 real MMAs per complex
+// k4 step: Re += Ar Br + Ai (-Bi), Im += Ar Bi + Ai Br).
+// Operands are staged global -> registers -> shared (double-buffered, the
+// next stage's loads in flight during the current stage's MMAs); the R - A
+// difference of the COR sum is formed in registers on the way.
+__global__ void __launch_bounds__(kFFThreads, 2)
+    ff_contract_kernel(const FFTile *__restrict__ tiles, const FFRow *__restrict__ rows, int P, int G,
+                       const double2 *__restrict__ aqsn, const double2 *__restrict__ R, int r_f0,
+                       const double2 *__restrict__ A, int a_f0, const double2 *__restrict__ W,
+                       double *__restrict__ partials) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  FFSmem &sm = *reinterpret_cast<FFSmem *>(smem_raw);
+  const FFTile t = tiles[blockIdx.x];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g8 = lane >> 2, t4 = lane & 3;
+
+  const size_t slice = (size_t)P * G;
+  // R / A point at slice r_f0 / a_f0 (host-staged inputs hold only the
+  // slices the plan reads).
+  const double2 *X0 = (t.src == SRC_A) ? A + (size_t)(t.f - a_f0) * slice : R + (size_t)(t.f - r_f0) * slice;
+  const double2 *X1 = (t.src == SRC_RA) ? A + (size_t)(t.f - a_f0) * slice : nullptr;
+
+  // Staging assignment: element idx = q * 128 + tid of a [rows][kBK] tile.
+  const int kc = tid & (kBK - 1);
+  const int r_lo = tid >> 4;  // 0..7
+  int a_band[kTM / 8];
+#pragma unroll
+  for (int q = 0; q < kTM / 8; ++q) {
+    const int r = q * 8 + r_lo;
+    a_band[q] = r < t.row_count ? rows[t.row_begin + r].band : -1;
+  }
+
+  double2 ra[kTM / 8], rb[kTN / 8];
+  auto load_stage = [&](int kb) {
+    const int k = t.k_begin + kb * kBK + kc;
+    const bool kin = (kb * kBK + kc) < t.k_count;
+#pragma unroll
+    for (int q = 0; q < kTM / 8; ++q) {
+      ra[q] = make_double2(0.0, 0.0);
+      if (kin && a_band[q] >= 0) ra[q] = __ldg(aqsn + (size_t)a_band[q] * G + k);
+    }
+#pragma unroll
+    for (int q = 0; q < kTN / 8; ++q) {
+      const int p = t.p_begin + q * 8 + r_lo;
+      rb[q] = make_double2(0.0, 0.0);
+      if (kin && p < P) {
+        double2 x = __ldcs(X0 + (size_t)p * G + k);
+        if (X1) {
+          const double2 y = __ldcs(X1 + (size_t)p * G + k);
+          x.x -= y.x;
+          x.y -= y.y;
+        }
+        rb[q] = x;
+      }
+    }
+  };
+  auto store_stage = [&](int buf) {
+#pragma unroll
+    for (int q = 0; q < kTM / 8; ++q) sm.a[buf][(q * 8 + r_lo) * kLds + kc] = ra[q];
+#pragma unroll
+    for (int q = 0; q < kTN / 8; ++q) sm.b[buf][(q * 8 + r_lo) * kLds + kc] = rb[q];
+  };
+
+  double cr[4][2][2], ci[4][2][2];
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+#pragma unroll
+    for (int n = 0; n < 2; ++n) cr[m][n][0] = cr[m][n][1] = ci[m][n][0] = ci[m][n][1] = 0.0;
+
+  const int nk = (t.k_count + kBK - 1) / kBK;
+  if (nk > 0) {
+    load_stage(0);
+    store_stage(0);
+  }
+  __syncthreads();
+  for (int kb = 0; kb < nk; ++kb) {
+    const int buf = kb & 1;
+    if (kb + 1 < nk) load_stage(kb + 1);
+    const double2 *sa = sm.a[buf];
+    const double2 *sb = sm.b[buf] + (warp * 16) * kLds;
+#pragma unroll
+    for (int ks = 0; ks < kBK / 4; ++ks) {
+      double ar[4], ai[4], br[2], bi[2], bn[2];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const double2 v = sa[(m * 8 + g8) * kLds + ks * 4 + t4];
+        ar[m] = v.x;
+        ai[m] = v.y;
+      }
+#pragma unroll
+      for (int n = 0; n < 2; ++n) {
+        const double2 v = sb[(n * 8 + g8) * kLds + ks * 4 + t4];
+        br[n] = v.x;
+        bi[n] = v.y;
+        bn[n] = -v.y;
+      }
+#pragma unroll
+      for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int n = 0; n < 2; ++n) {
+          dmma_f64(cr[m][n][0], cr[m][n][1], ar[m], br[n]);
+          dmma_f64(cr[m][n][0], cr[m][n][1], ai[m], bn[n]);
+          dmma_f64(ci[m][n][0], ci[m][n][1], ar[m], bi[n]);
+          dmma_f64(ci[m][n][0], ci[m][n][1], ai[m], br[n]);
+        }
+    }
+    if (kb + 1 < nk) store_stage(buf ^ 1);
+    __syncthreads();
+  }
+
+  // Epilogue: sum_r coef(r) sum_p W(band(r), p) C(r, p) over this thread's
+  // accumulator entries (row m*8+g8, column warp*16 + n*8 + 2*t4 + j).
+  double vr = 0.0, vi = 0.0;
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    const int r = m * 8 + g8;
+    if (r >= t.row_count) continue;
+    const FFRow row = rows[t.row_begin + r];
+#pragma unroll
+    for (int n = 0; n < 2; ++n)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int p = t.p_begin + warp * 16 + n * 8 + 2 * t4 + j;
+        if (p >= P) continue;
+        const double2 w = W[(size_t)row.band * P + p];
+        const double xr = cr[m][n][j], xi = ci[m][n][j];
+        vr = fma(row.coef, xr * w.x - xi * w.y, vr);
+        vi = fma(row.coef, xr * w.y + xi * w.x, vi);
+      }
+  }
+  double v[2] = {vr, vi};
+  block_sum<2, kFFThreads>(v, sm.red);
+  if (tid == 0) {
+    partials[(size_t)blockIdx.x * 2 + 0] = v[0];
+    partials[(size_t)blockIdx.x * 2 + 1] = v[1];
+  }
+}
+
+// Sums the partials of each output segment in tile order and writes
+// achs (1 complex), asx (nE complex) and cor (nE complex).  One block.
+__global__ void __launch_bounds__(256)
+    ff_finalize_kernel(const double *__restrict__ partials, int s0, int s1, int s2, int s3, int nE,
+                       double *__restrict__ achs, double *__restrict__ asx, double *__restrict__ cor) {
+  __shared__ double red[8 * 2];
+  __shared__ double res[OUT_COUNT][2];
+  const int seg[4] = {s0, s1, s2, s3};
+  for (int o = 0; o < OUT_COUNT; ++o) {
+    double v[2] = {0.0, 0.0};
+    for (int i = seg[o] + threadIdx.x; i < seg[o + 1]; i += 256) {
+      v[0] += partials[(size_t)i * 2];
+      v[1] += partials[(size_t)i * 2 + 1];
+    }
+    block_sum<2, 256>(v, red);
+    if (threadIdx.x == 0) {
+      res[o][0] = v[0];
+      res[o][1] = v[1];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && achs) {
+    achs[0] = res[OUT_ACHS][0];
+    achs[1] = res[OUT_ACHS][1];
+  }
+  for (int i = threadIdx.x; i < nE; i += 256) {
+    if (asx) {
+      asx[2 * i] = res[OUT_ASX][0];
+      asx[2 * i + 1] = res[OUT_ASX][1];
+    }
+    if (cor) {
+      cor[2 * i] = res[OUT_COR][0];
+      cor[2 * i + 1] = res[OUT_COR][1];
+    }
+  }
+}
+
+}  // namespace
+
+// Builds the plan of the requested sums (host copies of ekq[0..nb) and
+// dFreqGrid); sizes the k split for the device.
+int ff_make_plan(CallEnv *env, int64_t nb, int64_t nvband, int64_t P, int64_t G, int64_t nFreq, double fmin,
+                 double fstep, double occ, const double *ekq_h, const double *grid_h, bool want_achs,
+                 bool want_asx, bool want_cor, FFPlan *plan) {
+  const size_t smem = sizeof(FFSmem);
+  BGW_CUDA_TRY(cudaFuncSetAttribute(ff_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  BGW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ff_contract_kernel, kFFThreads, smem));
+  return build_plan(nb, nvband, P, G, nFreq, fmin, fstep, occ, ekq_h, grid_h, want_achs, want_asx, want_cor,
+                    2 * env->ws->sm_count * std::max(per_sm, 1), plan);
+}
+
+// Enqueues a planned FF evaluation.  Device pointers; R / A point at
+// frequency slice r_f0 / a_f0.  Outputs are device pointers (nullptr skips).
+int ff_launch(CallEnv *env, const FFPlan &plan, int64_t nb_w, int64_t nE, int64_t G, int64_t P,
+              const int32_t *inv, const int32_t *indinv, int64_t indinv_len, const double2 *am, const double2 *an,
+              const double *vc, const double2 *R, int r_f0, const double2 *A, int a_f0, double *achs_dev,
+              double *asx_dev, double *cor_dev) {
+  Workspace *ws = env->ws;
+  cudaStream_t stream = env->stream;
+  const size_t smem = sizeof(FFSmem);
+
+  // Plan upload: rows then tiles, one copy.
+  const size_t rows_bytes = sizeof(FFRow) * plan.rows.size();
+  const size_t tiles_off = (rows_bytes + 255) & ~size_t(255);
+  const size_t plan_bytes = tiles_off + sizeof(FFTile) * plan.tiles.size();
+  std::vector<unsigned char> host_plan(std::max<size_t>(plan_bytes, 1));
+  if (rows_bytes) std::memcpy(host_plan.data(), plan.rows.data(), rows_bytes);
+  if (!plan.tiles.empty())
+    std::memcpy(host_plan.data() + tiles_off, plan.tiles.data(), sizeof(FFTile) * plan.tiles.size());
+  void *d_plan = nullptr, *W = nullptr, *partials = nullptr;
+  BGW_TRY(ws_reserve(ws, SLOT_PLAN, host_plan.size(), &d_plan));
+  BGW_CUDA_TRY(cudaMemcpyAsync(d_plan, host_plan.data(), host_plan.size(), cudaMemcpyHostToDevice, stream));
+  const FFRow *d_rows = reinterpret_cast<const FFRow *>(d_plan);
+  const FFTile *d_tiles = reinterpret_cast<const FFTile *>(static_cast<unsigned char *>(d_plan) + tiles_off);
+
+  BGW_TRY(ws_reserve(ws, SLOT_TABLE2, sizeof(double2) * (size_t)std::max<int64_t>(nb_w * P, 1), &W));
+  if (nb_w * P > 0) {
+    int g = (int)std::min<long long>((nb_w * P + 255) / 256, (long long)ws->sm_count * 8);
+    ff_w_kernel<<<g, 256, 0, stream>>>((int)nb_w, (int)P, (int)G, inv, indinv, indinv_len, am, vc, (double2 *)W,
+                                       env->d_status);
+    count_launch();
+    BGW_CUDA_TRY(cudaGetLastError());
+  }
+  const int ntiles = (int)plan.tiles.size();
+  BGW_TRY(ws_reserve(ws, SLOT_PARTIALS, sizeof(double) * 2 * (size_t)std::max(ntiles, 1), &partials));
+  BGW_TRY(prof_mark(env, 1));
+  if (ntiles > 0) {
+    ff_contract_kernel<<<ntiles, kFFThreads, smem, stream>>>(d_tiles, d_rows, (int)P, (int)G, an, R, r_f0, A, a_f0,
+                                                             (const double2 *)W, (double *)partials);
+    count_launch();
+    BGW_CUDA_TRY(cudaGetLastError());
+  }
+  BGW_TRY(prof_mark(env, 2));
+  {
+    // Compulsory bytes of the contraction: every frequency slice it reads
+    // (R, A or both) once, plus the aqsn rows and the W table.
+    double slices = 0.0;
+    for (const auto &b : plan.slice_reads) slices += b;
+    env->prof.flops = 8.0 * plan.useful_cmacs;
+    env->prof.main_bytes = slices * 16.0 * (double)P * (double)G + 16.0 * (double)nb_w * (double)G +
+                           16.0 * (double)nb_w * (double)P;
+    env->prof.main_launches = ntiles > 0 ? 1 : 0;
+    std::snprintf(env->prof.main_kernel, sizeof(env->prof.main_kernel), "ff_contract_kernel");
+  }
+  ff_finalize_kernel<<<1, 256, 0, stream>>>((const double *)partials, plan.seg[0], plan.seg[1], plan.seg[2],
+                                            plan.seg[3], (int)nE, achs_dev, asx_dev, cor_dev);
+  count_launch();
+  BGW_CUDA_TRY(cudaGetLastError());
+  // The pageable plan buffer must outlive its (staged) upload.
+  BGW_CUDA_TRY(cudaStreamSynchronize(stream));
+  return BGW_OK;
+}
+
+}  // namespace bgw

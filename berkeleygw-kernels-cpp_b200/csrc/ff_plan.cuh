@@ -1,0 +1,47 @@
+// ff_plan.cuh -- host-side plan of the FF contractions (ff.cu).
+#pragma once
+
+#include <vector>
+
+#include "bgw_internal.cuh"
+
+namespace bgw {
+
+enum { SRC_R = 0, SRC_A = 1, SRC_RA = 2 };
+enum { OUT_ACHS = 0, OUT_ASX = 1, OUT_COR = 2, OUT_COUNT = 3 };
+
+struct FFRow {
+  int32_t band;
+  int32_t pad;
+  double coef;
+};
+
+struct FFTile {
+  int32_t src, f, row_begin, row_count;
+  int32_t p_begin, k_begin, k_count, out;
+};
+
+struct FFPlan {
+  std::vector<FFRow> rows;
+  std::vector<FFTile> tiles;
+  int seg[OUT_COUNT + 1] = {0, 0, 0, 0};  // tile range of each output
+  double useful_cmacs = 0.0;               // sum over groups rows * P * G
+  // Frequency slices read from I_epsR / I_epsA: [lo, hi] (lo > hi: none).
+  int r_lo = 1 << 30, r_hi = -1, a_lo = 1 << 30, a_hi = -1;
+  std::vector<double> slice_reads;  // distinct [ngpown][ncouls] slices read
+};
+
+// Builds the plan of the requested sums from host copies of ekq[0..nb) and
+// dFreqGrid; sizes the k split for the device.
+int ff_make_plan(CallEnv *env, int64_t nb, int64_t nvband, int64_t P, int64_t G, int64_t nFreq, double fmin,
+                 double fstep, double occ, const double *ekq_h, const double *grid_h, bool want_achs,
+                 bool want_asx, bool want_cor, FFPlan *plan);
+
+// Enqueues a planned FF evaluation.  Device pointers; R / A point at
+// frequency slice r_f0 / a_f0.  Outputs are device pointers (nullptr skips).
+int ff_launch(CallEnv *env, const FFPlan &plan, int64_t nb_w, int64_t nE, int64_t G, int64_t P,
+              const int32_t *inv, const int32_t *indinv, int64_t indinv_len, const double2 *am, const double2 *an,
+              const double *vc, const double2 *R, int r_f0, const double2 *A, int a_f0, double *achs_dev,
+              double *asx_dev, double *cor_dev);
+
+}  // namespace bgw

@@ -1,0 +1,424 @@
+// gpp.cu -- GPP self-energy summation (noflagOCC_solver, GPP/gpp.cpp:307-402)
+// on sm_100a, FP64.
+//
+// Work decomposition.  The reference sum
+//   achtemp[iw] = sum_{n1, p, ig} s(n1, p) * q(p, ig, iw; wx[n1][iw]),
+//   s(n1, p)    = conj(aqsm[n1][igp]) aqsn[n1][igp] 0.5 vcoul[igp] wtilde[p][igp]
+//                 (sch_store1, gpp.cpp:369-371),
+//   q           = conj(wdiff) / |wdiff|^2 * I_eps[p][ig],  wdiff = wx - wtilde[p][ig]
+//                 (gpp.cpp:374-380)
+// is split into items (p, a chunk of CH consecutive ig).  An item's wtilde /
+// I_eps chunk is staged once into shared memory by 1-D bulk copies (TMA
+// engine, mbarrier completion, double-buffered across items) and lifted into
+// registers; the CTA then sweeps every band n1 over it, so each element of
+// the 1.7 GB wtilde / I_eps arrays is read from HBM once while the FP64 pipe
+// evaluates nb * 3 quotients on it.  s(n1, p) is precomputed into a
+// [p][n1] table by gpp_prep_kernel and staged per item alongside the chunk.
+//
+// Reduction.  Each thread accumulates its own 3 complex sums; a CTA folds
+// them with warp butterflies and a fixed warp order into one partial; a
+// single-block kernel sums the partials in a fixed order.  No atomics, so
+// reruns are bitwise identical.
+#include <algorithm>
+#include <cstdio>
+
+#include "bgw_internal.cuh"
+#include "reduce.cuh"
+
+namespace bgw {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kElems = 4;                 // ig elements per thread
+constexpr int kChunk = kThreads * kElems;  // ig per item
+
+// ---------------------------------------------------------------- prep --
+// st[p][n1] = sch_store1(n1, p); wx4[n1] = (wx[n1][0..2], 0); S[p] (if
+// requested) = sum_n1 st[p][n1] in a fixed order.  Indices are checked: an
+// out-of-range inv_igp_index / indinv entry raises BGW_ERR_INDEX and that
+// column contributes zero (no out-of-bounds read is ever issued).
+__device__ __forceinline__ int resolve_igp(int p, const int *__restrict__ inv, const int *__restrict__ indinv,
+                                           long long indinv_len, int G, int *status) {
+  int a = inv[p];
+  if (a < 0 || (long long)a >= indinv_len) {
+    raise_status(status, BGW_ERR_INDEX, p);
+    return -1;
+  }
+  int g = indinv[a];
+  if (g < 0 || g >= G) {
+    raise_status(status, BGW_ERR_INDEX, p);
+    return -1;
+  }
+  return g;
+}
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+__device__ __forceinline__ double2 store1(const double2 *__restrict__ am, const double2 *__restrict__ an,
+                                          const double *__restrict__ vc, const double2 *__restrict__ wt, int n1,
+                                          int p, int g, int G) {
+  double2 m = am[(size_t)n1 * G + g];
+  m.y = -m.y;
+  double2 r = cmul(m, an[(size_t)n1 * G + g]);
+  r.x *= 0.5;
+  r.y *= 0.5;
+  double v = vc[g];
+  r.x *= v;
+  r.y *= v;
+  return cmul(r, wt[(size_t)p * G + g]);
+}
+
+// One warp per column p: st row (if st != nullptr) and S[p] (if S != nullptr).
+__global__ void __launch_bounds__(256) gpp_prep_kernel(int nb, int P, int G, const int *__restrict__ inv,
+                                                       const int *__restrict__ indinv, long long indinv_len,
+                                                       const double2 *__restrict__ wt, const double2 *__restrict__ am,
+                                                       const double2 *__restrict__ an, const double *__restrict__ vc,
+                                                       double2 *__restrict__ st, double2 *__restrict__ S,
+                                                       int *status) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < P; p += warps) {
+    int g = resolve_igp(p, inv, indinv, indinv_len, G, status);
+    double sr = 0.0, si = 0.0;
+    for (int n1 = lane; n1 < nb; n1 += 32) {
+      double2 s = make_double2(0.0, 0.0);
+      if (g >= 0) s = store1(am, an, vc, wt, n1, p, g, G);
+      if (st) st[(size_t)p * nb + n1] = s;
+      sr += s.x;
+      si += s.y;
+    }
+    if (S) {
+      sr = warp_sum(sr);
+      si = warp_sum(si);
+      if (lane == 0) S[p] = make_double2(sr, si);
+    }
+  }
+}
+
+__global__ void gpp_wx_kernel(int nb, const double *__restrict__ wx, long long stride, double4 *__restrict__ wx4) {
+  for (int n1 = blockIdx.x * blockDim.x + threadIdx.x; n1 < nb; n1 += gridDim.x * blockDim.x) {
+    const double *w = wx + (size_t)n1 * stride;
+    wx4[n1] = make_double4(w[0], w[1], w[2], 0.0);
+  }
+}
+
+// ------------------------------------------------------------ band loop --
+// Per element (wtilde = wr + i wi, I_eps = Ir + i Ii) the band-independent
+// constants are kept in registers:  wi^2, a = -wi*Ii, b = wi*Ir, so that for
+// a frequency x:
+//   dr  = x - wr,  |wdiff|^2 = dr^2 + wi^2,
+//   conj(wdiff) * I_eps = (dr*Ir + a) + i (dr*Ii + b).
+struct Elem {
+  double wr, wi2, Ir, Ii, a, b;
+};
+
+template <int BCH, bool WX_SHARED>
+struct BandSmem {
+  double2 wt[2][kChunk];
+  double2 ie[2][kChunk];
+  double2 st[2][BCH];
+  double4 wx[2][WX_SHARED ? 1 : BCH];
+  unsigned long long bar[2];
+  double red[(kThreads / 32) * 6];
+};
+
+template <int BCH, bool WX_SHARED>
+__global__ void __launch_bounds__(kThreads, 2)
+    gpp_bandloop_kernel(int nb, int G, long long items, int nchunks_g, const double2 *__restrict__ wtilde,
+                        const double2 *__restrict__ ieps, const double2 *__restrict__ st,
+                        const double4 *__restrict__ wx4, const double *__restrict__ wx3,
+                        double *__restrict__ partials, int *status) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  using Smem = BandSmem<BCH, WX_SHARED>;
+  Smem &sm = *reinterpret_cast<Smem *>(smem_raw);
+  const int tid = threadIdx.x;
+  const int nbc = (nb + BCH - 1) / BCH;
+
+  long long my_items = 0;
+  if ((long long)blockIdx.x < items) my_items = (items - 1 - blockIdx.x) / gridDim.x + 1;
+  const long long nsteps = my_items * nbc;
+
+  if (tid == 0) {
+    mbar_init(reinterpret_cast<uint64_t *>(&sm.bar[0]), 1);
+    mbar_init(reinterpret_cast<uint64_t *>(&sm.bar[1]), 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  // Thread 0 stages step j into buffer j & 1.
+  auto issue = [&](long long j) {
+    const long long item = blockIdx.x + (j / nbc) * (long long)gridDim.x;
+    const int c = (int)(j % nbc);
+    const long long p = item / nchunks_g;
+    const int g0 = (int)(item % nchunks_g) * kChunk;
+    const int nvalid = min(kChunk, G - g0);
+    const int b0 = c * BCH;
+    const int nbv = min(BCH, nb - b0);
+    const int buf = (int)(j & 1);
+    uint32_t bytes = 2u * nvalid * 16u + nbv * 16u + (WX_SHARED ? 0u : nbv * 32u);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(&sm.bar[buf]);
+    mbar_expect_tx(bar, bytes);
+    bulk_g2s(sm.wt[buf], wtilde + p * G + g0, nvalid * 16u, bar);
+    bulk_g2s(sm.ie[buf], ieps + p * G + g0, nvalid * 16u, bar);
+    bulk_g2s(sm.st[buf], st + p * nb + b0, nbv * 16u, bar);
+    if (!WX_SHARED) bulk_g2s(sm.wx[buf], wx4 + b0, nbv * 32u, bar);
+  };
+
+  double x0s = 0.0, x1s = 0.0, x2s = 0.0;
+  if (WX_SHARED) {
+    x0s = wx3[0];
+    x1s = wx3[1];
+    x2s = wx3[2];
+  }
+  double acc_r[3] = {0.0, 0.0, 0.0}, acc_i[3] = {0.0, 0.0, 0.0};
+  bool ok = true;
+  if (tid == 0 && nsteps > 0) issue(0);
+
+  for (long long j = 0; j < nsteps; ++j) {
+    if (tid == 0 && j + 1 < nsteps) issue(j + 1);
+    const int buf = (int)(j & 1);
+    if (!mbar_wait_bounded(reinterpret_cast<uint64_t *>(&sm.bar[buf]), (uint32_t)((j >> 1) & 1), kWaitCycles)) {
+      raise_status(status, BGW_ERR_TIMEOUT, blockIdx.x);
+      ok = false;
+    }
+    // Every thread must agree before leaving the loop.
+    if (__syncthreads_or(!ok)) break;
+
+    const long long item = blockIdx.x + (j / nbc) * (long long)gridDim.x;
+    const int c = (int)(j % nbc);
+    const int g0 = (int)(item % nchunks_g) * kChunk;
+    const int nvalid = min(kChunk, G - g0);
+    const int b0 = c * BCH;
+    const int nbv = min(BCH, nb - b0);
+
+    Elem e[kElems];
+#pragma unroll
+    for (int k = 0; k < kElems; ++k) {
+      const int idx = k * kThreads + tid;
+      if (idx < nvalid) {
+        double2 w = sm.wt[buf][idx], v = sm.ie[buf][idx];
+        e[k].wr = w.x;
+        e[k].wi2 = w.y * w.y;
+        e[k].Ir = v.x;
+        e[k].Ii = v.y;
+        e[k].a = -w.y * v.y;
+        e[k].b = w.y * v.x;
+      } else {  // padding: contributes exactly zero, keeps |wdiff|^2 >= 1
+        e[k].wr = 0.0;
+        e[k].wi2 = 1.0;
+        e[k].Ir = e[k].Ii = e[k].a = e[k].b = 0.0;
+      }
+    }
+
+    for (int bb = 0; bb < nbv; ++bb) {
+      double x[3];
+      if (WX_SHARED) {
+        x[0] = x0s;
+        x[1] = x1s;
+        x[2] = x2s;
+      } else {
+        double4 w4 = sm.wx[buf][bb];
+        x[0] = w4.x;
+        x[1] = w4.y;
+        x[2] = w4.z;
+      }
+      const double2 s = sm.st[buf][bb];
+      double tr[3] = {0.0, 0.0, 0.0}, ti[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+      for (int k = 0; k < kElems; ++k) {
+#pragma unroll
+        for (int iw = 0; iw < 3; ++iw) {
+          const double dr = x[iw] - e[k].wr;
+          const double den = fma(dr, dr, e[k].wi2);
+          const double r = rcp_refined(den);
+          const double nr = fma(dr, e[k].Ir, e[k].a);
+          const double ni = fma(dr, e[k].Ii, e[k].b);
+          tr[iw] = fma(nr, r, tr[iw]);
+          ti[iw] = fma(ni, r, ti[iw]);
+        }
+      }
+#pragma unroll
+      for (int iw = 0; iw < 3; ++iw) {
+        acc_r[iw] = fma(tr[iw], s.x, acc_r[iw]);
+        acc_r[iw] = fma(-ti[iw], s.y, acc_r[iw]);
+        acc_i[iw] = fma(tr[iw], s.y, acc_i[iw]);
+        acc_i[iw] = fma(ti[iw], s.x, acc_i[iw]);
+      }
+    }
+    __syncthreads();  // buffer `buf` is free for step j + 2
+  }
+  if (!ok && tid == 0) {
+    // Let copies still in flight land before the CTA's shared memory is
+    // released (bounded as well).
+    (void)mbar_wait_bounded(reinterpret_cast<uint64_t *>(&sm.bar[0]), 0, kWaitCycles);
+    (void)mbar_wait_bounded(reinterpret_cast<uint64_t *>(&sm.bar[1]), 0, kWaitCycles);
+  }
+
+  double v[6] = {acc_r[0], acc_i[0], acc_r[1], acc_i[1], acc_r[2], acc_i[2]};
+  block_sum<6, kThreads>(v, sm.red);
+  if (tid == 0) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) partials[(size_t)blockIdx.x * 6 + k] = v[k];
+  }
+}
+
+// ------------------------------------------------------------- factored --
+// Band-independent wx: achtemp[iw] = sum_p S(p) * sum_ig q(p, ig, iw).
+// HBM-bound stream over wtilde / I_eps with 128-bit loads; one item =
+// (p, chunk of kChunk ig); per-thread sums are folded per CTA.
+__global__ void __launch_bounds__(kThreads)
+    gpp_factored_kernel(int G, long long items, int nchunks_g, const double2 *__restrict__ wtilde,
+                        const double2 *__restrict__ ieps, const double2 *__restrict__ S,
+                        const double *__restrict__ wx3, double *__restrict__ partials) {
+  __shared__ double red[(kThreads / 32) * 6];
+  const int tid = threadIdx.x;
+  const double x[3] = {wx3[0], wx3[1], wx3[2]};
+  double acc_r[3] = {0.0, 0.0, 0.0}, acc_i[3] = {0.0, 0.0, 0.0};
+  for (long long item = blockIdx.x; item < items; item += gridDim.x) {
+    const long long p = item / nchunks_g;
+    const int g0 = (int)(item % nchunks_g) * kChunk;
+    double2 w[kElems], v[kElems];
+#pragma unroll
+    for (int k = 0; k < kElems; ++k) {
+      const int ig = g0 + k * kThreads + tid;
+      if (ig < G) {
+        w[k] = __ldcs(wtilde + p * G + ig);
+        v[k] = __ldcs(ieps + p * G + ig);
+      } else {
+        w[k] = make_double2(0.0, 1.0);
+        v[k] = make_double2(0.0, 0.0);
+      }
+    }
+    double tr[3] = {0.0, 0.0, 0.0}, ti[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < kElems; ++k) {
+      const double wi2 = w[k].y * w[k].y, a = -w[k].y * v[k].y, b = w[k].y * v[k].x;
+#pragma unroll
+      for (int iw = 0; iw < 3; ++iw) {
+        const double dr = x[iw] - w[k].x;
+        const double r = rcp_refined(fma(dr, dr, wi2));
+        tr[iw] = fma(fma(dr, v[k].x, a), r, tr[iw]);
+        ti[iw] = fma(fma(dr, v[k].y, b), r, ti[iw]);
+      }
+    }
+    const double2 s = S[p];
+#pragma unroll
+    for (int iw = 0; iw < 3; ++iw) {
+      acc_r[iw] = fma(tr[iw], s.x, acc_r[iw]);
+      acc_r[iw] = fma(-ti[iw], s.y, acc_r[iw]);
+      acc_i[iw] = fma(tr[iw], s.y, acc_i[iw]);
+      acc_i[iw] = fma(ti[iw], s.x, acc_i[iw]);
+    }
+  }
+  double vv[6] = {acc_r[0], acc_i[0], acc_r[1], acc_i[1], acc_r[2], acc_i[2]};
+  block_sum<6, kThreads>(vv, red);
+  if (tid == 0) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) partials[(size_t)blockIdx.x * 6 + k] = vv[k];
+  }
+}
+
+template <int BCH, bool WX_SHARED>
+int launch_bandloop(Workspace *ws,cudaStream_t stream, int nb, int G, long long items, int nchunks_g,
+                    const double2 *wt, const double2 *ie, const double2 *st, const double4 *wx4, const double *wx3,
+                    double **partials_out, int *grid_out, int *status) {
+  using Smem = BandSmem<BCH, WX_SHARED>;
+  const size_t smem = sizeof(Smem);
+  auto kfn = gpp_bandloop_kernel<BCH, WX_SHARED>;
+  BGW_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  BGW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kThreads, smem));
+  if (per_sm < 1) return BGW_ERR_UNSUPPORTED;
+  long long grid = std::min<long long>(items, (long long)ws->sm_count * per_sm);
+  if (grid < 1) grid = 1;
+  void *partials = nullptr;
+  BGW_TRY(ws_reserve(ws, SLOT_PARTIALS, sizeof(double) * 6 * (size_t)grid, &partials));
+  *grid_out = (int)grid;
+  *partials_out = (double *)partials;
+  kfn<<<(int)grid, kThreads, smem, stream>>>(nb, G, items, nchunks_g, wt, ie, st, wx4, wx3, (double *)partials,
+                                             status);
+  count_launch();
+  BGW_CUDA_TRY(cudaGetLastError());
+  return BGW_OK;
+}
+
+}  // namespace
+
+// Enqueues the GPP sum on env->stream.  All pointers are device pointers;
+// wx holds 3 doubles (wx_stride == 0) or nb rows of wx_stride doubles.
+// achtemp_dev receives 6 doubles (3 complex).
+int gpp_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *inv, const int32_t *indinv,
+                int64_t indinv_len, const double *wx, int64_t wx_stride, const double2 *wt, const double2 *am,
+                const double2 *an, const double2 *ie, const double *vc, double *achtemp_dev) {
+  Workspace *ws = env->ws;
+  cudaStream_t stream = env->stream;
+  const int nchunks_g = (int)((G + kChunk - 1) / kChunk);
+  const long long items = (long long)P * nchunks_g;
+  const bool factored = env->opt.gpp_algorithm == BGW_GPP_FACTORED;
+  int prep_grid = (int)std::min<long long>((P + 7) / 8, (long long)ws->sm_count * 16);
+  if (prep_grid < 1) prep_grid = 1;
+
+  if (factored) {
+    if (wx_stride != 0) return BGW_ERR_UNSUPPORTED;  // needs a band-independent wx
+    void *S = nullptr, *partials = nullptr;
+    BGW_TRY(ws_reserve(ws, SLOT_TABLE0, sizeof(double2) * (size_t)std::max<int64_t>(P, 1), &S));
+    gpp_prep_kernel<<<prep_grid, 256, 0, stream>>>((int)nb, (int)P, (int)G, inv, indinv, indinv_len, wt, am, an,
+                                                   vc, nullptr, (double2 *)S, env->d_status);
+    count_launch();
+    BGW_CUDA_TRY(cudaGetLastError());
+    int grid = (int)std::min<long long>(std::max<long long>(items, 1), (long long)ws->sm_count * 8);
+    BGW_TRY(ws_reserve(ws, SLOT_PARTIALS, sizeof(double) * 6 * (size_t)grid, &partials));
+    BGW_TRY(prof_mark(env, 1));
+    gpp_factored_kernel<<<grid, kThreads, 0, stream>>>((int)G, items, nchunks_g, wt, ie, (const double2 *)S, wx,
+                                                       (double *)partials);
+    count_launch();
+    BGW_CUDA_TRY(cudaGetLastError());
+    BGW_TRY(prof_mark(env, 2));
+    env->prof.main_bytes = 32.0 * (double)P * (double)G + 16.0 * (double)P;
+    env->prof.main_launches = 1;
+    std::snprintf(env->prof.main_kernel, sizeof(env->prof.main_kernel), "gpp_factored_kernel");
+    reduce_partials_kernel<6><<<1, 256, 0, stream>>>((const double *)partials, grid, achtemp_dev);
+    count_launch();
+    BGW_CUDA_TRY(cudaGetLastError());
+    return BGW_OK;
+  }
+
+  void *st = nullptr, *wx4 = nullptr;
+  BGW_TRY(ws_reserve(ws, SLOT_TABLE0, sizeof(double2) * (size_t)std::max<int64_t>(P * nb, 1), &st));
+  gpp_prep_kernel<<<prep_grid, 256, 0, stream>>>((int)nb, (int)P, (int)G, inv, indinv, indinv_len, wt, am, an, vc,
+                                                 (double2 *)st, nullptr, env->d_status);
+  count_launch();
+  BGW_CUDA_TRY(cudaGetLastError());
+  const bool wx_shared = (wx_stride == 0);
+  if (!wx_shared) {
+    BGW_TRY(ws_reserve(ws, SLOT_TABLE1, sizeof(double4) * (size_t)std::max<int64_t>(nb, 1), &wx4));
+    int g = (int)std::min<int64_t>((nb + 255) / 256, 1024);
+    gpp_wx_kernel<<<std::max(g, 1), 256, 0, stream>>>((int)nb, wx, wx_stride, (double4 *)wx4);
+    count_launch();
+    BGW_CUDA_TRY(cudaGetLastError());
+  }
+  int grid = 0;
+  double *partials = nullptr;
+  BGW_TRY(prof_mark(env, 1));
+  if (wx_shared) {
+    BGW_TRY((launch_bandloop<512, true>(ws, stream, (int)nb, (int)G, items, nchunks_g, wt, ie, (const double2 *)st,
+                                        nullptr, wx, &partials, &grid, env->d_status)));
+  } else {
+    BGW_TRY((launch_bandloop<256, false>(ws, stream, (int)nb, (int)G, items, nchunks_g, wt, ie,
+                                         (const double2 *)st, (const double4 *)wx4, nullptr, &partials, &grid,
+                                         env->d_status)));
+  }
+  BGW_TRY(prof_mark(env, 2));
+  env->prof.main_bytes = 32.0 * (double)P * (double)G + 16.0 * (double)P * (double)nb +
+                         (wx_shared ? 24.0 : 32.0 * (double)nb);
+  env->prof.main_launches = 1;
+  std::snprintf(env->prof.main_kernel, sizeof(env->prof.main_kernel), "gpp_bandloop_kernel");
+  reduce_partials_kernel<6><<<1, 256, 0, stream>>>(partials, grid, achtemp_dev);
+  count_launch();
+  BGW_CUDA_TRY(cudaGetLastError());
+  return BGW_OK;
+}
+
+}  // namespace bgw

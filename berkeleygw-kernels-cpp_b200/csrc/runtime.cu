@@ -1,0 +1,219 @@
+// runtime.cu -- options, per-device workspace cache, host<->device staging
+// and status handling shared by every libbgwsigma entry point.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+
+#include "bgw_internal.cuh"
+
+namespace bgw {
+
+std::atomic<uint64_t> g_launches{0};
+
+void note_cuda_error(cudaError_t e, const char *what, const char *file, int line) {
+  if (std::getenv("BGW_SIGMA_QUIET") == nullptr)
+    std::fprintf(stderr, "libbgwsigma: %s failed: %s (%s:%d)\n", what, cudaGetErrorString(e), file, line);
+}
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_ws_mu;
+std::unique_ptr<Workspace> g_ws[kMaxDevices];
+}  // namespace
+
+Workspace *workspace_for(int device) {
+  if (device < 0 || device >= kMaxDevices) return nullptr;
+  std::lock_guard<std::mutex> lk(g_ws_mu);
+  if (!g_ws[device]) {
+    g_ws[device].reset(new Workspace());
+    g_ws[device]->device = device;
+  }
+  return g_ws[device].get();
+}
+
+int ws_reserve(Workspace *ws, int s, size_t bytes, void **out) {
+  if (bytes == 0) bytes = 256;
+  if (ws->cap[s] < bytes) {
+    if (ws->buf[s]) {
+      // The old buffer may still be read by an earlier call's kernels.
+      BGW_CUDA_TRY(cudaDeviceSynchronize());
+      BGW_CUDA_TRY(cudaFree(ws->buf[s]));
+      ws->buf[s] = nullptr;
+      ws->cap[s] = 0;
+    }
+    size_t rounded = (bytes + 255) & ~size_t(255);
+    cudaError_t e = cudaMalloc(&ws->buf[s], rounded);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      ws->buf[s] = nullptr;
+      return BGW_ERR_ALLOC;
+    }
+    ws->cap[s] = rounded;
+  }
+  *out = ws->buf[s];
+  return BGW_OK;
+}
+
+int ws_acquire(Workspace *ws, cudaStream_t stream) {
+  if (!ws->last_use) {
+    BGW_CUDA_TRY(cudaEventCreateWithFlags(&ws->last_use, cudaEventDisableTiming));
+    for (auto &e : ws->prof) BGW_CUDA_TRY(cudaEventCreate(&e));
+    BGW_CUDA_TRY(cudaDeviceGetAttribute(&ws->sm_count, cudaDevAttrMultiProcessorCount, ws->device));
+    return BGW_OK;
+  }
+  BGW_CUDA_TRY(cudaStreamWaitEvent(stream, ws->last_use, 0));
+  return BGW_OK;
+}
+
+int ws_release(Workspace *ws, cudaStream_t stream) {
+  BGW_CUDA_TRY(cudaEventRecord(ws->last_use, stream));
+  return BGW_OK;
+}
+
+namespace {
+thread_local bgw_profile t_last_profile = {};
+}
+
+int prof_mark(CallEnv *env, int which) {
+  if (!env->profile) return BGW_OK;
+  BGW_CUDA_TRY(cudaEventRecord(env->ws->prof[which], env->stream));
+  return BGW_OK;
+}
+
+int begin_call(const bgw_options *user, CallEnv *env) {
+  bgw_options_init(&env->opt);
+  if (user) {
+    if (user->struct_size < (int32_t)offsetof(bgw_options, device_status) + (int32_t)sizeof(int32_t *))
+      return BGW_ERR_INVALID_ARG;
+    std::memcpy(&env->opt, user, sizeof(bgw_options));
+  }
+  const bgw_options &o = env->opt;
+  if (o.memory != BGW_MEMORY_HOST && o.memory != BGW_MEMORY_DEVICE) return BGW_ERR_INVALID_ARG;
+  if (o.precision != BGW_PRECISION_FP64 && o.precision != BGW_PRECISION_MIXED) return BGW_ERR_INVALID_ARG;
+  if (o.gpp_algorithm != BGW_GPP_BANDLOOP && o.gpp_algorithm != BGW_GPP_FACTORED) return BGW_ERR_INVALID_ARG;
+  if (o.wx_band_stride < 0) return BGW_ERR_INVALID_ARG;
+  if ((o.flags & BGW_FLAG_ASYNC) && (o.memory != BGW_MEMORY_DEVICE || o.device_status == nullptr))
+    return BGW_ERR_INVALID_ARG;
+  if ((o.flags & BGW_FLAG_PROFILE) && (o.flags & BGW_FLAG_ASYNC)) return BGW_ERR_INVALID_ARG;
+  env->profile = (o.flags & BGW_FLAG_PROFILE) != 0;
+  env->launches0 = g_launches.load();
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+    (void)cudaGetLastError();
+    return BGW_ERR_NO_DEVICE;
+  }
+  int dev = o.device;
+  if (dev < 0) BGW_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev >= ndev) return BGW_ERR_INVALID_ARG;
+  BGW_CUDA_TRY(cudaSetDevice(dev));
+  env->device = dev;
+  env->stream = static_cast<cudaStream_t>(o.stream);
+  env->host = (o.memory == BGW_MEMORY_HOST);
+  env->ws = workspace_for(dev);
+  if (!env->ws) return BGW_ERR_INVALID_ARG;
+  return BGW_OK;
+}
+
+int stage_input(CallEnv *env, int s, const void *src, size_t bytes, const void **dev_out) {
+  if (!env->host) {
+    if ((reinterpret_cast<uintptr_t>(src) & 15u) != 0) return BGW_ERR_INVALID_ARG;
+    *dev_out = src;
+    return BGW_OK;
+  }
+  void *d = nullptr;
+  BGW_TRY(ws_reserve(env->ws, s, bytes, &d));
+  if (bytes) BGW_CUDA_TRY(cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, env->stream));
+  *dev_out = d;
+  return BGW_OK;
+}
+
+int finish_call(CallEnv *env) {
+  BGW_TRY(ws_release(env->ws, env->stream));
+  if (env->opt.flags & BGW_FLAG_ASYNC) {
+    BGW_CUDA_TRY(cudaMemcpyAsync(env->opt.device_status, env->d_status, sizeof(int32_t),
+                                 cudaMemcpyDeviceToDevice, env->stream));
+    BGW_CUDA_TRY(cudaGetLastError());
+    return BGW_OK;
+  }
+  int32_t st[STATUS_WORDS] = {0, 0, 0, 0};
+  BGW_TRY(prof_mark(env, 3));
+  BGW_CUDA_TRY(cudaMemcpyAsync(st, env->d_status, sizeof(st), cudaMemcpyDeviceToHost, env->stream));
+  BGW_CUDA_TRY(cudaStreamSynchronize(env->stream));
+  BGW_CUDA_TRY(cudaGetLastError());
+  if (env->profile) {
+    float a = 0.f, b = 0.f;
+    BGW_CUDA_TRY(cudaEventElapsedTime(&a, env->ws->prof[1], env->ws->prof[2]));
+    BGW_CUDA_TRY(cudaEventElapsedTime(&b, env->ws->prof[0], env->ws->prof[3]));
+    env->prof.main_kernel_ms = a;
+    env->prof.device_ms = b;
+    env->prof.total_launches = (int32_t)(g_launches.load() - env->launches0);
+    t_last_profile = env->prof;
+  }
+  return st[0];
+}
+
+}  // namespace bgw
+
+extern "C" {
+
+void bgw_options_init(bgw_options *opt) {
+  if (!opt) return;
+  std::memset(opt, 0, sizeof(*opt));
+  opt->struct_size = (int32_t)sizeof(bgw_options);
+  opt->memory = BGW_MEMORY_HOST;
+  opt->precision = BGW_PRECISION_FP64;
+  opt->gpp_algorithm = BGW_GPP_BANDLOOP;
+  opt->wx_band_stride = 0;
+  opt->device = -1;
+  opt->flags = 0;
+  opt->stream = nullptr;
+  opt->device_status = nullptr;
+}
+
+const char *bgw_status_string(int status) {
+  switch (status) {
+    case BGW_OK: return "success";
+    case BGW_ERR_INVALID_ARG: return "invalid argument";
+    case BGW_ERR_INDEX: return "index out of range (inv_igp_index/indinv)";
+    case BGW_ERR_CUDA: return "CUDA runtime error";
+    case BGW_ERR_ALLOC: return "allocation failed";
+    case BGW_ERR_NO_DEVICE: return "no usable CUDA device";
+    case BGW_ERR_TIMEOUT: return "device-side wait timed out";
+    case BGW_ERR_UNSUPPORTED: return "unsupported option combination";
+    default: return "unknown status";
+  }
+}
+
+int bgw_abi_version(void) { return BGW_SIGMA_ABI_VERSION; }
+
+int bgw_last_profile(bgw_profile *out) {
+  if (!out) return BGW_ERR_INVALID_ARG;
+  *out = bgw::t_last_profile;
+  return BGW_OK;
+}
+
+uint64_t bgw_launch_count(void) { return bgw::g_launches.load(); }
+
+int bgw_release_workspace(int32_t device) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return BGW_ERR_NO_DEVICE;
+  }
+  for (int d = 0; d < ndev && d < 64; ++d) {
+    if (device >= 0 && d != device) continue;
+    bgw::Workspace *ws = bgw::workspace_for(d);
+    std::lock_guard<std::mutex> lk(ws->mu);
+    BGW_CUDA_TRY(cudaSetDevice(d));
+    BGW_CUDA_TRY(cudaDeviceSynchronize());
+    for (int s = 0; s < bgw::SLOT_COUNT; ++s) {
+      if (ws->buf[s]) BGW_CUDA_TRY(cudaFree(ws->buf[s]));
+      ws->buf[s] = nullptr;
+      ws->cap[s] = 0;
+    }
+  }
+  return BGW_OK;
+}
+
+}  // extern "C"

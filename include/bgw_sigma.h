@@ -1,0 +1,200 @@
+/*
+ * bgw_sigma.h -- C ABI of libbgwsigma.so, the B200 (sm_100a) implementation
+ * of the BerkeleyGW GPP and full-frequency (FF) self-energy summations.
+ *
+ * Every entry point takes plain pointers and sizes, returns a bgw_status
+ * (0 = success, negative = error), never exits the process and never falls
+ * back to a CPU path: with no usable CUDA device it returns
+ * BGW_ERR_NO_DEVICE.
+ *
+ * Array conventions (identical to the reference's ArrayMD storage,
+ * arrayMD/arrayMD.h:156-184, with ComplexType = std::complex<double>,
+ * common/Defines.h:21-25):
+ *   - complex arrays are interleaved (re, im) doubles, row-major, last index
+ *     fastest; a complex [n][m] array is 2*n*m doubles;
+ *   - index arrays are int32.
+ * Pointers live in host memory (BGW_MEMORY_HOST, the default: the call copies
+ * what it reads to the GPU and the results back) or in device memory of the
+ * selected GPU (BGW_MEMORY_DEVICE).  Outputs are overwritten, never
+ * accumulated into, as in the reference (GPP/gpp.cpp:399-401,
+ * FF/ff.cpp:288-289, 374-375).
+ *
+ * Reductions are deterministic: no floating-point atomics, fixed-order
+ * combination, so a rerun on the same inputs and device is bitwise
+ * identical.
+ */
+#ifndef BGW_SIGMA_H
+#define BGW_SIGMA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BGW_SIGMA_ABI_VERSION 1
+
+typedef enum bgw_status {
+  BGW_OK = 0,
+  BGW_ERR_INVALID_ARG = -1, /* bad size, null pointer or option          */
+  BGW_ERR_INDEX = -2,       /* inv_igp_index / indinv entry out of range */
+  BGW_ERR_CUDA = -3,        /* a CUDA runtime call failed                */
+  BGW_ERR_ALLOC = -4,       /* device or pinned allocation failed        */
+  BGW_ERR_NO_DEVICE = -5,   /* no usable CUDA device                     */
+  BGW_ERR_TIMEOUT = -6,     /* a bounded device-side wait ran out        */
+  BGW_ERR_UNSUPPORTED = -7  /* option combination not implemented        */
+} bgw_status;
+
+enum { BGW_MEMORY_HOST = 0, BGW_MEMORY_DEVICE = 1 };
+enum { BGW_PRECISION_FP64 = 0, BGW_PRECISION_MIXED = 1 };
+/* GPP evaluation strategy:
+ *   BANDLOOP  evaluates every (band, G', G, frequency) quotient, as the
+ *             reference loop nest does (GPP/gpp.cpp:343-390); supports a
+ *             band-dependent wx (wx_band_stride != 0).
+ *   FACTORED  uses sum_n1 sch_store1(n1, p) once per G' column; valid only
+ *             for a band-independent wx (wx_band_stride == 0, the
+ *             reference's case) and bound by HBM bandwidth. */
+enum { BGW_GPP_BANDLOOP = 0, BGW_GPP_FACTORED = 1 };
+/* flags */
+enum {
+  BGW_FLAG_ASYNC = 1,  /* device memory only: enqueue on `stream` and return
+                          without synchronising; the device-side status is
+                          written to options->device_status (required).   */
+  BGW_FLAG_PROFILE = 2 /* time the call's dominant kernel and all its device
+                          work with CUDA events on `stream`; read back with
+                          bgw_last_profile() (synchronous calls only).     */
+};
+
+typedef struct bgw_options {
+  int32_t struct_size;     /* sizeof(bgw_options) (forward compatibility)   */
+  int32_t memory;          /* BGW_MEMORY_HOST / BGW_MEMORY_DEVICE           */
+  int32_t precision;       /* BGW_PRECISION_FP64 / BGW_PRECISION_MIXED      */
+  int32_t gpp_algorithm;   /* BGW_GPP_BANDLOOP / BGW_GPP_FACTORED           */
+  int64_t wx_band_stride;  /* doubles between bands' wx triples; 0 = shared */
+  int32_t device;          /* CUDA ordinal; -1 = the calling thread's one   */
+  int32_t flags;           /* BGW_FLAG_*                                    */
+  void *stream;            /* cudaStream_t; NULL = legacy default stream    */
+  int32_t *device_status;  /* device int written with BGW_FLAG_ASYNC        */
+} bgw_options;
+
+/* Fills *opt with the defaults (host memory, FP64, BANDLOOP, stride 0,
+ * current device, default stream, synchronous). */
+void bgw_options_init(bgw_options *opt);
+
+/* ------------------------------------------------------------------ GPP --
+ * Replaces noflagOCC_solver (GPP/gpp.cpp:307-402; prototype
+ * common/Defines.h:50-62).  Same argument order and meaning:
+ *   inv_igp_index [ngpown], indinv [indinv_len] (the reference allocates
+ *   ncouls + 1, GPP/gpp.cpp:235), wx_array [3] (or [number_bands][stride]
+ *   with opt->wx_band_stride), wtilde_array / I_eps_array complex
+ *   [ngpown][ncouls], aqsmtemp / aqsntemp complex [number_bands][ncouls],
+ *   vcoul [ncouls]; output achtemp complex [3].
+ * achtemp[iw] = sum_{n1, my_igp, ig} sch_store1(n1, my_igp) *
+ *               conj(wdiff) / |wdiff|^2 * I_eps[my_igp][ig],
+ *   wdiff = wx[iw] - wtilde[my_igp][ig],  igp = indinv[inv_igp_index[my_igp]],
+ *   sch_store1 = conj(aqsm[n1][igp]) aqsn[n1][igp] 0.5 vcoul[igp]
+ *                wtilde[my_igp][igp].
+ * Precision FP64: within 1e-12 relative of the reference's OpenMP build.
+ * Precision MIXED: per-term quotients in FP32, compensated FP64
+ * accumulation. */
+int bgw_noflagOCC_solver(int64_t number_bands, int64_t ngpown, int64_t ncouls,
+                         const int32_t *inv_igp_index, const int32_t *indinv,
+                         int64_t indinv_len, const double *wx_array,
+                         const double *wtilde_array, const double *aqsmtemp,
+                         const double *aqsntemp, const double *I_eps_array,
+                         const double *vcoul, double *achtemp,
+                         const bgw_options *opt);
+
+/* ------------------------------------------------------------------- FF --
+ * Replaces achsDtemp_Kernel (FF/ff.cpp:171-209).  Note the reference order
+ * aqsntemp before aqsmtemp.  I_epsR_array complex [nFreq][ngpown][ncouls]
+ * (only frequency 1 is read, ff.cpp:200); indinv [indinv_len] (ncouls in
+ * the FF driver, ff.cpp:552); achsDtemp: 1 complex. */
+int bgw_achsDtemp_Kernel(int64_t number_bands, int64_t ngpown, int64_t ncouls,
+                         const int32_t *inv_igp_index, const int32_t *indinv,
+                         int64_t indinv_len, const double *aqsntemp,
+                         const double *aqsmtemp, const double *I_epsR_array,
+                         int64_t nFreq, const double *vcoul, double *achsDtemp,
+                         const bgw_options *opt);
+
+/* Replaces asxDtemp_Kernel (FF/ff.cpp:211-293).  ekq [number_bands] (only
+ * the first nvband entries are read), dFreqGrid [nFreq], I_epsR_array /
+ * I_epsA_array complex [nFreq][ngpown][ncouls], aqsm/aqsn complex
+ * [number_bands][ncouls]; asxDtemp: nfreqeval complex.  number_bands is the
+ * row extent of aqsm/aqsn/ekq (the reference takes it from the ArrayMDs). */
+int bgw_asxDtemp_Kernel(int64_t nvband, int64_t nfreqeval, int64_t ncouls,
+                        int64_t ngpown, int64_t nFreq, double freqevalmin,
+                        double freqevalstep, double occ, const double *ekq,
+                        const double *dFreqGrid, const int32_t *inv_igp_index,
+                        const int32_t *indinv, int64_t indinv_len,
+                        const double *aqsmtemp, const double *aqsntemp,
+                        int64_t number_bands, const double *vcoul,
+                        const double *I_epsR_array, const double *I_epsA_array,
+                        double *asxDtemp, const bgw_options *opt);
+
+/* Replaces achDtemp_cor_Kernel (FF/ff.cpp:295-379, with
+ * schDttt_corKernel1/2 :381-451); achDtemp_cor: nfreqeval complex.
+ * flag_occ is evaluated per band (n1 < nvband), the intended meaning of the
+ * reference's shared variable (ff.cpp:310, 334). */
+int bgw_achDtemp_cor_Kernel(int64_t number_bands, int64_t nvband,
+                            int64_t nfreqeval, int64_t ncouls, int64_t ngpown,
+                            int64_t nFreq, double freqevalmin,
+                            double freqevalstep, const double *ekq,
+                            const double *dFreqGrid,
+                            const int32_t *inv_igp_index,
+                            const int32_t *indinv, int64_t indinv_len,
+                            const double *aqsmtemp, const double *aqsntemp,
+                            const double *vcoul, const double *I_epsR_array,
+                            const double *I_epsA_array, double *achDtemp_cor,
+                            const bgw_options *opt);
+
+/* The three FF sums of one driver run (FF/ff.cpp:697-733) in one call that
+ * stages each input once and launches one contraction over all three.
+ * Outputs as the three entry points above; any output pointer may be NULL
+ * to skip that sum. */
+int bgw_ff_sigma(int64_t number_bands, int64_t nvband, int64_t nfreqeval,
+                 int64_t ncouls, int64_t ngpown, int64_t nFreq,
+                 double freqevalmin, double freqevalstep, double occ,
+                 const double *ekq, const double *dFreqGrid,
+                 const int32_t *inv_igp_index, const int32_t *indinv,
+                 int64_t indinv_len, const double *aqsmtemp,
+                 const double *aqsntemp, const double *vcoul,
+                 const double *I_epsR_array, const double *I_epsA_array,
+                 double *achsDtemp, double *asxDtemp, double *achDtemp_cor,
+                 const bgw_options *opt);
+
+/* ------------------------------------------------------------- profiling --
+ * Filled by a synchronous call made with BGW_FLAG_PROFILE; per thread. */
+typedef struct bgw_profile {
+  double main_kernel_ms; /* dominant kernel: GPP band loop / factored stream,
+                            FF contraction (CUDA events on the call's stream) */
+  double device_ms;      /* everything the call enqueued, staging included   */
+  double flops;          /* algorithmic flops of the call (GPP: 63 per
+                            (band, G', G) triple, i.e. 21 per frequency;
+                            FF: 8 per complex multiply-add of the useful
+                            contraction rows)                                */
+  double main_bytes;     /* compulsory HBM bytes of the dominant kernel      */
+  int32_t main_launches; /* launches of the dominant kernel                  */
+  int32_t total_launches;/* kernel launches of the call                      */
+  char main_kernel[48];  /* name of the dominant kernel                      */
+} bgw_profile;
+int bgw_last_profile(bgw_profile *out);
+
+/* --------------------------------------------------------------- utility */
+const char *bgw_status_string(int status);
+int bgw_abi_version(void);
+/* Number of kernel launches the library issued on this process so far (all
+ * devices).  Lets a caller count launches inside a timed region. */
+uint64_t bgw_launch_count(void);
+/* Times FP64 DFMA and DMMA (mma.sync m8n8k4 f64) throughput microkernels on
+ * `device` and returns TFLOP/s (2 flops per FMA).  Used as the measured
+ * FP64 roofline denominators. */
+int bgw_measure_fp64_peak(int32_t device, double *dfma_tflops,
+                          double *dmma_tflops);
+/* Releases the library's cached device workspace on `device` (-1: all). */
+int bgw_release_workspace(int32_t device);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BGW_SIGMA_H */

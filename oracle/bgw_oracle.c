@@ -1,0 +1,408 @@
+/*
+ * bgw_oracle.c -- CPU oracle for the GPP and full-frequency self-energy sums.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker, never the product:
+ * only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg may
+ * load the library built from it.  The product path (libbgwsigma.so) never
+ * links or calls anything here.
+ *
+ * It restates, in long double (x87 80-bit) arithmetic, the algorithms of the
+ * reference mini-apps (rgayatri23/BerkeleyGW-Kernels-CPP):
+ *   - GPP  noflagOCC_solver             GPP/gpp.cpp:307-402
+ *   - FF   compute_fact                 FF/ff.cpp:103-152
+ *   - FF   achsDtemp_Kernel             FF/ff.cpp:171-209
+ *   - FF   asxDtemp_Kernel (+ssxDittt)  FF/ff.cpp:154-169, 211-293
+ *   - FF   achDtemp_cor_Kernel (+schDttt_corKernel1/2)  FF/ff.cpp:295-451
+ *
+ * Every sum is accumulated in long double and combined in a fixed order, so
+ * the result does not depend on the OpenMP thread count.  The oracle is
+ * pinned (i) against closed-form known answers of the reference's own uniform
+ * fills and (ii) against the reference sources compiled unmodified into
+ * oracle/_ref/libbgwref.so (see oracle/Makefile and tests/golden/).
+ *
+ * Complex arrays are interleaved (re, im) doubles, row-major with the last
+ * index fastest, exactly the memory image of ArrayMD<std::complex<double>>
+ * (arrayMD/arrayMD.h:156-184).
+ *
+ * All functions return 0 on success and -1 on an out-of-range size or index,
+ * without touching memory outside the stated extents.
+ */
+#include <stddef.h>
+#include <stdint.h>
+#include <stdlib.h>
+
+typedef long double ld;
+
+/* Resolve igp = indinv[inv_igp_index[p]] with bounds checks (gpp.cpp:362-363,
+ * ff.cpp:183-184).  Returns -1 if an index is out of range. */
+static int resolve_igp(long P, long G, const int *inv_igp_index,
+                       const int *indinv, long indinv_len, long *igp_out) {
+  for (long p = 0; p < P; ++p) {
+    int a = inv_igp_index[p];
+    if (a < 0 || (long)a >= indinv_len) return -1;
+    int b = indinv[a];
+    if (b < 0 || (long)b >= G) return -1;
+    igp_out[p] = b;
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------------------ GPP -- */
+
+/* sch_store1 of gpp.cpp:369-371:
+ *   conj(aqsm[n1][igp]) * aqsn[n1][igp] * 0.5 * vcoul[igp] * wtilde[p][igp] */
+static void gpp_store1(const double *am, const double *an, double vc,
+                       const double *wt, ld *sr, ld *si) {
+  ld ar = am[0], ai = -(ld)am[1];       /* conj(aqsm) */
+  ld br = an[0], bi = an[1];
+  ld r = ar * br - ai * bi, i = ar * bi + ai * br;
+  r *= 0.5L; i *= 0.5L;
+  r *= (ld)vc; i *= (ld)vc;
+  ld cr = wt[0], ci = wt[1];
+  *sr = r * cr - i * ci;
+  *si = r * ci + i * cr;
+}
+
+/* One (my_igp, ig, iw) quotient of gpp.cpp:374-380 without sch_store1:
+ *   conj(wdiff) / |wdiff|^2 * I_eps,  wdiff = wx - wtilde. */
+static void gpp_quot(double wx, const double *wt, const double *ie, ld *qr,
+                     ld *qi) {
+  ld dr = (ld)wx - (ld)wt[0];
+  ld di = -(ld)wt[1];
+  ld rcp = 1.0L / (dr * dr + di * di);
+  ld cr = dr * rcp, ci = -di * rcp;      /* conj(wdiff) * rcp */
+  ld er = ie[0], ei = ie[1];
+  *qr = cr * er - ci * ei;
+  *qi = cr * ei + ci * er;
+}
+
+/* Direct restatement of the n1 x my_igp x ig x iw loop of gpp.cpp:343-390.
+ * wx is read as wx[n1 * wx_band_stride + iw]; stride 0 is the reference
+ * (wx_array has no band index, gpp.cpp:239).  achtemp receives 3 complex
+ * values (6 doubles).  Cost O(nb * P * G * 3): small sizes only. */
+int orc_gpp_direct(long nb, long P, long G, const int *inv_igp_index,
+                   const int *indinv, long indinv_len, const double *wx,
+                   long wx_band_stride, const double *wtilde,
+                   const double *aqsm, const double *aqsn,
+                   const double *I_eps, const double *vcoul,
+                   double *achtemp) {
+  if (nb < 0 || P < 0 || G <= 0 || wx_band_stride < 0) return -1;
+  long *igp = (long *)malloc(sizeof(long) * (size_t)(P > 0 ? P : 1));
+  ld *part = (ld *)calloc((size_t)(nb > 0 ? nb : 1) * 6, sizeof(ld));
+  if (!igp || !part) { free(igp); free(part); return -1; }
+  if (resolve_igp(P, G, inv_igp_index, indinv, indinv_len, igp)) {
+    free(igp); free(part); return -1;
+  }
+#pragma omp parallel for schedule(dynamic, 1)
+  for (long n1 = 0; n1 < nb; ++n1) {
+    ld acc[6] = {0, 0, 0, 0, 0, 0};
+    for (long p = 0; p < P; ++p) {
+      long g = igp[p];
+      ld sr, si;
+      gpp_store1(aqsm + 2 * (n1 * G + g), aqsn + 2 * (n1 * G + g), vcoul[g],
+                 wtilde + 2 * (p * G + g), &sr, &si);
+      for (long ig = 0; ig < G; ++ig) {
+        const double *wt = wtilde + 2 * (p * G + ig);
+        const double *ie = I_eps + 2 * (p * G + ig);
+        for (int iw = 0; iw < 3; ++iw) {
+          ld qr, qi;
+          gpp_quot(wx[n1 * wx_band_stride + iw], wt, ie, &qr, &qi);
+          acc[2 * iw] += qr * sr - qi * si;
+          acc[2 * iw + 1] += qr * si + qi * sr;
+        }
+      }
+    }
+    for (int k = 0; k < 6; ++k) part[6 * n1 + k] = acc[k];
+  }
+  ld tot[6] = {0, 0, 0, 0, 0, 0};
+  for (long n1 = 0; n1 < nb; ++n1)
+    for (int k = 0; k < 6; ++k) tot[k] += part[6 * n1 + k];
+  for (int k = 0; k < 6; ++k) achtemp[k] = (double)tot[k];
+  free(igp); free(part);
+  return 0;
+}
+
+/* Factored evaluation of the same sum for a band-independent wx (the
+ * reference's case): nothing inside the ig/iw loop of gpp.cpp:373-390 depends
+ * on n1 except sch_store1, so
+ *   achtemp[iw] = sum_p S(p) * T(p, iw),
+ *   S(p) = sum_n1 sch_store1(n1, p),  T(p, iw) = sum_ig quot(p, ig, iw).
+ * This is an exact algebraic identity; only rounding differs, and long double
+ * keeps that far below the 1e-12 parity bar.  Cost O(P * G * 3 + nb * P), so
+ * it serves as the oracle at the full benchmark sizes. */
+int orc_gpp_factored(long nb, long P, long G, const int *inv_igp_index,
+                     const int *indinv, long indinv_len, const double *wx,
+                     const double *wtilde, const double *aqsm,
+                     const double *aqsn, const double *I_eps,
+                     const double *vcoul, double *achtemp) {
+  if (nb < 0 || P < 0 || G <= 0) return -1;
+  long *igp = (long *)malloc(sizeof(long) * (size_t)(P > 0 ? P : 1));
+  ld *part = (ld *)calloc((size_t)(P > 0 ? P : 1) * 6, sizeof(ld));
+  if (!igp || !part) { free(igp); free(part); return -1; }
+  if (resolve_igp(P, G, inv_igp_index, indinv, indinv_len, igp)) {
+    free(igp); free(part); return -1;
+  }
+#pragma omp parallel for schedule(dynamic, 4)
+  for (long p = 0; p < P; ++p) {
+    long g = igp[p];
+    ld Sr = 0, Si = 0;
+    for (long n1 = 0; n1 < nb; ++n1) {
+      ld sr, si;
+      gpp_store1(aqsm + 2 * (n1 * G + g), aqsn + 2 * (n1 * G + g), vcoul[g],
+                 wtilde + 2 * (p * G + g), &sr, &si);
+      Sr += sr; Si += si;
+    }
+    ld T[6] = {0, 0, 0, 0, 0, 0};
+    for (long ig = 0; ig < G; ++ig) {
+      const double *wt = wtilde + 2 * (p * G + ig);
+      const double *ie = I_eps + 2 * (p * G + ig);
+      for (int iw = 0; iw < 3; ++iw) {
+        ld qr, qi;
+        gpp_quot(wx[iw], wt, ie, &qr, &qi);
+        T[2 * iw] += qr;
+        T[2 * iw + 1] += qi;
+      }
+    }
+    for (int iw = 0; iw < 3; ++iw) {
+      part[6 * p + 2 * iw] = T[2 * iw] * Sr - T[2 * iw + 1] * Si;
+      part[6 * p + 2 * iw + 1] = T[2 * iw] * Si + T[2 * iw + 1] * Sr;
+    }
+  }
+  ld tot[6] = {0, 0, 0, 0, 0, 0};
+  for (long p = 0; p < P; ++p)
+    for (int k = 0; k < 6; ++k) tot[k] += part[6 * p + k];
+  for (int k = 0; k < 6; ++k) achtemp[k] = (double)tot[k];
+  free(igp); free(part);
+  return 0;
+}
+
+/* ------------------------------------------------------------------- FF -- */
+
+/* Last interval j (0 <= j < nFreq-1) with grid[j] < x < grid[j+1], or `init`
+ * if none: the linear search of ff.cpp:107-110 (strict inequalities, the
+ * last match wins). */
+static int last_bracket(double x, int nFreq, const double *grid, int init) {
+  int ifreq = init;
+  for (int j = 0; j < nFreq - 1; ++j)
+    if (x > grid[j] && x < grid[j + 1]) ifreq = j;
+  return ifreq;
+}
+
+/* compute_fact of ff.cpp:103-152 with its quirks kept bit-for-bit:
+ *   loop 1 (SX): a found ifreq == 0 is overwritten with nFreq-2 (:111, :121);
+ *   loop 2 (COR), wx > 0: the `ifreq == -1` test can never fire (:133), and
+ *     both weights carry a -0.5 factor (:135-138);
+ *   loop 2, wx <= 0, occupied: search on -wx, 0 -> nFreq-2 (:146-147);
+ *   loop 2, wx <= 0, unoccupied: outputs untouched (ifreq 0, facts 0).
+ * *ifreq, *f1, *f2 must hold the caller's initial values (0, 0, 0 in both
+ * reference callers, ff.cpp:249-250, 339-340). */
+void orc_compute_fact(double wx, int nFreq, const double *g, int loop,
+                      int flag_occ, int *ifreq, double *f1, double *f2) {
+  if (loop == 1 && wx > 0.0) {
+    int i = last_bracket(wx, nFreq, g, *ifreq);
+    if (i == 0) i = nFreq - 2;
+    *f1 = (g[i + 1] - wx) / (g[i + 1] - g[i]);
+    *f2 = (wx - g[i]) / (g[i + 1] - g[i]);
+    *ifreq = i;
+  } else if (loop == 1) {
+    int i = last_bracket(-wx, nFreq, g, *ifreq);
+    if (i == 0) i = nFreq - 2;
+    *f1 = (g[i + 1] + wx) / (g[i + 1] - g[i]);
+    *f2 = (-g[i] - wx) / (g[i + 1] - g[i]);
+    *ifreq = i;
+  }
+  if (loop == 2 && wx > 0.0) {
+    int i = last_bracket(wx, nFreq, g, *ifreq);
+    if (i == -1) i = nFreq - 2;
+    *f1 = -0.5 * (g[i + 1] - wx) / (g[i + 1] - g[i]);
+    *f2 = -0.5 * (wx - g[i]) / (g[i + 1] - g[i]);
+    *ifreq = i;
+  } else if (loop == 2 && flag_occ) {
+    double x = -wx;
+    int i = last_bracket(x, nFreq, g, 0);
+    if (i == 0) i = nFreq - 2;
+    *f1 = (g[i + 1] - x) / (g[i + 1] - g[i]);
+    *f2 = (x - g[i]) / (g[i + 1] - g[i]);
+    *ifreq = i;
+  }
+}
+
+static int ff_check(long nb, long P, long G, long nFreq) {
+  return (nb < 0 || P < 0 || G <= 0 || P > G || nFreq < 2) ? -1 : 0;
+}
+
+/* achsDtemp_Kernel, ff.cpp:171-209:
+ *   achsDtemp = sum_{n1<nb, p} 0.5 vcoul[igp] *
+ *               ( - sum_ig aqsn[n1][ig] conj(aqsm[n1][igp]) I_epsR[1][p][ig] )
+ * conj(aqsm[n1][igp]) does not depend on ig and is factored out of the ig sum
+ * (exact algebra).  out = 1 complex (2 doubles). */
+int orc_ff_achs(long nb, long P, long G, long nFreq, const int *inv_igp_index,
+                const int *indinv, long indinv_len, const double *aqsn,
+                const double *aqsm, const double *I_epsR, const double *vcoul,
+                double *out) {
+  if (ff_check(nb, P, G, nFreq)) return -1;
+  long *igp = (long *)malloc(sizeof(long) * (size_t)(P > 0 ? P : 1));
+  ld *part = (ld *)calloc((size_t)(nb > 0 ? nb : 1) * 2, sizeof(ld));
+  if (!igp || !part) { free(igp); free(part); return -1; }
+  if (resolve_igp(P, G, inv_igp_index, indinv, indinv_len, igp)) {
+    free(igp); free(part); return -1;
+  }
+  const double *R1 = I_epsR + 2 * (1 * P * G);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (long n1 = 0; n1 < nb; ++n1) {
+    ld accr = 0, acci = 0;
+    const double *a = aqsn + 2 * n1 * G;
+    for (long p = 0; p < P; ++p) {
+      const double *r = R1 + 2 * p * G;
+      ld cr = 0, ci = 0;
+      for (long ig = 0; ig < G; ++ig) {
+        ld ar = a[2 * ig], ai = a[2 * ig + 1];
+        ld br = r[2 * ig], bi = r[2 * ig + 1];
+        cr += ar * br - ai * bi;
+        ci += ar * bi + ai * br;
+      }
+      long g = igp[p];
+      ld mr = aqsm[2 * (n1 * G + g)], mi = -(ld)aqsm[2 * (n1 * G + g) + 1];
+      ld sr = cr * mr - ci * mi, si = cr * mi + ci * mr;
+      ld v = (ld)vcoul[g] * 0.5L;
+      accr += -sr * v;
+      acci += -si * v;
+    }
+    part[2 * n1] = accr;
+    part[2 * n1 + 1] = acci;
+  }
+  ld tr = 0, ti = 0;
+  for (long n1 = 0; n1 < nb; ++n1) { tr += part[2 * n1]; ti += part[2 * n1 + 1]; }
+  out[0] = (double)tr;
+  out[1] = (double)ti;
+  free(igp); free(part);
+  return 0;
+}
+
+/* sum_{p, ig} aqsn[n1][ig] * W(n1, p) * (X[i][p][ig] * c1 + X[i+1][p][ig] * c2)
+ * with W(n1, p) = conj(aqsm[n1][igp]) * vcoul[igp] and X = R - A (sub = 1)
+ * or X = E (sub = 0, B ignored).  Shared by the SX and COR restatements. */
+static void ff_band_sum(long n1, long P, long G, const long *igp,
+                        const double *aqsn, const double *aqsm,
+                        const double *vcoul, const double *E,
+                        const double *B, int sub, int i, ld c1, ld c2,
+                        ld *out_r, ld *out_i) {
+  const double *a = aqsn + 2 * n1 * G;
+  ld accr = 0, acci = 0;
+  for (long p = 0; p < P; ++p) {
+    const double *x0 = E + 2 * (((long)i * P + p) * G);
+    const double *x1 = E + 2 * (((long)(i + 1) * P + p) * G);
+    const double *y0 = sub ? B + 2 * (((long)i * P + p) * G) : NULL;
+    const double *y1 = sub ? B + 2 * (((long)(i + 1) * P + p) * G) : NULL;
+    ld cr = 0, ci = 0;
+    for (long ig = 0; ig < G; ++ig) {
+      ld u0r = x0[2 * ig], u0i = x0[2 * ig + 1];
+      ld u1r = x1[2 * ig], u1i = x1[2 * ig + 1];
+      if (sub) {
+        u0r -= y0[2 * ig]; u0i -= y0[2 * ig + 1];
+        u1r -= y1[2 * ig]; u1i -= y1[2 * ig + 1];
+      }
+      ld xr = u0r * c1 + u1r * c2, xi = u0i * c1 + u1i * c2;
+      ld ar = a[2 * ig], ai = a[2 * ig + 1];
+      cr += ar * xr - ai * xi;
+      ci += ar * xi + ai * xr;
+    }
+    long g = igp[p];
+    ld mr = aqsm[2 * (n1 * G + g)], mi = -(ld)aqsm[2 * (n1 * G + g) + 1];
+    ld v = vcoul[g];
+    mr *= v; mi *= v;
+    accr += cr * mr - ci * mi;
+    acci += cr * mi + ci * mr;
+  }
+  *out_r = accr;
+  *out_i = acci;
+}
+
+/* asxDtemp_Kernel + ssxDittt_kernel, ff.cpp:154-169, 211-293.  For n1 <
+ * nvband: wx = freqevalmin - ekq[n1] + freqevalstep (no iw term, :245),
+ * compute_fact(loop 1), X = I_epsR if wx > 0 else I_epsA (:254-261), times
+ * occ.  Every asxDtemp[iw] receives the same sum; out has nfreqeval complex
+ * values. */
+int orc_ff_asx(long nvband, long nfreqeval, long G, long P, long nFreq,
+               double freqevalmin, double freqevalstep, double occ,
+               const double *ekq, const double *dFreqGrid,
+               const int *inv_igp_index, const int *indinv, long indinv_len,
+               const double *aqsm, const double *aqsn, const double *vcoul,
+               const double *I_epsR, const double *I_epsA, double *out) {
+  if (ff_check(nvband, P, G, nFreq) || nfreqeval < 0) return -1;
+  long *igp = (long *)malloc(sizeof(long) * (size_t)(P > 0 ? P : 1));
+  ld *part = (ld *)calloc((size_t)(nvband > 0 ? nvband : 1) * 2, sizeof(ld));
+  if (!igp || !part) { free(igp); free(part); return -1; }
+  if (resolve_igp(P, G, inv_igp_index, indinv, indinv_len, igp)) {
+    free(igp); free(part); return -1;
+  }
+#pragma omp parallel for schedule(dynamic, 1)
+  for (long n1 = 0; n1 < nvband; ++n1) {
+    double wx = freqevalmin - ekq[n1] + freqevalstep;
+    int ifreq = 0;
+    double f1 = 0, f2 = 0;
+    orc_compute_fact(wx, (int)nFreq, dFreqGrid, 1, 0, &ifreq, &f1, &f2);
+    ld r, i;
+    ff_band_sum(n1, P, G, igp, aqsn, aqsm, vcoul, wx > 0 ? I_epsR : I_epsA,
+                NULL, 0, ifreq, f1, f2, &r, &i);
+    part[2 * n1] = r * (ld)occ;
+    part[2 * n1 + 1] = i * (ld)occ;
+  }
+  ld tr = 0, ti = 0;
+  for (long n1 = 0; n1 < nvband; ++n1) { tr += part[2 * n1]; ti += part[2 * n1 + 1]; }
+  for (long iw = 0; iw < nfreqeval; ++iw) {
+    out[2 * iw] = (double)tr;
+    out[2 * iw + 1] = (double)ti;
+  }
+  free(igp); free(part);
+  return 0;
+}
+
+/* achDtemp_cor_Kernel + schDttt_corKernel1/2, ff.cpp:295-451.  For every
+ * band: flag_occ = n1 < nvband (the intended per-iteration value; the
+ * reference shares the variable across OpenMP threads, :310), wx as in SX,
+ * compute_fact(loop 2).  wx > 0 and unoccupied -> Kernel1 with (f1, f2);
+ * wx <= 0 and occupied -> Kernel2 with an extra -0.5 (:437-444); otherwise
+ * nothing.  X = I_epsR - I_epsA.  Every achDtemp_cor[iw] receives the same
+ * sum. */
+int orc_ff_cor(long nb, long nvband, long nfreqeval, long G, long P,
+               long nFreq, double freqevalmin, double freqevalstep,
+               const double *ekq, const double *dFreqGrid,
+               const int *inv_igp_index, const int *indinv, long indinv_len,
+               const double *aqsm, const double *aqsn, const double *vcoul,
+               const double *I_epsR, const double *I_epsA, double *out) {
+  if (ff_check(nb, P, G, nFreq) || nfreqeval < 0 || nvband < 0) return -1;
+  long *igp = (long *)malloc(sizeof(long) * (size_t)(P > 0 ? P : 1));
+  ld *part = (ld *)calloc((size_t)(nb > 0 ? nb : 1) * 2, sizeof(ld));
+  if (!igp || !part) { free(igp); free(part); return -1; }
+  if (resolve_igp(P, G, inv_igp_index, indinv, indinv_len, igp)) {
+    free(igp); free(part); return -1;
+  }
+#pragma omp parallel for schedule(dynamic, 1)
+  for (long n1 = 0; n1 < nb; ++n1) {
+    int occ = n1 < nvband;
+    double wx = freqevalmin - ekq[n1] + freqevalstep;
+    int ifreq = 0;
+    double f1 = 0, f2 = 0;
+    orc_compute_fact(wx, (int)nFreq, dFreqGrid, 2, occ, &ifreq, &f1, &f2);
+    ld r = 0, i = 0;
+    if (wx > 0) {
+      if (!occ)
+        ff_band_sum(n1, P, G, igp, aqsn, aqsm, vcoul, I_epsR, I_epsA, 1,
+                    ifreq, f1, f2, &r, &i);
+    } else if (occ) {
+      ff_band_sum(n1, P, G, igp, aqsn, aqsm, vcoul, I_epsR, I_epsA, 1, ifreq,
+                  -0.5L * f1, -0.5L * f2, &r, &i);
+    }
+    part[2 * n1] = r;
+    part[2 * n1 + 1] = i;
+  }
+  ld tr = 0, ti = 0;
+  for (long n1 = 0; n1 < nb; ++n1) { tr += part[2 * n1]; ti += part[2 * n1 + 1]; }
+  for (long iw = 0; iw < nfreqeval; ++iw) {
+    out[2 * iw] = (double)tr;
+    out[2 * iw + 1] = (double)ti;
+  }
+  free(igp); free(part);
+  return 0;
+}

@@ -1,0 +1,166 @@
+"""ctypes loaders of the CPU checkers (TEST INFRASTRUCTURE ONLY).
+
+  Oracle      oracle/_build/liboracle.so -- long-double restatement
+              (bgw_oracle.c) of the reference algorithms
+  Reference   oracle/_ref/libbgwref.so   -- the reference's own GPP/FF kernels
+              compiled unmodified (oracle/Makefile target `ref`); present
+              only where it was built
+
+Only tests/, __graft_entry__.smoke() and bench.py (cpu_baseline leg and the
+reference arm) may import this module; the product never does.
+Both take the arrays of bgwsigma.inputs.GppInputs / FFInputs (host numpy).
+"""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_LIB = HERE / "_build" / "liboracle.so"
+REF_LIB = HERE / "_ref" / "libbgwref.so"
+REF_SRC = Path("/root/reference")
+
+_P = ctypes.c_void_p
+_L = ctypes.c_long
+_D = ctypes.c_double
+
+
+def build_oracle(ref: bool | None = None) -> None:
+    """Builds liboracle.so, and libbgwref.so when the reference tree exists."""
+    subprocess.run(["make", "-s", "-C", str(HERE), "oracle"], check=True)
+    if ref is None:
+        ref = (REF_SRC / "GPP" / "gpp.cpp").exists()
+    if ref:
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+
+
+def _p(a) -> int:
+    assert isinstance(a, np.ndarray) and a.flags.c_contiguous, "host C-contiguous numpy array required"
+    return a.ctypes.data
+
+
+class Oracle:
+    """Long-double CPU restatement of the reference (bgw_oracle.c)."""
+
+    def __init__(self, path: Path = ORACLE_LIB):
+        if not path.exists():
+            build_oracle(ref=False)
+        lib = ctypes.CDLL(str(path))
+        lib.orc_gpp_direct.argtypes = [_L, _L, _L, _P, _P, _L, _P, _L, _P, _P, _P, _P, _P, _P]
+        lib.orc_gpp_factored.argtypes = [_L, _L, _L, _P, _P, _L, _P, _P, _P, _P, _P, _P, _P]
+        lib.orc_compute_fact.argtypes = [_D, ctypes.c_int, _P, ctypes.c_int, ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_int), ctypes.POINTER(_D), ctypes.POINTER(_D)]
+        lib.orc_compute_fact.restype = None
+        lib.orc_ff_achs.argtypes = [_L, _L, _L, _L, _P, _P, _L, _P, _P, _P, _P, _P]
+        lib.orc_ff_asx.argtypes = [_L, _L, _L, _L, _L, _D, _D, _D, _P, _P, _P, _P, _L, _P, _P, _P, _P, _P, _P]
+        lib.orc_ff_cor.argtypes = [_L, _L, _L, _L, _L, _L, _D, _D, _P, _P, _P, _P, _L, _P, _P, _P, _P, _P, _P]
+        self.lib = lib
+
+    def gpp(self, g, factored: bool = False) -> np.ndarray:
+        out = np.zeros(3, dtype=np.complex128)
+        if factored:
+            assert g.wx_band_stride == 0
+            st = self.lib.orc_gpp_factored(g.number_bands, g.ngpown, g.ncouls, _p(g.inv_igp_index), _p(g.indinv),
+                                           len(g.indinv), _p(g.wx_array), _p(g.wtilde_array), _p(g.aqsmtemp),
+                                           _p(g.aqsntemp), _p(g.I_eps_array), _p(g.vcoul), _p(out))
+        else:
+            st = self.lib.orc_gpp_direct(g.number_bands, g.ngpown, g.ncouls, _p(g.inv_igp_index), _p(g.indinv),
+                                         len(g.indinv), _p(g.wx_array), g.wx_band_stride, _p(g.wtilde_array),
+                                         _p(g.aqsmtemp), _p(g.aqsntemp), _p(g.I_eps_array), _p(g.vcoul), _p(out))
+        if st != 0:
+            raise ValueError("oracle rejected the GPP inputs")
+        return out
+
+    def compute_fact(self, wx: float, grid: np.ndarray, loop: int, flag_occ: bool):
+        i, f1, f2 = ctypes.c_int(0), _D(0.0), _D(0.0)
+        self.lib.orc_compute_fact(wx, len(grid), _p(grid), loop, int(flag_occ), ctypes.byref(i), ctypes.byref(f1),
+                                  ctypes.byref(f2))
+        return i.value, f1.value, f2.value
+
+    def achs(self, f) -> complex:
+        out = np.zeros(1, dtype=np.complex128)
+        st = self.lib.orc_ff_achs(f.number_bands, f.ngpown, f.ncouls, f.nFreq, _p(f.inv_igp_index), _p(f.indinv),
+                                  len(f.indinv), _p(f.aqsntemp), _p(f.aqsmtemp), _p(f.I_epsR_array), _p(f.vcoul),
+                                  _p(out))
+        if st != 0:
+            raise ValueError("oracle rejected the FF inputs")
+        return complex(out[0])
+
+    def asx(self, f) -> np.ndarray:
+        out = np.zeros(max(f.nfreqeval, 1), dtype=np.complex128)
+        st = self.lib.orc_ff_asx(f.nvband, f.nfreqeval, f.ncouls, f.ngpown, f.nFreq, f.freqevalmin, f.freqevalstep,
+                                 f.occ, _p(f.ekq), _p(f.dFreqGrid), _p(f.inv_igp_index), _p(f.indinv),
+                                 len(f.indinv), _p(f.aqsmtemp), _p(f.aqsntemp), _p(f.vcoul), _p(f.I_epsR_array),
+                                 _p(f.I_epsA_array), _p(out))
+        if st != 0:
+            raise ValueError("oracle rejected the FF inputs")
+        return out[:f.nfreqeval]
+
+    def cor(self, f) -> np.ndarray:
+        out = np.zeros(max(f.nfreqeval, 1), dtype=np.complex128)
+        st = self.lib.orc_ff_cor(f.number_bands, f.nvband, f.nfreqeval, f.ncouls, f.ngpown, f.nFreq, f.freqevalmin,
+                                 f.freqevalstep, _p(f.ekq), _p(f.dFreqGrid), _p(f.inv_igp_index), _p(f.indinv),
+                                 len(f.indinv), _p(f.aqsmtemp), _p(f.aqsntemp), _p(f.vcoul), _p(f.I_epsR_array),
+                                 _p(f.I_epsA_array), _p(out))
+        if st != 0:
+            raise ValueError("oracle rejected the FF inputs")
+        return out[:f.nfreqeval]
+
+
+class Reference:
+    """The reference's own kernels (compiled unmodified into libbgwref.so)."""
+
+    def __init__(self, path: Path = REF_LIB):
+        if not path.exists():
+            raise FileNotFoundError(f"{path} not built (needs the reference tree; make -C oracle ref)")
+        lib = ctypes.CDLL(str(path))
+        lib.ref_gpp_noflagocc.argtypes = [_L, _L, _L, _P, _P, _L, _P, _P, _P, _P, _P, _P, _P]
+        lib.ref_gpp_noflagocc.restype = None
+        lib.ref_ff_achs.argtypes = [_L, _L, _L, _L, _P, _P, _L, _P, _P, _P, _P, _P]
+        lib.ref_ff_achs.restype = None
+        lib.ref_ff_asx.argtypes = [_L, _L, _L, _L, _L, _D, _D, _D, _P, _L, _P, _P, _P, _L, _P, _P, _P, _P, _P, _P]
+        lib.ref_ff_asx.restype = None
+        lib.ref_ff_cor.argtypes = [_L, _L, _L, _L, _L, _L, _D, _D, _P, _P, _P, _P, _L, _P, _P, _P, _P, _P, _P]
+        lib.ref_ff_cor.restype = None
+        lib.ref_num_threads.restype = ctypes.c_int
+        self.lib = lib
+
+    @staticmethod
+    def available() -> bool:
+        return REF_LIB.exists()
+
+    def num_threads(self) -> int:
+        return int(self.lib.ref_num_threads())
+
+    def gpp(self, g) -> np.ndarray:
+        assert g.wx_band_stride == 0, "the reference has a band-independent wx_array"
+        out = np.zeros(3, dtype=np.complex128)
+        self.lib.ref_gpp_noflagocc(g.number_bands, g.ngpown, g.ncouls, _p(g.inv_igp_index), _p(g.indinv),
+                                   len(g.indinv), _p(g.wx_array), _p(g.wtilde_array), _p(g.aqsmtemp),
+                                   _p(g.aqsntemp), _p(g.I_eps_array), _p(g.vcoul), _p(out))
+        return out
+
+    def achs(self, f) -> complex:
+        out = np.zeros(1, dtype=np.complex128)
+        self.lib.ref_ff_achs(f.number_bands, f.ngpown, f.ncouls, f.nFreq, _p(f.inv_igp_index), _p(f.indinv),
+                             len(f.indinv), _p(f.aqsntemp), _p(f.aqsmtemp), _p(f.I_epsR_array), _p(f.vcoul), _p(out))
+        return complex(out[0])
+
+    def asx(self, f) -> np.ndarray:
+        out = np.zeros(max(f.nfreqeval, 1), dtype=np.complex128)
+        self.lib.ref_ff_asx(f.nvband, f.nfreqeval, f.ncouls, f.ngpown, f.nFreq, f.freqevalmin, f.freqevalstep, f.occ,
+                            _p(f.ekq), f.number_bands, _p(f.dFreqGrid), _p(f.inv_igp_index), _p(f.indinv),
+                            len(f.indinv), _p(f.aqsmtemp), _p(f.aqsntemp), _p(f.vcoul), _p(f.I_epsR_array),
+                            _p(f.I_epsA_array), _p(out))
+        return out[:f.nfreqeval]
+
+    def cor(self, f) -> np.ndarray:
+        out = np.zeros(max(f.nfreqeval, 1), dtype=np.complex128)
+        self.lib.ref_ff_cor(f.number_bands, f.nvband, f.nfreqeval, f.ncouls, f.ngpown, f.nFreq, f.freqevalmin,
+                            f.freqevalstep, _p(f.ekq), _p(f.dFreqGrid), _p(f.inv_igp_index), _p(f.indinv),
+                            len(f.indinv), _p(f.aqsmtemp), _p(f.aqsntemp), _p(f.vcoul), _p(f.I_epsR_array),
+                            _p(f.I_epsA_array), _p(out))
+        return out[:f.nfreqeval]

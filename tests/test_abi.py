@@ -1,0 +1,128 @@
+"""CPU: the C ABI library builds, loads and exports every symbol the header
+declares; the C++11 shim exports the reference's mangled kernel names; host
+argument validation rejects bad calls before any device work; without a GPU
+every compute entry point fails loudly (no CPU fallback)."""
+from __future__ import annotations
+
+import ctypes
+import re
+import subprocess
+
+import numpy as np
+import pytest
+from conftest import REPO
+
+from bgwsigma import inputs as I
+
+HEADER = REPO / "include" / "bgw_sigma.h"
+
+
+def header_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(bgw_\w+)\s*\(", text)))
+
+
+def exported(path):
+    out = subprocess.run(["nm", "-D", "--defined-only", str(path)], capture_output=True, text=True, check=True)
+    return {ln.split()[-1] for ln in out.stdout.splitlines() if ln.strip()}
+
+
+def test_header_declares_entry_points():
+    fns = header_functions()
+    for f in ("bgw_noflagOCC_solver", "bgw_achsDtemp_Kernel", "bgw_asxDtemp_Kernel", "bgw_achDtemp_cor_Kernel",
+              "bgw_ff_sigma"):
+        assert f in fns
+
+
+def test_library_exports_every_header_symbol(bgw):
+    syms = exported(bgw.lib_path())
+    missing = [f for f in header_functions() if f not in syms]
+    assert not missing, missing
+    lib = bgw.load()
+    for f in header_functions():
+        assert hasattr(lib, f)
+    assert set(bgw.EXPORTS) <= set(header_functions())
+
+
+def test_abi_version_and_status_strings(bgw):
+    lib = bgw.load()
+    assert lib.bgw_abi_version() == 1
+    for code in bgw.STATUS:
+        assert lib.bgw_status_string(code)
+    assert b"index" in lib.bgw_status_string(-2)
+
+
+def test_options_defaults(bgw):
+    o = bgw.Options()
+    bgw.load().bgw_options_init(ctypes.byref(o))
+    assert o.struct_size == ctypes.sizeof(bgw.Options)
+    assert (o.memory, o.precision, o.gpp_algorithm, o.wx_band_stride, o.device, o.flags) == (0, 0, 0, 0, -1, 0)
+
+
+def test_shim_exports_reference_mangled_names(bgw, golden):
+    from bgwsigma import build
+    syms = exported(build.SHIM_LIB)
+    for s in golden["reference_symbols"]:
+        assert s in syms, s
+
+
+def _gpp_call(bgw, g, **kw):
+    lib = bgw.load()
+    out = np.zeros(3, dtype=np.complex128)
+    o = bgw.make_options("host", **kw)
+    args = dict(nb=g.number_bands, P=g.ngpown, G=g.ncouls, indinv_len=len(g.indinv))
+    return lib.bgw_noflagOCC_solver(args["nb"], args["P"], args["G"], bgw._ptr(g.inv_igp_index), bgw._ptr(g.indinv),
+                                    args["indinv_len"], bgw._ptr(g.wx_array), bgw._ptr(g.wtilde_array),
+                                    bgw._ptr(g.aqsmtemp), bgw._ptr(g.aqsntemp), bgw._ptr(g.I_eps_array),
+                                    bgw._ptr(g.vcoul), bgw._ptr(out), ctypes.byref(o))
+
+
+def test_invalid_arguments_rejected_on_host(bgw):
+    lib = bgw.load()
+    g = I.gpp_seeded(2, 1, 40, 20)
+    o = bgw.make_options("host")
+    out = np.zeros(3, dtype=np.complex128)
+    p = bgw._ptr
+    # ncouls <= 0
+    assert lib.bgw_noflagOCC_solver(2, 2, 0, p(g.inv_igp_index), p(g.indinv), 41, p(g.wx_array),
+                                    p(g.wtilde_array), p(g.aqsmtemp), p(g.aqsntemp), p(g.I_eps_array),
+                                    p(g.vcoul), p(out), ctypes.byref(o)) == -1
+    # null output
+    assert lib.bgw_noflagOCC_solver(2, 2, 40, p(g.inv_igp_index), p(g.indinv), 41, p(g.wx_array),
+                                    p(g.wtilde_array), p(g.aqsmtemp), p(g.aqsntemp), p(g.I_eps_array),
+                                    p(g.vcoul), None, ctypes.byref(o)) == -1
+    # FF: ngpown > ncouls (the reference driver's own guard, FF/ff.cpp:492-499)
+    f = I.ff_seeded(4, 1, 16, 8, 3, 2)
+    res = np.zeros(1, dtype=np.complex128)
+    assert lib.bgw_achsDtemp_Kernel(4, 32, 16, p(f.inv_igp_index), p(f.indinv), 16, p(f.aqsntemp), p(f.aqsmtemp),
+                                    p(f.I_epsR_array), 3, p(f.vcoul), p(res), ctypes.byref(o)) == -1
+    # FF: fewer than 2 frequencies
+    assert lib.bgw_achsDtemp_Kernel(4, 8, 16, p(f.inv_igp_index), p(f.indinv), 16, p(f.aqsntemp), p(f.aqsmtemp),
+                                    p(f.I_epsR_array), 1, p(f.vcoul), p(res), ctypes.byref(o)) == -1
+
+
+def test_no_cpu_fallback_without_gpu(bgw):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    g = I.gpp_seeded(2, 1, 40, 20)
+    assert _gpp_call(bgw, g) == -5  # BGW_ERR_NO_DEVICE
+    with pytest.raises(bgw.BgwError):
+        bgw.noflagOCC_solver(g)
+    f = I.ff_seeded(4, 1, 16, 8, 3, 2)
+    with pytest.raises(bgw.BgwError):
+        bgw.ff_sigma(f)
+
+
+def test_dropin_drivers_link():
+    """The reference drivers (their own `main`) link against the shim."""
+    ref = REPO / "oracle" / "_ref"
+    exes = [ref / "gpp_dropin.ex", ref / "ff_dropin.ex"]
+    if not all(e.exists() for e in exes):
+        pytest.skip("drop-in drivers not built here (need the reference tree)")
+    for e in exes:
+        out = subprocess.run(["nm", str(e)], capture_output=True, text=True, check=True).stdout
+        # main calls the kernels through undefined (shim) symbols, and the
+        # weakened reference definitions are overridden.
+        assert "noflagOCC_solver" in out or "achsDtemp_Kernel" in out

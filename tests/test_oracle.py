@@ -1,0 +1,107 @@
+"""CPU: the oracle is pinned against the reference's own outputs (golden
+vectors made by tests/golden/make_golden.py from the reference build) and
+against closed-form known answers of the reference's uniform fills."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+from conftest import FP64_RTOL, l2c, rel_err
+
+from bgwsigma import inputs as I
+from cases import FF_CASES, GPP_CASES
+
+
+@pytest.mark.parametrize("name", sorted(GPP_CASES))
+def test_gpp_inputs_stable(golden, name):
+    assert I.fingerprint(GPP_CASES[name]()) == golden["gpp"][name]["fingerprint"]
+
+
+@pytest.mark.parametrize("name", sorted(FF_CASES))
+def test_ff_inputs_stable(golden, name):
+    assert I.fingerprint(FF_CASES[name]()) == golden["ff"][name]["fingerprint"]
+
+
+@pytest.mark.parametrize("name", sorted(GPP_CASES))
+def test_gpp_oracle_vs_reference(golden, oracle, name):
+    g = GPP_CASES[name]()
+    ref = l2c(golden["gpp"][name]["reference"])
+    assert rel_err(oracle.gpp(g), ref) < FP64_RTOL
+    if g.wx_band_stride == 0:
+        assert rel_err(oracle.gpp(g, factored=True), ref) < FP64_RTOL
+
+
+@pytest.mark.parametrize("name", sorted(FF_CASES))
+def test_ff_oracle_vs_reference(golden, oracle, name):
+    f = FF_CASES[name]()
+    ref = golden["ff"][name]["reference"]
+    assert rel_err(oracle.achs(f), l2c(ref["achs"])) < FP64_RTOL
+    assert rel_err(oracle.asx(f), l2c(ref["asx"])) < FP64_RTOL
+    assert rel_err(oracle.cor(f), l2c(ref["cor"])) < FP64_RTOL
+
+
+def test_gpp_uniform_closed_form(oracle):
+    # GPP/gpp.cpp fills: achtemp[iw] = N * 0.125i / (wx - 0.5 - 0.5i).
+    for dims in [(64, 2048, 20), (8, 1000, 10), (1, 40, 20)]:
+        nb, G, npg = dims
+        g = I.gpp_uniform(nb, 2, G, npg)
+        kat = I.gpp_uniform_closed_form(nb, G, npg)
+        assert rel_err(oracle.gpp(g), kat) < 1e-14
+        assert rel_err(oracle.gpp(g, factored=True), kat) < 1e-14
+
+
+def test_gpp_default_size_closed_form_value():
+    # The default GPP size (512 2 32768 20): achtemp(0) = (-264241152, 1321205760)
+    # exactly; the reference OpenMP build gives (-264241151.999477,
+    # 1321205760.003231).
+    kat = I.gpp_uniform_closed_form(512, 32768, 20)
+    assert kat[0] == complex(-264241152.0, 1321205760.0)
+
+
+def test_ff_uniform_closed_forms(oracle):
+    # FF/ff.cpp fills: a conj(am) = 0.5, R = 0.5+0.5i, A = 0.5-0.5i, R - A = i,
+    # interpolation weights sum to 1.
+    nb, nv, G, P, F, E = 64, 2, 512, 64, 15, 10
+    f = I.ff_uniform(nb, nv, G, P, F, E)
+    assert oracle.achs(f) == -0.125 * (1 + 1j) * nb * P * G
+    assert np.all(oracle.asx(f) == 0.25 * (1 + 1j) * nv * P * G)
+    # Kernel1 bands: wx = 10.5 - n1 > 0 and n1 >= nvband  ->  n1 = 2..10.
+    assert np.all(oracle.cor(f) == -0.25j * 9 * P * G)
+
+
+def test_compute_fact_quirks(oracle):
+    grid = np.linspace(0.0, 2.0, 9)  # 0, 0.25, ..., 2
+    # loop 1: a found ifreq == 0 is replaced by nFreq - 2 = 7 (ff.cpp:111).
+    i, f1, f2 = oracle.compute_fact(0.1, grid, 1, False)
+    assert i == 7 and f1 == pytest.approx((2.0 - 0.1) / 0.25) and f2 == pytest.approx((0.1 - 1.75) / 0.25)
+    # loop 1 on a grid point: no strict bracket -> 0 -> 7.
+    assert oracle.compute_fact(0.25, grid, 1, False)[0] == 7
+    # loop 1, negative wx searches -wx (ff.cpp:116-126).
+    i, f1, f2 = oracle.compute_fact(-0.6, grid, 1, False)
+    assert i == 2 and f1 == pytest.approx((0.75 - 0.6) / 0.25) and f2 == pytest.approx((0.6 - 0.5) / 0.25)
+    # loop 2, wx > 0: ifreq 0 is kept (the `== -1` test never fires), -0.5 factor.
+    i, f1, f2 = oracle.compute_fact(0.1, grid, 2, False)
+    assert i == 0 and f1 == pytest.approx(-0.5 * 0.15 / 0.25) and f2 == pytest.approx(-0.5 * 0.1 / 0.25)
+    # loop 2, wx <= 0 and occupied: search -wx.
+    i, f1, f2 = oracle.compute_fact(-0.3, grid, 2, True)
+    assert i == 1 and f1 == pytest.approx(0.8) and f2 == pytest.approx(0.2)
+    # loop 2, wx <= 0 and unoccupied: untouched.
+    assert oracle.compute_fact(-0.3, grid, 2, False) == (0, 0.0, 0.0)
+
+
+def test_compute_fact_golden(golden, oracle):
+    grid = np.array(golden["compute_fact_grid"])
+    for wx, loop, occ, i, f1, f2 in golden["compute_fact"]:
+        assert oracle.compute_fact(wx, grid, loop, bool(occ)) == (i, f1, f2)
+
+
+def test_reference_live_if_built(oracle):
+    from oracle.oracle import Reference
+    if not Reference.available():
+        pytest.skip("reference build (oracle/_ref) not present on this machine")
+    ref = Reference()
+    g = I.gpp_seeded(16, 2, 512, 8, seed=99)
+    assert rel_err(ref.gpp(g), oracle.gpp(g)) < FP64_RTOL
+    f = I.ff_seeded(16, 3, 256, 32, 5, 2, seed=99)
+    assert rel_err(ref.achs(f), oracle.achs(f)) < FP64_RTOL
+    assert rel_err(ref.asx(f), oracle.asx(f)) < FP64_RTOL
+    assert rel_err(ref.cor(f), oracle.cor(f)) < FP64_RTOL
