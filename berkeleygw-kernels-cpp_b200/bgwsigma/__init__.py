@@ -38,7 +38,8 @@ FLAG_PROFILE = 2
 # Every extern "C" symbol include/bgw_sigma.h declares.
 EXPORTS = ("bgw_options_init", "bgw_noflagOCC_solver", "bgw_achsDtemp_Kernel", "bgw_asxDtemp_Kernel",
            "bgw_achDtemp_cor_Kernel", "bgw_ff_sigma", "bgw_status_string", "bgw_abi_version",
-           "bgw_launch_count", "bgw_measure_fp64_peak", "bgw_release_workspace", "bgw_last_profile")
+           "bgw_launch_count", "bgw_measure_fp64_peak", "bgw_release_workspace", "bgw_last_profile",
+           "bgw_noflagOCC_solver_noalloc")
 
 
 class BgwError(RuntimeError):
@@ -96,6 +97,8 @@ def load(build_if_needed: bool = True) -> ctypes.CDLL:
     lib.bgw_last_profile.argtypes = [ctypes.POINTER(Profile)]
     opt = ctypes.POINTER(Options)
     lib.bgw_noflagOCC_solver.argtypes = [_I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, opt]
+    lib.bgw_noflagOCC_solver_noalloc.argtypes = [_I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P,
+                                                 ctypes.c_int32, _P]
     lib.bgw_achsDtemp_Kernel.argtypes = [_I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _I64, _P, _P, opt]
     lib.bgw_asxDtemp_Kernel.argtypes = [_I64, _I64, _I64, _I64, _I64, _D, _D, _D, _P, _P, _P, _P, _I64, _P, _P,
                                         _I64, _P, _P, _P, _P, opt]

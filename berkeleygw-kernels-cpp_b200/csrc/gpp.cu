@@ -421,4 +421,114 @@ int gpp_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *i
   return BGW_OK;
 }
 
+// ------------------------------------------------------ no-allocation path --
+//
+// bgw_noflagOCC_solver_noalloc (include/bgw_sigma.h) serves callers that
+// cannot allocate GPU memory: it evaluates the factored GPP sum with the
+// kernels above, and all its scratch -- the status words, the per-column
+// sums S[ngpown] and the per-CTA partials -- lives in one static device
+// array compiled into the library.  The host never dereferences the array's
+// name: on a device's first call the address is fetched with
+// cudaGetSymbolAddress (with that device current) and cached.
+namespace {
+
+constexpr int64_t kNoAllocMaxNgpown = BGW_NOALLOC_MAX_NGPOWN;
+constexpr int kNoAllocMaxGrid = 2048;  // grid-stride kernel: any grid works
+constexpr size_t kNoAllocStatusOff = 0;
+constexpr size_t kNoAllocSOff = 256;
+constexpr size_t kNoAllocPartialOff = kNoAllocSOff + sizeof(double2) * (size_t)kNoAllocMaxNgpown;
+constexpr size_t kNoAllocBytes = kNoAllocPartialOff + sizeof(double) * 6 * (size_t)kNoAllocMaxGrid;
+static_assert(kNoAllocBytes == BGW_NOALLOC_SCRATCH_BYTES, "scratch size must match the header");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char *g_noalloc_base[kNoAllocMaxDevices] = {};
+int g_noalloc_sms[kNoAllocMaxDevices] = {};
+
+// Once per device, with `dev` current: the device address of the scratch
+// array and the SM count.
+int noalloc_setup(int dev, unsigned char **base, int *sms) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_base[dev]) {
+    void *p = nullptr;
+    BGW_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    int n = 0;
+    BGW_CUDA_TRY(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+    g_noalloc_sms[dev] = n;
+    g_noalloc_base[dev] = static_cast<unsigned char *>(p);
+  }
+  *base = g_noalloc_base[dev];
+  *sms = g_noalloc_sms[dev];
+  return BGW_OK;
+}
+
+bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+}  // namespace
+
 }  // namespace bgw
+
+extern "C" int bgw_noflagOCC_solver_noalloc(int64_t number_bands, int64_t ngpown, int64_t ncouls,
+                                            const int32_t *inv_igp_index, const int32_t *indinv,
+                                            int64_t indinv_len, const double *wx_array,
+                                            const double *wtilde_array, const double *aqsmtemp,
+                                            const double *aqsntemp, const double *I_eps_array,
+                                            const double *vcoul, double *achtemp, int32_t device, void *stream) {
+  using namespace bgw;
+  const int64_t nb = number_bands, P = ngpown, G = ncouls;
+  if (nb < 0 || P < 0 || G <= 0 || nb > INT32_MAX || G > INT32_MAX) return BGW_ERR_INVALID_ARG;
+  if (P > kNoAllocMaxNgpown) return BGW_ERR_INVALID_ARG;  // beyond the static scratch
+  if (indinv_len <= 0 || indinv_len > INT32_MAX) return BGW_ERR_INVALID_ARG;
+  if (!achtemp || !wx_array || !vcoul || !indinv) return BGW_ERR_INVALID_ARG;
+  if (P > 0 && (!inv_igp_index || !wtilde_array || !I_eps_array)) return BGW_ERR_INVALID_ARG;
+  if (nb > 0 && P > 0 && (!aqsmtemp || !aqsntemp)) return BGW_ERR_INVALID_ARG;
+  if (!aligned16(wtilde_array) || !aligned16(I_eps_array) || !aligned16(aqsmtemp) || !aligned16(aqsntemp))
+    return BGW_ERR_INVALID_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+    (void)cudaGetLastError();
+    return BGW_ERR_NO_DEVICE;
+  }
+  int dev = device;
+  if (dev < 0) BGW_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev >= ndev || dev >= kNoAllocMaxDevices) return BGW_ERR_INVALID_ARG;
+  BGW_CUDA_TRY(cudaSetDevice(dev));
+  unsigned char *base = nullptr;
+  int sms = 0;
+  BGW_TRY(noalloc_setup(dev, &base, &sms));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int *status = reinterpret_cast<int *>(base + kNoAllocStatusOff);
+  double2 *S = reinterpret_cast<double2 *>(base + kNoAllocSOff);
+  double *partials = reinterpret_cast<double *>(base + kNoAllocPartialOff);
+
+  // The scratch keeps the previous call's contents: only the status words
+  // must start at zero (S and the partials are fully rewritten below).
+  BGW_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int32_t) * STATUS_WORDS, s));
+  const int nchunks_g = (int)((G + kChunk - 1) / kChunk);
+  const long long items = (long long)P * nchunks_g;
+  int prep_grid = (int)std::min<long long>((P + 7) / 8, (long long)sms * 16);
+  if (prep_grid < 1) prep_grid = 1;
+  gpp_prep_kernel<<<prep_grid, 256, 0, s>>>((int)nb, (int)P, (int)G, inv_igp_index, indinv, indinv_len,
+                                            reinterpret_cast<const double2 *>(wtilde_array),
+                                            reinterpret_cast<const double2 *>(aqsmtemp),
+                                            reinterpret_cast<const double2 *>(aqsntemp), vcoul, nullptr, S, status);
+  count_launch();
+  BGW_CUDA_TRY(cudaGetLastError());
+  int grid = (int)std::min<long long>(std::max<long long>(items, 1), (long long)sms * 8);
+  grid = std::min(grid, kNoAllocMaxGrid);
+  gpp_factored_kernel<<<grid, kThreads, 0, s>>>((int)G, items, nchunks_g,
+                                                reinterpret_cast<const double2 *>(wtilde_array),
+                                                reinterpret_cast<const double2 *>(I_eps_array), S, wx_array,
+                                                partials);
+  count_launch();
+  BGW_CUDA_TRY(cudaGetLastError());
+  reduce_partials_kernel<6><<<1, 256, 0, s>>>(partials, grid, achtemp);
+  count_launch();
+  BGW_CUDA_TRY(cudaGetLastError());
+  int32_t st[STATUS_WORDS] = {0, 0, 0, 0};
+  BGW_CUDA_TRY(cudaMemcpyAsync(st, status, sizeof(st), cudaMemcpyDeviceToHost, s));
+  BGW_CUDA_TRY(cudaStreamSynchronize(s));
+  return st[0];
+}

@@ -105,6 +105,47 @@ int bgw_noflagOCC_solver(int64_t number_bands, int64_t ngpown, int64_t ncouls,
                          const double *vcoul, double *achtemp,
                          const bgw_options *opt);
 
+/* --------------------------------------------------- GPP, no allocation --
+ * No counterpart in the reference.  A variant of bgw_noflagOCC_solver for
+ * callers that cannot allocate GPU memory: code whose device memory is all
+ * owned by another runtime or a preallocated pool (so a cudaMalloc outside
+ * it would fail or break the budget), and latency-critical loops that must
+ * never enter the CUDA allocator, because cudaMalloc/cudaFree can
+ * synchronise the whole device.  The regular entry points cannot serve them:
+ * they grow a cached workspace with cudaMalloc on first use.
+ *
+ * This variant allocates nothing.  Its scratch (status words, the per-column
+ * sums of sch_store1 over bands and per-CTA partials) is one static device
+ * array of BGW_NOALLOC_SCRATCH_BYTES (1.1 MiB) compiled into the library;
+ * every GPU that loads the library holds that array until the process exits.
+ * It evaluates the factored GPP sum (exact algebra for the reference's
+ * band-independent wx_array[3]; within 1e-12 of bgw_noflagOCC_solver).
+ *   - Every pointer must be device memory of `device` (-1: current device);
+ *     complex arrays 16-byte aligned.  achtemp: 3 complex (6 doubles).
+ *   - ngpown must not exceed BGW_NOALLOC_MAX_NGPOWN: larger sizes return
+ *     BGW_ERR_INVALID_ARG before any device work.
+ *   - The call enqueues on `stream` (cudaStream_t, NULL = default stream)
+ *     and synchronises it to read the status.
+ *   - A device's first call fetches the array's device address
+ *     (cudaGetSymbolAddress) for that device; make that first call before
+ *     any stream capture.
+ *   - All calls on a device share the array, which keeps the last call's
+ *     contents; the call clears the status words itself.  Calls that overlap
+ *     on the GPU (other threads or streams) race on the scratch: serialise
+ *     them. */
+#define BGW_NOALLOC_MAX_NGPOWN 65536
+#define BGW_NOALLOC_SCRATCH_BYTES 1147136
+int bgw_noflagOCC_solver_noalloc(int64_t number_bands, int64_t ngpown,
+                                 int64_t ncouls, const int32_t *inv_igp_index,
+                                 const int32_t *indinv, int64_t indinv_len,
+                                 const double *wx_array,
+                                 const double *wtilde_array,
+                                 const double *aqsmtemp,
+                                 const double *aqsntemp,
+                                 const double *I_eps_array,
+                                 const double *vcoul, double *achtemp,
+                                 int32_t device, void *stream);
+
 /* ------------------------------------------------------------------- FF --
  * Replaces achsDtemp_Kernel (FF/ff.cpp:171-209).  Note the reference order
  * aqsntemp before aqsmtemp.  I_epsR_array complex [nFreq][ngpown][ncouls]
