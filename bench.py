@@ -231,7 +231,7 @@ def run_ours(args, world, rank, local):
 
     # Warm-up.
     for _ in range(args.warmup):
-        bgw.noflagOCC_solver(d, stream=sh, out=out, flags=bgw.FLAG_PROFILE)
+        bgw.noflagOCC_solver(d, stream=sh, out=out, algorithm="bandloop", flags=bgw.FLAG_PROFILE)
     torch.cuda.synchronize(dev)
     barrier()
     torch.cuda.synchronize(dev)
@@ -245,7 +245,7 @@ def run_ours(args, world, rank, local):
     main_ms = []
     e0.record(stream)
     for _ in range(args.steps):
-        bgw.noflagOCC_solver(d, stream=sh, out=out, flags=bgw.FLAG_PROFILE)
+        bgw.noflagOCC_solver(d, stream=sh, out=out, algorithm="bandloop", flags=bgw.FLAG_PROFILE)
         main_ms.append(bgw.last_profile()["main_kernel_ms"])
     e1.record(stream)
     torch.cuda.synchronize(dev)
@@ -261,6 +261,7 @@ def run_ours(args, world, rank, local):
 
     kernel_ms = statistics.mean(main_ms)
     achieved = prof["flops"] / (kernel_ms * 1e-3) / 1e12
+    extra = {}
     roofline = {"bound": "fp64", "achieved": achieved, "peak": dfma_peak, "unit": "TFLOP/s",
                 "frac": achieved / dfma_peak, "traffic": traffic_from_profiles("gpp_bandloop_kernel"),
                 "kernel": prof["main_kernel"], "kernel_ms": kernel_ms,
@@ -269,24 +270,32 @@ def run_ours(args, world, rank, local):
                                "entry", "peak_dmma": dmma_peak,
                 "flop_convention": "21 flops per (band, G', G, frequency) term, 63 per triple (gpp.cpp:374-383)"}
 
-    extra = {}
     # End to end: host (pinned) inputs, H2D + kernels + D2H inside the timed region.
     gp = bgw.to_pinned(g)
-    bgw.noflagOCC_solver(gp, stream=sh)
-    torch.cuda.synchronize(dev)
-    barrier()
-    h0 = torch.cuda.Event(enable_timing=True)
-    h1 = torch.cuda.Event(enable_timing=True)
-    e2e_steps = max(3, min(args.steps, 10))
-    h0.record(stream)
-    for _ in range(e2e_steps):
-        host_res = bgw.noflagOCC_solver(gp, stream=sh)
-    h1.record(stream)
-    torch.cuda.synchronize(dev)
-    e2e_ms = max_over_ranks(h0.elapsed_time(h1))
-    e2e = {"value": e2e_ms / 1e3 / (e2e_steps * world), "unit": "s", "h2d_bytes_per_step": int(g.nbytes()),
-           "d2h_bytes_per_step": 48, "steps": e2e_steps,
-           "note": "bgw_noflagOCC_solver with BGW_MEMORY_HOST on pinned buffers (the drop-in path)"}
+
+    def time_e2e(algorithm):
+        bgw.noflagOCC_solver(gp, stream=sh, algorithm=algorithm)
+        torch.cuda.synchronize(dev)
+        barrier()
+        h0 = torch.cuda.Event(enable_timing=True)
+        h1 = torch.cuda.Event(enable_timing=True)
+        n = max(3, min(args.steps, 10))
+        h0.record(stream)
+        for _ in range(n):
+            res = bgw.noflagOCC_solver(gp, stream=sh, algorithm=algorithm)
+        h1.record(stream)
+        torch.cuda.synchronize(dev)
+        return max_over_ranks(h0.elapsed_time(h1)) / 1e3 / (n * world), n, res
+
+    e2e_s, e2e_steps, host_res = time_e2e("bandloop")
+    e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(g.nbytes()), "d2h_bytes_per_step": 48,
+           "steps": e2e_steps, "note": "bgw_noflagOCC_solver (band loop) with BGW_MEMORY_HOST on pinned buffers: "
+                                       "H2D of every input + kernels + D2H of achtemp per step"}
+    if not args.quick:
+        auto_s, _, auto_res = time_e2e("auto")
+        extra["e2e_auto"] = {"value": auto_s, "unit": "s", "h2d_bytes_per_step": int(g.nbytes()),
+                             "d2h_bytes_per_step": 48,
+                             "note": "default algorithm (factored for the band-independent wx), the drop-in's path"}
     del gp
 
     # Factored GPP path (band-independent wx): HBM-bound stream.
@@ -381,6 +390,43 @@ def run_ours(args, world, rank, local):
     return 0
 
 
+def run_only(args, local):
+    """Diagnostic mode for profilers: runs one kernel path W + K times on the
+    benchmark shapes (GPP bands optionally reduced with --bands) and prints a
+    JSON line with the library's per-call timings.  Not the benchmark line."""
+    import torch
+    import bgwsigma as bgw
+    from bgwsigma import inputs as I
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    bgw.load()
+    if args.only in ("gpp_bandloop", "gpp_factored"):
+        dims = dict(GPP_DIMS)
+        if args.bands:
+            dims["number_bands"] = args.bands
+        d = bgw.to_device(I.gpp_seeded(**dims, seed=1234), dev)
+        alg = args.only.split("_")[1]
+        call = lambda: bgw.noflagOCC_solver(d, algorithm=alg, flags=bgw.FLAG_PROFILE)  # noqa: E731
+    else:
+        dims = dict(FF_DIMS)
+        if args.bands:
+            dims["number_bands"] = args.bands
+        d = bgw.to_device(I.ff_seeded(**dims, seed=1234), dev)
+        call = lambda: bgw.ff_sigma(d, flags=bgw.FLAG_PROFILE)  # noqa: E731
+    for _ in range(args.warmup):
+        call()
+    profs = []
+    for _ in range(args.steps):
+        call()
+        profs.append(bgw.last_profile())
+    ms = statistics.mean(p["main_kernel_ms"] for p in profs)
+    print(json.dumps({"only": args.only, "dims": dims, "kernel": profs[-1]["main_kernel"], "kernel_ms": ms,
+                      "device_ms": statistics.mean(p["device_ms"] for p in profs), "flops": profs[-1]["flops"],
+                      "tflops": profs[-1]["flops"] / (ms * 1e-3) / 1e12, "main_bytes": profs[-1]["main_bytes"],
+                      "GBps": profs[-1]["main_bytes"] / (ms * 1e-3) / 1e9}), flush=True)
+    return 0
+
+
 def _hbm_peak() -> float:
     p = REPO / "MEASURED_PEAKS.json"
     try:
@@ -398,10 +444,15 @@ def main():
     ap.add_argument("--quick", action="store_true", help="GPP band loop + e2e only")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and oracle check")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--only", choices=["gpp_bandloop", "gpp_factored", "ff"], default=None,
+                    help="diagnostic: time one kernel path only (for profilers)")
+    ap.add_argument("--bands", type=int, default=0, help="with --only: number_bands override")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local = dist_setup(args)
+    if args.only:
+        return run_only(args, local)
     if args.impl == "reference":
         return run_reference_arm(args, world, rank)
     return run_ours(args, world, rank, local)

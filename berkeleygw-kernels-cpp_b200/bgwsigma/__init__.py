@@ -31,7 +31,7 @@ STATUS = {0: "BGW_OK", -1: "BGW_ERR_INVALID_ARG", -2: "BGW_ERR_INDEX", -3: "BGW_
           -4: "BGW_ERR_ALLOC", -5: "BGW_ERR_NO_DEVICE", -6: "BGW_ERR_TIMEOUT", -7: "BGW_ERR_UNSUPPORTED"}
 MEMORY = {"host": 0, "device": 1}
 PRECISION = {"fp64": 0, "mixed": 1}
-GPP_ALGO = {"bandloop": 0, "factored": 1}
+GPP_ALGO = {"bandloop": 0, "factored": 1, "auto": 2}
 FLAG_ASYNC = 1
 FLAG_PROFILE = 2
 
@@ -160,7 +160,7 @@ def _where(inp) -> str:
     return kinds.pop()
 
 
-def make_options(memory="host", precision="fp64", algorithm="bandloop", wx_band_stride=0, device=-1, stream=None,
+def make_options(memory="host", precision="fp64", algorithm="auto", wx_band_stride=0, device=-1, stream=None,
                  flags=0, device_status=None) -> Options:
     o = Options()
     load().bgw_options_init(ctypes.byref(o))
@@ -181,7 +181,7 @@ def _stream_handle(inp, stream):
     return None
 
 
-def noflagOCC_solver(inp: GppInputs, *, precision="fp64", algorithm="bandloop", stream=None, out=None,
+def noflagOCC_solver(inp: GppInputs, *, precision="fp64", algorithm="auto", stream=None, out=None,
                      flags=0, device_status=None) -> np.ndarray:
     """achtemp[3] (complex128).  `out`: optional preallocated output (host
     numpy complex128[3] or a CUDA tensor for device-resident inputs)."""

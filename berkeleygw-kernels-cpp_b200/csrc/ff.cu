@@ -86,10 +86,11 @@ Fact compute_fact_host(double wx, int nFreq, const double *g, int loop, bool fla
 
 namespace {
 
-constexpr int kTM = 32;       // rows (bands) per tile
-constexpr int kTN = 64;       // G' columns per tile
-constexpr int kBK = 16;       // complex k per stage
-constexpr int kLds = kBK + 4;  // padded row stride (double2): 320 B
+constexpr int kTM = 32;        // rows (bands) per tile
+constexpr int kTN = 64;        // G' columns per tile
+constexpr int kBK = 8;         // complex k per pipeline stage
+constexpr int kLds = kBK + 4;  // padded row stride (double2): 192 B, conflict-free fragment reads
+constexpr int kStages = 3;     // cp.async pipeline depth
 constexpr int kFFThreads = 128;
 
 struct GroupKey {
@@ -229,9 +230,26 @@ __device__ __forceinline__ void dmma_f64(double &c0, double &c1, double a, doubl
                : "d"(a), "d"(b));
 }
 
+// cp.async (16-byte, L2-only) global -> shared copies.  `valid` false
+// zero-fills the destination without reading the source.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool valid) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(smem)), "l"(gmem),
+               "r"(valid ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+struct FFStage {
+  double2 a[kTM * kLds];   // aqsn rows of the tile
+  double2 b[kTN * kLds];   // X_f rows (I_epsR or I_epsA)
+  double2 b2[kTN * kLds];  // I_epsA rows when the tile needs R - A
+};
 struct FFSmem {
-  double2 a[2][kTM * kLds];
-  double2 b[2][kTN * kLds];
+  FFStage st[kStages];
   double red[(kFFThreads / 32) * 2];
 };
 
@@ -239,9 +257,10 @@ struct FFSmem {
 // tile and all 32 rows: 4 x 2 m8n8 blocks, each a complex accumulator kept
 // as separate real and imaginary DMMA accumulators (4 real MMAs per complex
 // k4 step: Re += Ar Br + Ai (-Bi), Im += Ar Bi + Ai Br).
-// Operands are staged global -> registers -> shared (double-buffered, the
-// next stage's loads in flight during the current stage's MMAs); the R - A
-// difference of the COR sum is formed in registers on the way.
+// Operands stream global -> shared through a kStages-deep cp.async pipeline
+// (rows gathered by band index, out-of-range rows / k zero-filled); for the
+// COR sum the I_epsR and I_epsA rows are staged separately and R - A is
+// formed when the B fragments are read.
 __global__ void __launch_bounds__(kFFThreads, 2)
     ff_contract_kernel(const FFTile *__restrict__ tiles, const FFRow *__restrict__ rows, int P, int G,
                        const double2 *__restrict__ aqsn, const double2 *__restrict__ R, int r_f0,
@@ -257,47 +276,50 @@ __global__ void __launch_bounds__(kFFThreads, 2)
   // R / A point at slice r_f0 / a_f0 (host-staged inputs hold only the
   // slices the plan reads).
   const double2 *X0 = (t.src == SRC_A) ? A + (size_t)(t.f - a_f0) * slice : R + (size_t)(t.f - r_f0) * slice;
-  const double2 *X1 = (t.src == SRC_RA) ? A + (size_t)(t.f - a_f0) * slice : nullptr;
+  const bool sub = (t.src == SRC_RA);
+  const double2 *X1 = sub ? A + (size_t)(t.f - a_f0) * slice : X0;
 
-  // Staging assignment: element idx = q * 128 + tid of a [rows][kBK] tile.
-  const int kc = tid & (kBK - 1);
-  const int r_lo = tid >> 4;  // 0..7
-  int a_band[kTM / 8];
+  // Copy assignment: element idx = q * 128 + tid of a [rows][kBK] tile,
+  // row idx / kBK, k offset idx % kBK.
+  constexpr int kAq = kTM * kBK / kFFThreads, kBq = kTN * kBK / kFFThreads;
+  const int kc = tid % kBK;
+  const double2 *a_src[kAq];
+  bool a_ok[kAq];
 #pragma unroll
-  for (int q = 0; q < kTM / 8; ++q) {
-    const int r = q * 8 + r_lo;
-    a_band[q] = r < t.row_count ? rows[t.row_begin + r].band : -1;
+  for (int q = 0; q < kAq; ++q) {
+    const int r = (q * kFFThreads + tid) / kBK;
+    a_ok[q] = r < t.row_count;
+    a_src[q] = a_ok[q] ? aqsn + (size_t)rows[t.row_begin + r].band * G + t.k_begin + kc : aqsn;
+  }
+  const double2 *b_src[kBq];
+  const double2 *b2_src[kBq];
+  bool b_ok[kBq];
+#pragma unroll
+  for (int q = 0; q < kBq; ++q) {
+    const int p = t.p_begin + (q * kFFThreads + tid) / kBK;
+    b_ok[q] = p < P;
+    b_src[q] = b_ok[q] ? X0 + (size_t)p * G + t.k_begin + kc : X0;
+    b2_src[q] = b_ok[q] ? X1 + (size_t)p * G + t.k_begin + kc : X1;
   }
 
-  double2 ra[kTM / 8], rb[kTN / 8];
-  auto load_stage = [&](int kb) {
-    const int k = t.k_begin + kb * kBK + kc;
-    const bool kin = (kb * kBK + kc) < t.k_count;
+  const int nk = (t.k_count + kBK - 1) / kBK;
+  auto issue = [&](int kb, int buf) {
+    FFStage &s = sm.st[buf];
+    const bool kin = kb * kBK + kc < t.k_count;
+    const size_t off = (size_t)kb * kBK;
 #pragma unroll
-    for (int q = 0; q < kTM / 8; ++q) {
-      ra[q] = make_double2(0.0, 0.0);
-      if (kin && a_band[q] >= 0) ra[q] = __ldg(aqsn + (size_t)a_band[q] * G + k);
+    for (int q = 0; q < kAq; ++q) {
+      const int idx = q * kFFThreads + tid;
+      const bool v = kin && a_ok[q];
+      cp_async16(&s.a[(idx / kBK) * kLds + kc], v ? a_src[q] + off : aqsn, v);
     }
 #pragma unroll
-    for (int q = 0; q < kTN / 8; ++q) {
-      const int p = t.p_begin + q * 8 + r_lo;
-      rb[q] = make_double2(0.0, 0.0);
-      if (kin && p < P) {
-        double2 x = __ldcs(X0 + (size_t)p * G + k);
-        if (X1) {
-          const double2 y = __ldcs(X1 + (size_t)p * G + k);
-          x.x -= y.x;
-          x.y -= y.y;
-        }
-        rb[q] = x;
-      }
+    for (int q = 0; q < kBq; ++q) {
+      const int idx = q * kFFThreads + tid;
+      const bool v = kin && b_ok[q];
+      cp_async16(&s.b[(idx / kBK) * kLds + kc], v ? b_src[q] + off : X0, v);
+      if (sub) cp_async16(&s.b2[(idx / kBK) * kLds + kc], v ? b2_src[q] + off : X1, v);
     }
-  };
-  auto store_stage = [&](int buf) {
-#pragma unroll
-    for (int q = 0; q < kTM / 8; ++q) sm.a[buf][(q * 8 + r_lo) * kLds + kc] = ra[q];
-#pragma unroll
-    for (int q = 0; q < kTN / 8; ++q) sm.b[buf][(q * 8 + r_lo) * kLds + kc] = rb[q];
   };
 
   double cr[4][2][2], ci[4][2][2];
@@ -306,17 +328,21 @@ __global__ void __launch_bounds__(kFFThreads, 2)
 #pragma unroll
     for (int n = 0; n < 2; ++n) cr[m][n][0] = cr[m][n][1] = ci[m][n][0] = ci[m][n][1] = 0.0;
 
-  const int nk = (t.k_count + kBK - 1) / kBK;
-  if (nk > 0) {
-    load_stage(0);
-    store_stage(0);
+#pragma unroll
+  for (int s = 0; s < kStages - 1; ++s) {
+    if (s < nk) issue(s, s);
+    cp_async_commit();
   }
-  __syncthreads();
   for (int kb = 0; kb < nk; ++kb) {
-    const int buf = kb & 1;
-    if (kb + 1 < nk) load_stage(kb + 1);
-    const double2 *sa = sm.a[buf];
-    const double2 *sb = sm.b[buf] + (warp * 16) * kLds;
+    cp_async_wait<kStages - 2>();
+    __syncthreads();  // stage kb landed for every thread; stage kb-1 fully consumed
+    const int nxt = kb + kStages - 1;
+    if (nxt < nk) issue(nxt, nxt % kStages);
+    cp_async_commit();
+    const FFStage &s = sm.st[kb % kStages];
+    const double2 *sa = s.a;
+    const double2 *sb = s.b + (warp * 16) * kLds;
+    const double2 *sb2 = s.b2 + (warp * 16) * kLds;
 #pragma unroll
     for (int ks = 0; ks < kBK / 4; ++ks) {
       double ar[4], ai[4], br[2], bi[2], bn[2];
@@ -328,7 +354,12 @@ __global__ void __launch_bounds__(kFFThreads, 2)
       }
 #pragma unroll
       for (int n = 0; n < 2; ++n) {
-        const double2 v = sb[(n * 8 + g8) * kLds + ks * 4 + t4];
+        double2 v = sb[(n * 8 + g8) * kLds + ks * 4 + t4];
+        if (sub) {
+          const double2 y = sb2[(n * 8 + g8) * kLds + ks * 4 + t4];
+          v.x -= y.x;
+          v.y -= y.y;
+        }
         br[n] = v.x;
         bi[n] = v.y;
         bn[n] = -v.y;
@@ -343,9 +374,8 @@ __global__ void __launch_bounds__(kFFThreads, 2)
           dmma_f64(ci[m][n][0], ci[m][n][1], ai[m], br[n]);
         }
     }
-    if (kb + 1 < nk) store_stage(buf ^ 1);
-    __syncthreads();
   }
+  cp_async_wait<0>();
 
   // Epilogue: sum_r coef(r) sum_p W(band(r), p) C(r, p) over this thread's
   // accumulator entries (row m*8+g8, column warp*16 + n*8 + 2*t4 + j).

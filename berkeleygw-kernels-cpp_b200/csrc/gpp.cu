@@ -114,24 +114,26 @@ struct Elem {
   double wr, wi2, Ir, Ii, a, b;
 };
 
-template <int BCH, bool WX_SHARED>
+template <int BCH>
 struct BandSmem {
   double2 wt[2][kChunk];
   double2 ie[2][kChunk];
   double2 st[2][BCH];
-  double4 wx[2][WX_SHARED ? 1 : BCH];
+  double4 wx[2][BCH];
   unsigned long long bar[2];
   double red[(kThreads / 32) * 6];
 };
 
-template <int BCH, bool WX_SHARED>
+// Every band reads its own frequencies from the staged wx4 rows (for the
+// reference's band-independent wx the rows repeat one triple), so each
+// (band, G', G, frequency) quotient is evaluated, as in gpp.cpp:343-390.
+template <int BCH>
 __global__ void __launch_bounds__(kThreads, 2)
     gpp_bandloop_kernel(int nb, int G, long long items, int nchunks_g, const double2 *__restrict__ wtilde,
                         const double2 *__restrict__ ieps, const double2 *__restrict__ st,
-                        const double4 *__restrict__ wx4, const double *__restrict__ wx3,
-                        double *__restrict__ partials, int *status) {
+                        const double4 *__restrict__ wx4, double *__restrict__ partials, int *status) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  using Smem = BandSmem<BCH, WX_SHARED>;
+  using Smem = BandSmem<BCH>;
   Smem &sm = *reinterpret_cast<Smem *>(smem_raw);
   const int tid = threadIdx.x;
   const int nbc = (nb + BCH - 1) / BCH;
@@ -157,21 +159,15 @@ __global__ void __launch_bounds__(kThreads, 2)
     const int b0 = c * BCH;
     const int nbv = min(BCH, nb - b0);
     const int buf = (int)(j & 1);
-    uint32_t bytes = 2u * nvalid * 16u + nbv * 16u + (WX_SHARED ? 0u : nbv * 32u);
+    uint32_t bytes = 2u * nvalid * 16u + nbv * 16u + nbv * 32u;
     uint64_t *bar = reinterpret_cast<uint64_t *>(&sm.bar[buf]);
     mbar_expect_tx(bar, bytes);
     bulk_g2s(sm.wt[buf], wtilde + p * G + g0, nvalid * 16u, bar);
     bulk_g2s(sm.ie[buf], ieps + p * G + g0, nvalid * 16u, bar);
     bulk_g2s(sm.st[buf], st + p * nb + b0, nbv * 16u, bar);
-    if (!WX_SHARED) bulk_g2s(sm.wx[buf], wx4 + b0, nbv * 32u, bar);
+    bulk_g2s(sm.wx[buf], wx4 + b0, nbv * 32u, bar);
   };
 
-  double x0s = 0.0, x1s = 0.0, x2s = 0.0;
-  if (WX_SHARED) {
-    x0s = wx3[0];
-    x1s = wx3[1];
-    x2s = wx3[2];
-  }
   double acc_r[3] = {0.0, 0.0, 0.0}, acc_i[3] = {0.0, 0.0, 0.0};
   bool ok = true;
   if (tid == 0 && nsteps > 0) issue(0);
@@ -213,17 +209,8 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
 
     for (int bb = 0; bb < nbv; ++bb) {
-      double x[3];
-      if (WX_SHARED) {
-        x[0] = x0s;
-        x[1] = x1s;
-        x[2] = x2s;
-      } else {
-        double4 w4 = sm.wx[buf][bb];
-        x[0] = w4.x;
-        x[1] = w4.y;
-        x[2] = w4.z;
-      }
+      const double4 w4 = sm.wx[buf][bb];
+      const double x[3] = {w4.x, w4.y, w4.z};
       const double2 s = sm.st[buf][bb];
       double tr[3] = {0.0, 0.0, 0.0}, ti[3] = {0.0, 0.0, 0.0};
 #pragma unroll
@@ -320,13 +307,13 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-template <int BCH, bool WX_SHARED>
-int launch_bandloop(Workspace *ws,cudaStream_t stream, int nb, int G, long long items, int nchunks_g,
-                    const double2 *wt, const double2 *ie, const double2 *st, const double4 *wx4, const double *wx3,
+template <int BCH>
+int launch_bandloop(Workspace *ws, cudaStream_t stream, int nb, int G, long long items, int nchunks_g,
+                    const double2 *wt, const double2 *ie, const double2 *st, const double4 *wx4,
                     double **partials_out, int *grid_out, int *status) {
-  using Smem = BandSmem<BCH, WX_SHARED>;
+  using Smem = BandSmem<BCH>;
   const size_t smem = sizeof(Smem);
-  auto kfn = gpp_bandloop_kernel<BCH, WX_SHARED>;
+  auto kfn = gpp_bandloop_kernel<BCH>;
   BGW_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   BGW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kThreads, smem));
@@ -337,7 +324,7 @@ int launch_bandloop(Workspace *ws,cudaStream_t stream, int nb, int G, long long 
   BGW_TRY(ws_reserve(ws, SLOT_PARTIALS, sizeof(double) * 6 * (size_t)grid, &partials));
   *grid_out = (int)grid;
   *partials_out = (double *)partials;
-  kfn<<<(int)grid, kThreads, smem, stream>>>(nb, G, items, nchunks_g, wt, ie, st, wx4, wx3, (double *)partials,
+  kfn<<<(int)grid, kThreads, smem, stream>>>(nb, G, items, nchunks_g, wt, ie, st, wx4, (double *)partials,
                                              status);
   count_launch();
   BGW_CUDA_TRY(cudaGetLastError());
@@ -356,7 +343,8 @@ int gpp_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *i
   cudaStream_t stream = env->stream;
   const int nchunks_g = (int)((G + kChunk - 1) / kChunk);
   const long long items = (long long)P * nchunks_g;
-  const bool factored = env->opt.gpp_algorithm == BGW_GPP_FACTORED;
+  const bool factored = env->opt.gpp_algorithm == BGW_GPP_FACTORED ||
+                        (env->opt.gpp_algorithm == BGW_GPP_AUTO && wx_stride == 0);
   int prep_grid = (int)std::min<long long>((P + 7) / 8, (long long)ws->sm_count * 16);
   if (prep_grid < 1) prep_grid = 1;
 
@@ -391,9 +379,9 @@ int gpp_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *i
                                                  (double2 *)st, nullptr, env->d_status);
   count_launch();
   BGW_CUDA_TRY(cudaGetLastError());
-  const bool wx_shared = (wx_stride == 0);
-  if (!wx_shared) {
-    BGW_TRY(ws_reserve(ws, SLOT_TABLE1, sizeof(double4) * (size_t)std::max<int64_t>(nb, 1), &wx4));
+  // Per-band frequency rows (stride 0: the one triple repeated per band).
+  BGW_TRY(ws_reserve(ws, SLOT_TABLE1, sizeof(double4) * (size_t)std::max<int64_t>(nb, 1), &wx4));
+  if (nb > 0) {
     int g = (int)std::min<int64_t>((nb + 255) / 256, 1024);
     gpp_wx_kernel<<<std::max(g, 1), 256, 0, stream>>>((int)nb, wx, wx_stride, (double4 *)wx4);
     count_launch();
@@ -402,17 +390,10 @@ int gpp_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *i
   int grid = 0;
   double *partials = nullptr;
   BGW_TRY(prof_mark(env, 1));
-  if (wx_shared) {
-    BGW_TRY((launch_bandloop<512, true>(ws, stream, (int)nb, (int)G, items, nchunks_g, wt, ie, (const double2 *)st,
-                                        nullptr, wx, &partials, &grid, env->d_status)));
-  } else {
-    BGW_TRY((launch_bandloop<256, false>(ws, stream, (int)nb, (int)G, items, nchunks_g, wt, ie,
-                                         (const double2 *)st, (const double4 *)wx4, nullptr, &partials, &grid,
-                                         env->d_status)));
-  }
+  BGW_TRY((launch_bandloop<256>(ws, stream, (int)nb, (int)G, items, nchunks_g, wt, ie, (const double2 *)st,
+                                (const double4 *)wx4, &partials, &grid, env->d_status)));
   BGW_TRY(prof_mark(env, 2));
-  env->prof.main_bytes = 32.0 * (double)P * (double)G + 16.0 * (double)P * (double)nb +
-                         (wx_shared ? 24.0 : 32.0 * (double)nb);
+  env->prof.main_bytes = 32.0 * (double)P * (double)G + 16.0 * (double)P * (double)nb + 32.0 * (double)nb;
   env->prof.main_launches = 1;
   std::snprintf(env->prof.main_kernel, sizeof(env->prof.main_kernel), "gpp_bandloop_kernel");
   reduce_partials_kernel<6><<<1, 256, 0, stream>>>(partials, grid, achtemp_dev);

@@ -91,7 +91,8 @@ int begin_call(const bgw_options *user, CallEnv *env) {
   const bgw_options &o = env->opt;
   if (o.memory != BGW_MEMORY_HOST && o.memory != BGW_MEMORY_DEVICE) return BGW_ERR_INVALID_ARG;
   if (o.precision != BGW_PRECISION_FP64 && o.precision != BGW_PRECISION_MIXED) return BGW_ERR_INVALID_ARG;
-  if (o.gpp_algorithm != BGW_GPP_BANDLOOP && o.gpp_algorithm != BGW_GPP_FACTORED) return BGW_ERR_INVALID_ARG;
+  if (o.gpp_algorithm != BGW_GPP_BANDLOOP && o.gpp_algorithm != BGW_GPP_FACTORED && o.gpp_algorithm != BGW_GPP_AUTO)
+    return BGW_ERR_INVALID_ARG;
   if (o.wx_band_stride < 0) return BGW_ERR_INVALID_ARG;
   if ((o.flags & BGW_FLAG_ASYNC) && (o.memory != BGW_MEMORY_DEVICE || o.device_status == nullptr))
     return BGW_ERR_INVALID_ARG;
@@ -163,7 +164,7 @@ void bgw_options_init(bgw_options *opt) {
   opt->struct_size = (int32_t)sizeof(bgw_options);
   opt->memory = BGW_MEMORY_HOST;
   opt->precision = BGW_PRECISION_FP64;
-  opt->gpp_algorithm = BGW_GPP_BANDLOOP;
+  opt->gpp_algorithm = BGW_GPP_AUTO;
   opt->wx_band_stride = 0;
   opt->device = -1;
   opt->flags = 0;

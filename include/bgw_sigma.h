@@ -50,11 +50,12 @@ enum { BGW_PRECISION_FP64 = 0, BGW_PRECISION_MIXED = 1 };
 /* GPP evaluation strategy:
  *   BANDLOOP  evaluates every (band, G', G, frequency) quotient, as the
  *             reference loop nest does (GPP/gpp.cpp:343-390); supports a
- *             band-dependent wx (wx_band_stride != 0).
+ *             band-dependent wx (wx_band_stride != 0).  FP64-pipe bound.
  *   FACTORED  uses sum_n1 sch_store1(n1, p) once per G' column; valid only
  *             for a band-independent wx (wx_band_stride == 0, the
- *             reference's case) and bound by HBM bandwidth. */
-enum { BGW_GPP_BANDLOOP = 0, BGW_GPP_FACTORED = 1 };
+ *             reference's case) and bound by HBM bandwidth.
+ *   AUTO      (default) FACTORED when wx_band_stride == 0, else BANDLOOP. */
+enum { BGW_GPP_BANDLOOP = 0, BGW_GPP_FACTORED = 1, BGW_GPP_AUTO = 2 };
 /* flags */
 enum {
   BGW_FLAG_ASYNC = 1,  /* device memory only: enqueue on `stream` and return
@@ -69,7 +70,7 @@ typedef struct bgw_options {
   int32_t struct_size;     /* sizeof(bgw_options) (forward compatibility)   */
   int32_t memory;          /* BGW_MEMORY_HOST / BGW_MEMORY_DEVICE           */
   int32_t precision;       /* BGW_PRECISION_FP64 / BGW_PRECISION_MIXED      */
-  int32_t gpp_algorithm;   /* BGW_GPP_BANDLOOP / BGW_GPP_FACTORED           */
+  int32_t gpp_algorithm;   /* BGW_GPP_AUTO / BGW_GPP_BANDLOOP / _FACTORED   */
   int64_t wx_band_stride;  /* doubles between bands' wx triples; 0 = shared */
   int32_t device;          /* CUDA ordinal; -1 = the calling thread's one   */
   int32_t flags;           /* BGW_FLAG_*                                    */
@@ -77,7 +78,7 @@ typedef struct bgw_options {
   int32_t *device_status;  /* device int written with BGW_FLAG_ASYNC        */
 } bgw_options;
 
-/* Fills *opt with the defaults (host memory, FP64, BANDLOOP, stride 0,
+/* Fills *opt with the defaults (host memory, FP64, AUTO, stride 0,
  * current device, default stream, synchronous). */
 void bgw_options_init(bgw_options *opt);
 

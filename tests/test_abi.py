@@ -57,7 +57,7 @@ def test_options_defaults(bgw):
     o = bgw.Options()
     bgw.load().bgw_options_init(ctypes.byref(o))
     assert o.struct_size == ctypes.sizeof(bgw.Options)
-    assert (o.memory, o.precision, o.gpp_algorithm, o.wx_band_stride, o.device, o.flags) == (0, 0, 0, 0, -1, 0)
+    assert (o.memory, o.precision, o.gpp_algorithm, o.wx_band_stride, o.device, o.flags) == (0, 0, 2, 0, -1, 0)
 
 
 def test_shim_exports_reference_mangled_names(bgw, golden):
