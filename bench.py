@@ -316,6 +316,44 @@ def run_ours(args, world, rank, local):
                          "algorithmic_bytes_per_launch": p["main_bytes"],
                          "traffic": traffic_from_profiles("gpp_factored_kernel")},
             "rel_err_vs_bandloop": rel_err(fres.cpu().numpy(), result)}
+    # Mixed precision band loop (FP32 quotients, compensated FP64 sums).
+    if not args.quick:
+        for _ in range(2):
+            bgw.noflagOCC_solver(d, stream=sh, algorithm="bandloop", precision="mixed", flags=bgw.FLAG_PROFILE)
+        mms = []
+        for _ in range(max(3, args.steps // 2)):
+            mres = bgw.noflagOCC_solver(d, stream=sh, algorithm="bandloop", precision="mixed",
+                                        flags=bgw.FLAG_PROFILE)
+            mms.append(bgw.last_profile()["main_kernel_ms"])
+        mk = statistics.mean(mms)
+        extra["gpp_mixed"] = {"kernel": "gpp_bandloop_kernel<mixed>", "kernel_ms": mk,
+                              "speedup_vs_fp64_bandloop": kernel_ms / mk,
+                              "achieved_TFLOPs": prof["flops"] / (mk * 1e-3) / 1e12,
+                              "rel_err_vs_fp64": rel_err(mres.cpu().numpy(), result)}
+        # Adjoint (factored, HBM-bound): dSigma/domega and both [1638][32768] gradients.
+        gcot = np.array([0.3 - 1.1j, 0.7 + 0.2j, -0.4 + 0.9j])
+        for _ in range(2):
+            bgw.noflagOCC_solver_backward(d, gcot, stream=sh, flags=bgw.FLAG_PROFILE)
+        ams, adev = [], []
+        for _ in range(max(3, args.steps // 2)):
+            adj = bgw.noflagOCC_solver_backward(d, gcot, stream=sh, flags=bgw.FLAG_PROFILE)
+            p = bgw.last_profile()
+            ams.append(p["main_kernel_ms"])
+            adev.append(p["device_ms"])
+        ak = statistics.mean(ams)
+        extra["gpp_adjoint"] = {
+            "kernel": p["main_kernel"], "kernel_ms": ak, "s_per_call": statistics.mean(adev) / 1e3,
+            "roofline": {"bound": "hbm", "achieved": p["main_bytes"] / (ak * 1e-3) / 1e9, "unit": "GB/s",
+                         "peak": _hbm_peak(), "frac": p["main_bytes"] / (ak * 1e-3) / 1e9 / _hbm_peak(),
+                         "algorithmic_bytes_per_launch": p["main_bytes"]}}
+        if rank == 0 and not args.no_cpu:
+            from oracle.oracle import Oracle
+            rw, ri, rd = Oracle().gpp_backward(g, gcot)
+            extra["gpp_adjoint"]["rel_err_vs_oracle"] = {
+                "grad_wtilde": rel_err(adj[0].cpu().numpy(), rw), "grad_I_eps": rel_err(adj[1].cpu().numpy(), ri),
+                "dachtemp_domega": rel_err(adj[2].cpu().numpy(), rd)}
+            extra["gpp_mixed"]["rel_err_vs_oracle"] = rel_err(mres.cpu().numpy(), Oracle().gpp(g, factored=True))
+        del adj
     del d
     torch.cuda.empty_cache()
 
@@ -400,13 +438,18 @@ def run_only(args, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     bgw.load()
-    if args.only in ("gpp_bandloop", "gpp_factored"):
+    if args.only.startswith("gpp"):
         dims = dict(GPP_DIMS)
         if args.bands:
             dims["number_bands"] = args.bands
         d = bgw.to_device(I.gpp_seeded(**dims, seed=1234), dev)
-        alg = args.only.split("_")[1]
-        call = lambda: bgw.noflagOCC_solver(d, algorithm=alg, flags=bgw.FLAG_PROFILE)  # noqa: E731
+        if args.only == "gpp_adjoint":
+            call = lambda: bgw.noflagOCC_solver_backward(d, [1, 1j, -1], flags=bgw.FLAG_PROFILE)  # noqa: E731
+        else:
+            alg = "bandloop" if args.only == "gpp_mixed" else args.only.split("_")[1]
+            prec = "mixed" if args.only == "gpp_mixed" else "fp64"
+            call = lambda: bgw.noflagOCC_solver(d, algorithm=alg, precision=prec,  # noqa: E731
+                                                flags=bgw.FLAG_PROFILE)
     else:
         dims = dict(FF_DIMS)
         if args.bands:
@@ -444,7 +487,8 @@ def main():
     ap.add_argument("--quick", action="store_true", help="GPP band loop + e2e only")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and oracle check")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--only", choices=["gpp_bandloop", "gpp_factored", "ff"], default=None,
+    ap.add_argument("--only", choices=["gpp_bandloop", "gpp_mixed", "gpp_factored", "gpp_adjoint", "ff"],
+                    default=None,
                     help="diagnostic: time one kernel path only (for profilers)")
     ap.add_argument("--bands", type=int, default=0, help="with --only: number_bands override")
     args = ap.parse_args()

@@ -39,7 +39,7 @@ FLAG_PROFILE = 2
 EXPORTS = ("bgw_options_init", "bgw_noflagOCC_solver", "bgw_achsDtemp_Kernel", "bgw_asxDtemp_Kernel",
            "bgw_achDtemp_cor_Kernel", "bgw_ff_sigma", "bgw_status_string", "bgw_abi_version",
            "bgw_launch_count", "bgw_measure_fp64_peak", "bgw_release_workspace", "bgw_last_profile",
-           "bgw_noflagOCC_solver_noalloc")
+           "bgw_noflagOCC_solver_noalloc", "bgw_noflagOCC_solver_backward")
 
 
 class BgwError(RuntimeError):
@@ -99,6 +99,8 @@ def load(build_if_needed: bool = True) -> ctypes.CDLL:
     lib.bgw_noflagOCC_solver.argtypes = [_I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, opt]
     lib.bgw_noflagOCC_solver_noalloc.argtypes = [_I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P,
                                                  ctypes.c_int32, _P]
+    lib.bgw_noflagOCC_solver_backward.argtypes = [_I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P,
+                                                  _P, _P, opt]
     lib.bgw_achsDtemp_Kernel.argtypes = [_I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _I64, _P, _P, opt]
     lib.bgw_asxDtemp_Kernel.argtypes = [_I64, _I64, _I64, _I64, _I64, _D, _D, _D, _P, _P, _P, _P, _I64, _P, _P,
                                         _I64, _P, _P, _P, _P, opt]
@@ -201,6 +203,36 @@ def noflagOCC_solver(inp: GppInputs, *, precision="fp64", algorithm="auto", stre
                                   _ptr(out), ctypes.byref(o))
     _check("bgw_noflagOCC_solver", st)
     return out
+
+
+def noflagOCC_solver_backward(inp: GppInputs, grad_achtemp, *, want_wtilde=True, want_I_eps=True,
+                              want_domega=True, stream=None, flags=0):
+    """Adjoint of noflagOCC_solver.  grad_achtemp: 3 complex cotangents
+    (dL/dRe + i dL/dIm of each achtemp entry).  Returns (grad_wtilde,
+    grad_I_eps, dachtemp_domega) -- complex arrays [ngpown][ncouls],
+    [ngpown][ncouls], [3] -- on the inputs' side (host or device)."""
+    lib = load()
+    mem = _where(inp)
+    P, G = inp.ngpown, inp.ncouls
+    if mem == "host":
+        gc = np.ascontiguousarray(np.asarray(grad_achtemp, dtype=np.complex128).reshape(3))
+        gw = np.zeros((P, G), np.complex128) if want_wtilde else None
+        gi = np.zeros((P, G), np.complex128) if want_I_eps else None
+        dw = np.zeros(3, np.complex128) if want_domega else None
+    else:
+        import torch
+        dev = inp.wtilde_array.device
+        gc = torch.as_tensor(np.asarray(grad_achtemp, dtype=np.complex128).reshape(3)).to(dev)
+        gw = torch.zeros((P, G), dtype=torch.complex128, device=dev) if want_wtilde else None
+        gi = torch.zeros((P, G), dtype=torch.complex128, device=dev) if want_I_eps else None
+        dw = torch.zeros(3, dtype=torch.complex128, device=dev) if want_domega else None
+    o = make_options(mem, "fp64", "auto", inp.wx_band_stride, stream=_stream_handle(inp, stream), flags=flags)
+    st = lib.bgw_noflagOCC_solver_backward(inp.number_bands, P, G, _ptr(inp.inv_igp_index), _ptr(inp.indinv),
+                                           len(inp.indinv), _ptr(inp.wx_array), _ptr(inp.wtilde_array),
+                                           _ptr(inp.aqsmtemp), _ptr(inp.aqsntemp), _ptr(inp.I_eps_array),
+                                           _ptr(inp.vcoul), _ptr(gc), _nz(gw), _nz(gi), _nz(dw), ctypes.byref(o))
+    _check("bgw_noflagOCC_solver_backward", st)
+    return gw, gi, dw
 
 
 def _ff_out(inp: FFInputs, n: int, mem: str):

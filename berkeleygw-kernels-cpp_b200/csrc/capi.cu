@@ -17,6 +17,11 @@ int gpp_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *i
                 int64_t indinv_len, const double *wx, int64_t wx_stride, const double2 *wt, const double2 *am,
                 const double2 *an, const double2 *ie, const double *vc, double *achtemp_dev);
 
+int gpp_adjoint_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *inv, const int32_t *indinv,
+                        int64_t indinv_len, const double *wx, const double2 *wt, const double2 *am,
+                        const double2 *an, const double2 *ie, const double *vc, const double2 *gcot,
+                        double2 *grad_wt, double2 *grad_ie, double *domega);
+
 }  // namespace bgw
 
 #include "ff_plan.cuh"
@@ -80,7 +85,6 @@ extern "C" int bgw_noflagOCC_solver(int64_t number_bands, int64_t ngpown, int64_
   CallEnv *env = &c.env;
   const int64_t stride = env->opt.wx_band_stride;
   if (stride != 0 && stride < 3) return BGW_ERR_INVALID_ARG;
-  if (env->opt.precision != BGW_PRECISION_FP64) return BGW_ERR_UNSUPPORTED;
   const size_t wx_n = stride == 0 ? 3 : (size_t)(nb > 0 ? (nb - 1) * stride + 3 : 3);
   const void *inv = nullptr, *ind = nullptr, *wx = nullptr, *wt = nullptr, *am = nullptr, *an = nullptr,
              *ie = nullptr, *vc = nullptr;
@@ -100,6 +104,70 @@ extern "C" int bgw_noflagOCC_solver(int64_t number_bands, int64_t ngpown, int64_
                       (const double *)vc, out));
   if (env->host) BGW_CUDA_TRY(cudaMemcpyAsync(achtemp, out, 6 * sizeof(double), cudaMemcpyDeviceToHost, env->stream));
   env->prof.flops = 63.0 * (double)nb * (double)P * (double)G;
+  return finish_call(env);
+}
+
+extern "C" int bgw_noflagOCC_solver_backward(int64_t number_bands, int64_t ngpown, int64_t ncouls,
+                                             const int32_t *inv_igp_index, const int32_t *indinv,
+                                             int64_t indinv_len, const double *wx_array, const double *wtilde_array,
+                                             const double *aqsmtemp, const double *aqsntemp,
+                                             const double *I_eps_array, const double *vcoul,
+                                             const double *grad_achtemp, double *grad_wtilde, double *grad_I_eps,
+                                             double *dachtemp_domega, const bgw_options *opt) {
+  const int64_t nb = number_bands, P = ngpown, G = ncouls;
+  if (nb < 0 || P < 0 || G <= 0 || G > INT32_MAX || nb > INT32_MAX || P > INT32_MAX) return BGW_ERR_INVALID_ARG;
+  if (!dims_ok(nb, G) || !dims_ok(P, G) || indinv_len <= 0 || indinv_len > INT32_MAX) return BGW_ERR_INVALID_ARG;
+  if (!grad_achtemp || !wx_array || !vcoul || !indinv) return BGW_ERR_INVALID_ARG;
+  if (!grad_wtilde && !grad_I_eps && !dachtemp_domega) return BGW_ERR_INVALID_ARG;
+  if (P > 0 && (!inv_igp_index || !wtilde_array || !I_eps_array)) return BGW_ERR_INVALID_ARG;
+  if (nb > 0 && P > 0 && (!aqsmtemp || !aqsntemp)) return BGW_ERR_INVALID_ARG;
+  Call c(opt);
+  if (c.st != BGW_OK) return c.st;
+  CallEnv *env = &c.env;
+  if (env->opt.wx_band_stride != 0) return BGW_ERR_UNSUPPORTED;  // factored adjoint only
+  const void *inv = nullptr, *ind = nullptr, *wx = nullptr, *wt = nullptr, *am = nullptr, *an = nullptr,
+             *ie = nullptr, *vc = nullptr, *gc = nullptr;
+  const size_t pg = (size_t)P * (size_t)G * 16, ng = (size_t)nb * (size_t)G * 16;
+  BGW_TRY(stage_input(env, SLOT_IN0, inv_igp_index, sizeof(int32_t) * (size_t)P, &inv));
+  BGW_TRY(stage_input(env, SLOT_IN1, indinv, sizeof(int32_t) * (size_t)indinv_len, &ind));
+  BGW_TRY(stage_input(env, SLOT_IN2, wx_array, sizeof(double) * 3, &wx));
+  BGW_TRY(stage_input(env, SLOT_IN3, wtilde_array, pg, &wt));
+  BGW_TRY(stage_input(env, SLOT_IN4, aqsmtemp, ng, &am));
+  BGW_TRY(stage_input(env, SLOT_IN5, aqsntemp, ng, &an));
+  BGW_TRY(stage_input(env, SLOT_IN6, I_eps_array, pg, &ie));
+  BGW_TRY(stage_input(env, SLOT_IN7, vcoul, sizeof(double) * (size_t)G, &vc));
+  BGW_TRY(stage_input(env, SLOT_IN8, grad_achtemp, sizeof(double) * 6, &gc));
+  double *d_gw = grad_wtilde, *d_gi = grad_I_eps, *d_dw = dachtemp_domega;
+  if (env->host) {
+    void *p = nullptr;
+    if (grad_wtilde) {
+      BGW_TRY(ws_reserve(env->ws, SLOT_IN9, pg, &p));
+      d_gw = static_cast<double *>(p);
+    }
+    if (grad_I_eps) {
+      BGW_TRY(ws_reserve(env->ws, SLOT_IN10, pg, &p));
+      d_gi = static_cast<double *>(p);
+    }
+    if (dachtemp_domega) {
+      BGW_TRY(ws_reserve(env->ws, SLOT_IN11, sizeof(double) * 6, &p));
+      d_dw = static_cast<double *>(p);
+    }
+  } else if (((uintptr_t)grad_wtilde | (uintptr_t)grad_I_eps) & 15u) {
+    return BGW_ERR_INVALID_ARG;
+  }
+  BGW_TRY(gpp_adjoint_enqueue(env, nb, P, G, (const int32_t *)inv, (const int32_t *)ind, indinv_len,
+                              (const double *)wx, (const double2 *)wt, (const double2 *)am, (const double2 *)an,
+                              (const double2 *)ie, (const double *)vc, (const double2 *)gc, (double2 *)d_gw,
+                              (double2 *)d_gi, d_dw));
+  if (env->host) {
+    if (grad_wtilde) BGW_CUDA_TRY(cudaMemcpyAsync(grad_wtilde, d_gw, pg, cudaMemcpyDeviceToHost, env->stream));
+    if (grad_I_eps) BGW_CUDA_TRY(cudaMemcpyAsync(grad_I_eps, d_gi, pg, cudaMemcpyDeviceToHost, env->stream));
+    if (dachtemp_domega)
+      BGW_CUDA_TRY(cudaMemcpyAsync(dachtemp_domega, d_dw, sizeof(double) * 6, cudaMemcpyDeviceToHost, env->stream));
+  }
+  // Algorithmic flops: per (G', G, frequency) element the quotient (as the
+  // forward) plus 4 complex products; 21 + 24 = 45.
+  env->prof.flops = 45.0 * 3.0 * (double)P * (double)G;
   return finish_call(env);
 }
 

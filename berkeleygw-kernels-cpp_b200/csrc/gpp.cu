@@ -21,8 +21,10 @@
 // reruns are bitwise identical.
 #include <algorithm>
 #include <cstdio>
+#include <type_traits>
 
 #include "bgw_internal.cuh"
+#include "gpp_common.cuh"
 #include "reduce.cuh"
 
 namespace bgw {
@@ -37,39 +39,6 @@ constexpr int kChunk = kThreads * kElems;  // ig per item
 // requested) = sum_n1 st[p][n1] in a fixed order.  Indices are checked: an
 // out-of-range inv_igp_index / indinv entry raises BGW_ERR_INDEX and that
 // column contributes zero (no out-of-bounds read is ever issued).
-__device__ __forceinline__ int resolve_igp(int p, const int *__restrict__ inv, const int *__restrict__ indinv,
-                                           long long indinv_len, int G, int *status) {
-  int a = inv[p];
-  if (a < 0 || (long long)a >= indinv_len) {
-    raise_status(status, BGW_ERR_INDEX, p);
-    return -1;
-  }
-  int g = indinv[a];
-  if (g < 0 || g >= G) {
-    raise_status(status, BGW_ERR_INDEX, p);
-    return -1;
-  }
-  return g;
-}
-
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-
-__device__ __forceinline__ double2 store1(const double2 *__restrict__ am, const double2 *__restrict__ an,
-                                          const double *__restrict__ vc, const double2 *__restrict__ wt, int n1,
-                                          int p, int g, int G) {
-  double2 m = am[(size_t)n1 * G + g];
-  m.y = -m.y;
-  double2 r = cmul(m, an[(size_t)n1 * G + g]);
-  r.x *= 0.5;
-  r.y *= 0.5;
-  double v = vc[g];
-  r.x *= v;
-  r.y *= v;
-  return cmul(r, wt[(size_t)p * G + g]);
-}
-
 // One warp per column p: st row (if st != nullptr) and S[p] (if S != nullptr).
 __global__ void __launch_bounds__(256) gpp_prep_kernel(int nb, int P, int G, const int *__restrict__ inv,
                                                        const int *__restrict__ indinv, long long indinv_len,
@@ -110,30 +79,61 @@ __global__ void gpp_wx_kernel(int nb, const double *__restrict__ wx, long long s
 // a frequency x:
 //   dr  = x - wr,  |wdiff|^2 = dr^2 + wi^2,
 //   conj(wdiff) * I_eps = (dr*Ir + a) + i (dr*Ii + b).
+template <typename T>
 struct Elem {
-  double wr, wi2, Ir, Ii, a, b;
+  T wr, wi2, Ir, Ii, a, b;
 };
 
-template <int BCH>
+// Elements per thread: FP64 4, mixed 8 (the FP32 quotients are cheap, so a
+// longer run per band amortises the FP64 band combination).
+template <bool MIXED>
+struct BandCfg {
+  static constexpr int kE = MIXED ? 8 : 4;
+  static constexpr int kCH = kThreads * kE;
+};
+
+template <int BCH, bool MIXED>
 struct BandSmem {
-  double2 wt[2][kChunk];
-  double2 ie[2][kChunk];
+  double2 wt[2][BandCfg<MIXED>::kCH];
+  double2 ie[2][BandCfg<MIXED>::kCH];
   double2 st[2][BCH];
   double4 wx[2][BCH];
   unsigned long long bar[2];
   double red[(kThreads / 32) * 6];
 };
 
+__device__ __forceinline__ float rcp_approx_f32(float d) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(d));
+  return y;
+}
+
+// Error-free transformation of a + b (Knuth's TwoSum, TAOCP vol. 2,
+// 4.2.2): hi + lo == a + b exactly, no ordering assumption.
+__device__ __forceinline__ void two_sum_acc(double &hi, double &lo, double b) {
+  const double s = hi + b;
+  const double bb = s - hi;
+  const double err = (hi - (s - bb)) + (b - bb);
+  hi = s;
+  lo += err;
+}
+
 // Every band reads its own frequencies from the staged wx4 rows (for the
 // reference's band-independent wx the rows repeat one triple), so each
 // (band, G', G, frequency) quotient is evaluated, as in gpp.cpp:343-390.
-template <int BCH>
-__global__ void __launch_bounds__(kThreads, 2)
+// MIXED: quotients in FP32 (rcp.approx.ftz.f32), the per-band products with
+// sch_store1 and the accumulation over bands in FP64 with TwoSum
+// compensation.
+template <int BCH, bool MIXED>
+__global__ void __launch_bounds__(kThreads, MIXED ? 1 : 2)
     gpp_bandloop_kernel(int nb, int G, long long items, int nchunks_g, const double2 *__restrict__ wtilde,
                         const double2 *__restrict__ ieps, const double2 *__restrict__ st,
                         const double4 *__restrict__ wx4, double *__restrict__ partials, int *status) {
+  constexpr int kE = BandCfg<MIXED>::kE;
+  constexpr int kCH = BandCfg<MIXED>::kCH;
+  using T = typename std::conditional<MIXED, float, double>::type;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  using Smem = BandSmem<BCH>;
+  using Smem = BandSmem<BCH, MIXED>;
   Smem &sm = *reinterpret_cast<Smem *>(smem_raw);
   const int tid = threadIdx.x;
   const int nbc = (nb + BCH - 1) / BCH;
@@ -154,8 +154,8 @@ __global__ void __launch_bounds__(kThreads, 2)
     const long long item = blockIdx.x + (j / nbc) * (long long)gridDim.x;
     const int c = (int)(j % nbc);
     const long long p = item / nchunks_g;
-    const int g0 = (int)(item % nchunks_g) * kChunk;
-    const int nvalid = min(kChunk, G - g0);
+    const int g0 = (int)(item % nchunks_g) * kCH;
+    const int nvalid = min(kCH, G - g0);
     const int b0 = c * BCH;
     const int nbv = min(BCH, nb - b0);
     const int buf = (int)(j & 1);
@@ -169,6 +169,7 @@ __global__ void __launch_bounds__(kThreads, 2)
   };
 
   double acc_r[3] = {0.0, 0.0, 0.0}, acc_i[3] = {0.0, 0.0, 0.0};
+  double lo_r[3] = {0.0, 0.0, 0.0}, lo_i[3] = {0.0, 0.0, 0.0};  // TwoSum tails (MIXED)
   bool ok = true;
   if (tid == 0 && nsteps > 0) issue(0);
 
@@ -184,54 +185,65 @@ __global__ void __launch_bounds__(kThreads, 2)
 
     const long long item = blockIdx.x + (j / nbc) * (long long)gridDim.x;
     const int c = (int)(j % nbc);
-    const int g0 = (int)(item % nchunks_g) * kChunk;
-    const int nvalid = min(kChunk, G - g0);
+    const int g0 = (int)(item % nchunks_g) * kCH;
+    const int nvalid = min(kCH, G - g0);
     const int b0 = c * BCH;
     const int nbv = min(BCH, nb - b0);
 
-    Elem e[kElems];
+    Elem<T> e[kE];
 #pragma unroll
-    for (int k = 0; k < kElems; ++k) {
+    for (int k = 0; k < kE; ++k) {
       const int idx = k * kThreads + tid;
       if (idx < nvalid) {
         double2 w = sm.wt[buf][idx], v = sm.ie[buf][idx];
-        e[k].wr = w.x;
-        e[k].wi2 = w.y * w.y;
-        e[k].Ir = v.x;
-        e[k].Ii = v.y;
-        e[k].a = -w.y * v.y;
-        e[k].b = w.y * v.x;
+        e[k].wr = (T)w.x;
+        e[k].wi2 = (T)(w.y * w.y);
+        e[k].Ir = (T)v.x;
+        e[k].Ii = (T)v.y;
+        e[k].a = (T)(-w.y * v.y);
+        e[k].b = (T)(w.y * v.x);
       } else {  // padding: contributes exactly zero, keeps |wdiff|^2 >= 1
-        e[k].wr = 0.0;
-        e[k].wi2 = 1.0;
-        e[k].Ir = e[k].Ii = e[k].a = e[k].b = 0.0;
+        e[k].wr = (T)0;
+        e[k].wi2 = (T)1;
+        e[k].Ir = e[k].Ii = e[k].a = e[k].b = (T)0;
       }
     }
 
     for (int bb = 0; bb < nbv; ++bb) {
       const double4 w4 = sm.wx[buf][bb];
-      const double x[3] = {w4.x, w4.y, w4.z};
+      const T x[3] = {(T)w4.x, (T)w4.y, (T)w4.z};
       const double2 s = sm.st[buf][bb];
-      double tr[3] = {0.0, 0.0, 0.0}, ti[3] = {0.0, 0.0, 0.0};
+      T tr[3] = {(T)0, (T)0, (T)0}, ti[3] = {(T)0, (T)0, (T)0};
 #pragma unroll
-      for (int k = 0; k < kElems; ++k) {
+      for (int k = 0; k < kE; ++k) {
 #pragma unroll
         for (int iw = 0; iw < 3; ++iw) {
-          const double dr = x[iw] - e[k].wr;
-          const double den = fma(dr, dr, e[k].wi2);
-          const double r = rcp_refined(den);
-          const double nr = fma(dr, e[k].Ir, e[k].a);
-          const double ni = fma(dr, e[k].Ii, e[k].b);
+          const T dr = x[iw] - e[k].wr;
+          const T den = fma(dr, dr, e[k].wi2);
+          T r;
+          if constexpr (MIXED) {
+            r = rcp_approx_f32(den);
+          } else {
+            r = rcp_refined(den);
+          }
+          const T nr = fma(dr, e[k].Ir, e[k].a);
+          const T ni = fma(dr, e[k].Ii, e[k].b);
           tr[iw] = fma(nr, r, tr[iw]);
           ti[iw] = fma(ni, r, ti[iw]);
         }
       }
 #pragma unroll
       for (int iw = 0; iw < 3; ++iw) {
-        acc_r[iw] = fma(tr[iw], s.x, acc_r[iw]);
-        acc_r[iw] = fma(-ti[iw], s.y, acc_r[iw]);
-        acc_i[iw] = fma(tr[iw], s.y, acc_i[iw]);
-        acc_i[iw] = fma(ti[iw], s.x, acc_i[iw]);
+        const double trd = (double)tr[iw], tid_ = (double)ti[iw];
+        if constexpr (MIXED) {
+          two_sum_acc(acc_r[iw], lo_r[iw], fma(trd, s.x, -tid_ * s.y));
+          two_sum_acc(acc_i[iw], lo_i[iw], fma(trd, s.y, tid_ * s.x));
+        } else {
+          acc_r[iw] = fma(trd, s.x, acc_r[iw]);
+          acc_r[iw] = fma(-tid_, s.y, acc_r[iw]);
+          acc_i[iw] = fma(trd, s.y, acc_i[iw]);
+          acc_i[iw] = fma(tid_, s.x, acc_i[iw]);
+        }
       }
     }
     __syncthreads();  // buffer `buf` is free for step j + 2
@@ -243,7 +255,8 @@ __global__ void __launch_bounds__(kThreads, 2)
     (void)mbar_wait_bounded(reinterpret_cast<uint64_t *>(&sm.bar[1]), 0, kWaitCycles);
   }
 
-  double v[6] = {acc_r[0], acc_i[0], acc_r[1], acc_i[1], acc_r[2], acc_i[2]};
+  double v[6] = {acc_r[0] + lo_r[0], acc_i[0] + lo_i[0], acc_r[1] + lo_r[1],
+                 acc_i[1] + lo_i[1], acc_r[2] + lo_r[2], acc_i[2] + lo_i[2]};
   block_sum<6, kThreads>(v, sm.red);
   if (tid == 0) {
 #pragma unroll
@@ -307,13 +320,15 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-template <int BCH>
-int launch_bandloop(Workspace *ws, cudaStream_t stream, int nb, int G, long long items, int nchunks_g,
-                    const double2 *wt, const double2 *ie, const double2 *st, const double4 *wx4,
-                    double **partials_out, int *grid_out, int *status) {
-  using Smem = BandSmem<BCH>;
+template <int BCH, bool MIXED>
+int launch_bandloop(Workspace *ws, cudaStream_t stream, int nb, int G, const double2 *wt, const double2 *ie,
+                    const double2 *st, const double4 *wx4, int64_t P, double **partials_out, int *grid_out,
+                    int *status) {
+  using Smem = BandSmem<BCH, MIXED>;
   const size_t smem = sizeof(Smem);
-  auto kfn = gpp_bandloop_kernel<BCH>;
+  auto kfn = gpp_bandloop_kernel<BCH, MIXED>;
+  const int nchunks_g = (int)((G + BandCfg<MIXED>::kCH - 1) / BandCfg<MIXED>::kCH);
+  const long long items = (long long)P * nchunks_g;
   BGW_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   BGW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kThreads, smem));
@@ -344,7 +359,9 @@ int gpp_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *i
   const int nchunks_g = (int)((G + kChunk - 1) / kChunk);
   const long long items = (long long)P * nchunks_g;
   const bool factored = env->opt.gpp_algorithm == BGW_GPP_FACTORED ||
-                        (env->opt.gpp_algorithm == BGW_GPP_AUTO && wx_stride == 0);
+                        (env->opt.gpp_algorithm == BGW_GPP_AUTO && wx_stride == 0 &&
+                         env->opt.precision == BGW_PRECISION_FP64);
+  if (factored && env->opt.precision == BGW_PRECISION_MIXED) return BGW_ERR_UNSUPPORTED;
   int prep_grid = (int)std::min<long long>((P + 7) / 8, (long long)ws->sm_count * 16);
   if (prep_grid < 1) prep_grid = 1;
 
@@ -390,12 +407,18 @@ int gpp_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *i
   int grid = 0;
   double *partials = nullptr;
   BGW_TRY(prof_mark(env, 1));
-  BGW_TRY((launch_bandloop<256>(ws, stream, (int)nb, (int)G, items, nchunks_g, wt, ie, (const double2 *)st,
-                                (const double4 *)wx4, &partials, &grid, env->d_status)));
+  if (env->opt.precision == BGW_PRECISION_MIXED) {
+    BGW_TRY((launch_bandloop<256, true>(ws, stream, (int)nb, (int)G, wt, ie, (const double2 *)st,
+                                        (const double4 *)wx4, P, &partials, &grid, env->d_status)));
+  } else {
+    BGW_TRY((launch_bandloop<256, false>(ws, stream, (int)nb, (int)G, wt, ie, (const double2 *)st,
+                                         (const double4 *)wx4, P, &partials, &grid, env->d_status)));
+  }
   BGW_TRY(prof_mark(env, 2));
   env->prof.main_bytes = 32.0 * (double)P * (double)G + 16.0 * (double)P * (double)nb + 32.0 * (double)nb;
   env->prof.main_launches = 1;
-  std::snprintf(env->prof.main_kernel, sizeof(env->prof.main_kernel), "gpp_bandloop_kernel");
+  std::snprintf(env->prof.main_kernel, sizeof(env->prof.main_kernel),
+                env->opt.precision == BGW_PRECISION_MIXED ? "gpp_bandloop_kernel<mixed>" : "gpp_bandloop_kernel");
   reduce_partials_kernel<6><<<1, 256, 0, stream>>>(partials, grid, achtemp_dev);
   count_launch();
   BGW_CUDA_TRY(cudaGetLastError());

@@ -1,0 +1,201 @@
+// gpp_adjoint.cu -- analytic adjoint of the GPP sum (noflagOCC_solver,
+// GPP/gpp.cpp:307-402) on sm_100a, FP64.
+//
+// With q = conj(d) / |d|^2 = 1 / d, d = wx[iw] - wtilde[p][ig] (gpp.cpp:374-378),
+//   Sigma_iw = sum_p S(p) T(p, iw),  T(p, iw) = sum_ig I_eps[p][ig] q_iw(p, ig),
+//   S(p) = C(p) wtilde[p][igp],      C(p) = sum_n1 conj(aqsm[n1][igp]) aqsn[n1][igp] 0.5 vcoul[igp].
+// Sigma is holomorphic in wtilde and I_eps, so for a real loss
+// L = sum_iw Re(conj(G_iw) Sigma_iw)  (G_iw = dL/dRe Sigma_iw + i dL/dIm Sigma_iw)
+// the complex gradient dL/dRe z + i dL/dIm z equals sum_iw G_iw conj(dSigma_iw/dz):
+//   dSigma_iw/dI_eps[p][ig]  = S(p) q_iw
+//   dSigma_iw/dwtilde[p][ig] = S(p) I_eps[p][ig] q_iw^2   (+ C(p) T(p, iw) at ig = igp)
+//   dSigma_iw/domega         = - sum_{p, ig} S(p) I_eps[p][ig] q_iw^2
+// The quotients are recomputed (nothing of size bands x G' x G is stored).
+// This is the factored form: valid for the reference's band-independent wx.
+//
+// One CTA streams whole G' rows (round robin): it writes both gradient rows,
+// reduces T(p, .) over the row with a fixed-order block sum and adds the
+// sch_store1 term at (p, igp) itself, so no second pass over the row is
+// needed.  dSigma/domega is reduced per CTA, then in a fixed order.
+#include <algorithm>
+#include <cstdio>
+
+#include "bgw_internal.cuh"
+#include "gpp_common.cuh"
+#include "reduce.cuh"
+
+namespace bgw {
+namespace {
+
+constexpr int kAdjThreads = 256;
+constexpr int kAdjElems = 4;
+
+// C(p), S(p) = C(p) wtilde[p][igp] and igp(p) (-1 if out of range).  One
+// warp per column, fixed-order band sum.
+__global__ void __launch_bounds__(256)
+    gpp_adjoint_prep_kernel(int nb, int P, int G, const int *__restrict__ inv, const int *__restrict__ indinv,
+                            long long indinv_len, const double2 *__restrict__ wt, const double2 *__restrict__ am,
+                            const double2 *__restrict__ an, const double *__restrict__ vc, double2 *__restrict__ Cp,
+                            double2 *__restrict__ Sp, int *__restrict__ igp_out, int *status) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < P; p += warps) {
+    const int g = resolve_igp(p, inv, indinv, indinv_len, G, status);
+    double cr = 0.0, ci = 0.0;
+    if (g >= 0) {
+      for (int n1 = lane; n1 < nb; n1 += 32) {
+        double2 m = am[(size_t)n1 * G + g];
+        m.y = -m.y;
+        double2 r = cmul(m, an[(size_t)n1 * G + g]);
+        const double v = 0.5 * vc[g];
+        cr += r.x * v;
+        ci += r.y * v;
+      }
+    }
+    cr = warp_sum(cr);
+    ci = warp_sum(ci);
+    if (lane == 0) {
+      const double2 c = make_double2(cr, ci);
+      Cp[p] = c;
+      Sp[p] = g >= 0 ? cmul(c, wt[(size_t)p * G + g]) : make_double2(0.0, 0.0);
+      igp_out[p] = g;
+    }
+  }
+}
+
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+
+// grad_wt / grad_ie may be null (not requested).  partials: 6 doubles per
+// CTA (dSigma_iw/domega, re/im).
+__global__ void __launch_bounds__(kAdjThreads)
+    gpp_adjoint_kernel(int P, int G, const double2 *__restrict__ wtilde, const double2 *__restrict__ ieps,
+                       const double2 *__restrict__ Cp, const double2 *__restrict__ Sp, const int *__restrict__ igp,
+                       const double *__restrict__ wx3, const double2 *__restrict__ gcot,
+                       double2 *__restrict__ grad_wt, double2 *__restrict__ grad_ie, double *__restrict__ partials) {
+  __shared__ double red[(kAdjThreads / 32) * 6];
+  const int tid = threadIdx.x;
+  const double x[3] = {wx3[0], wx3[1], wx3[2]};
+  // conj(G_iw): the cotangents enter as sum_iw conj(G_iw) dSigma_iw/dz.
+  const double2 cg[3] = {cconj(gcot[0]), cconj(gcot[1]), cconj(gcot[2])};
+  double dw_r[3] = {0.0, 0.0, 0.0}, dw_i[3] = {0.0, 0.0, 0.0};  // sum S I q^2 (sign applied at the end)
+  for (int p = blockIdx.x; p < P; p += gridDim.x) {
+    const double2 S = Sp[p];
+    double t_r[3] = {0.0, 0.0, 0.0}, t_i[3] = {0.0, 0.0, 0.0};   // T(p, iw)
+    double u_r[3] = {0.0, 0.0, 0.0}, u_i[3] = {0.0, 0.0, 0.0};   // sum_ig I q^2 (this thread)
+    for (int g0 = 0; g0 < G; g0 += kAdjThreads * kAdjElems) {
+      double2 w[kAdjElems], v[kAdjElems];
+#pragma unroll
+      for (int k = 0; k < kAdjElems; ++k) {
+        const int ig = g0 + k * kAdjThreads + tid;
+        if (ig < G) {
+          w[k] = __ldcs(wtilde + (size_t)p * G + ig);
+          v[k] = __ldcs(ieps + (size_t)p * G + ig);
+        } else {
+          w[k] = make_double2(0.0, 1.0);
+          v[k] = make_double2(0.0, 0.0);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kAdjElems; ++k) {
+        const int ig = g0 + k * kAdjThreads + tid;
+        double2 hI = make_double2(0.0, 0.0), hW = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int iw = 0; iw < 3; ++iw) {
+          const double dr = x[iw] - w[k].x;
+          const double r = rcp_refined(fma(dr, dr, w[k].y * w[k].y));
+          const double2 q = make_double2(dr * r, w[k].y * r);         // 1 / (x - w)
+          const double2 iq = cmul(v[k], q);                            // I q
+          const double2 iq2 = cmul(iq, q);                             // I q^2
+          t_r[iw] += iq.x;
+          t_i[iw] += iq.y;
+          u_r[iw] += iq2.x;
+          u_i[iw] += iq2.y;
+          hI = cadd(hI, cmul(cg[iw], q));
+          hW = cadd(hW, cmul(cg[iw], iq2));
+        }
+        if (ig < G) {
+          // grad = conj(sum_iw conj(G_iw) dSigma_iw/dz)
+          if (grad_ie) grad_ie[(size_t)p * G + ig] = cconj(cmul(S, hI));
+          if (grad_wt) grad_wt[(size_t)p * G + ig] = cconj(cmul(S, hW));
+        }
+      }
+    }
+#pragma unroll
+    for (int iw = 0; iw < 3; ++iw) {
+      const double2 su = cmul(S, make_double2(u_r[iw], u_i[iw]));
+      dw_r[iw] += su.x;
+      dw_i[iw] += su.y;
+    }
+    // T(p, .) over the whole row, then the sch_store1 term at (p, igp):
+    // dSigma_iw/dwtilde[p][igp] += C(p) T(p, iw).
+    double tv[6] = {t_r[0], t_i[0], t_r[1], t_i[1], t_r[2], t_i[2]};
+    block_sum<6, kAdjThreads>(tv, red);
+    if (tid == 0 && grad_wt) {
+      const int g = igp[p];
+      if (g >= 0) {
+        double2 h = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int iw = 0; iw < 3; ++iw) h = cadd(h, cmul(cg[iw], make_double2(tv[2 * iw], tv[2 * iw + 1])));
+        const double2 add = cconj(cmul(Cp[p], h));
+        double2 cur = grad_wt[(size_t)p * G + g];
+        grad_wt[(size_t)p * G + g] = cadd(cur, add);
+      }
+    }
+    __syncthreads();
+  }
+  double vv[6] = {-dw_r[0], -dw_i[0], -dw_r[1], -dw_i[1], -dw_r[2], -dw_i[2]};
+  block_sum<6, kAdjThreads>(vv, red);
+  if (tid == 0) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) partials[(size_t)blockIdx.x * 6 + k] = vv[k];
+  }
+}
+
+}  // namespace
+
+// Enqueues the adjoint.  Device pointers; gcot: 3 complex cotangents;
+// grad_wt / grad_ie / domega may be null.
+int gpp_adjoint_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *inv, const int32_t *indinv,
+                        int64_t indinv_len, const double *wx, const double2 *wt, const double2 *am,
+                        const double2 *an, const double2 *ie, const double *vc, const double2 *gcot,
+                        double2 *grad_wt, double2 *grad_ie, double *domega) {
+  Workspace *ws = env->ws;
+  cudaStream_t stream = env->stream;
+  void *tab = nullptr, *partials = nullptr, *scratch_out = nullptr;
+  const size_t np = (size_t)std::max<int64_t>(P, 1);
+  // C[P] | S[P] (double2) | igp[P] (int)
+  BGW_TRY(ws_reserve(ws, SLOT_TABLE0, np * (2 * sizeof(double2) + sizeof(int)), &tab));
+  double2 *Cp = static_cast<double2 *>(tab);
+  double2 *Sp = Cp + np;
+  int *igp = reinterpret_cast<int *>(Sp + np);
+  int prep_grid = (int)std::min<long long>((P + 7) / 8, (long long)ws->sm_count * 16);
+  gpp_adjoint_prep_kernel<<<std::max(prep_grid, 1), 256, 0, stream>>>((int)nb, (int)P, (int)G, inv, indinv,
+                                                                       indinv_len, wt, am, an, vc, Cp, Sp, igp,
+                                                                       env->d_status);
+  count_launch();
+  BGW_CUDA_TRY(cudaGetLastError());
+  int per_sm = 0;
+  BGW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gpp_adjoint_kernel, kAdjThreads, 0));
+  int grid = (int)std::min<long long>(std::max<int64_t>(P, 1), (long long)ws->sm_count * std::max(per_sm, 1));
+  BGW_TRY(ws_reserve(ws, SLOT_PARTIALS, sizeof(double) * 6 * (size_t)grid, &partials));
+  if (!domega) {
+    BGW_TRY(ws_reserve(ws, SLOT_OUT, sizeof(double) * 6, &scratch_out));
+    domega = static_cast<double *>(scratch_out);
+  }
+  BGW_TRY(prof_mark(env, 1));
+  gpp_adjoint_kernel<<<grid, kAdjThreads, 0, stream>>>((int)P, (int)G, wt, ie, Cp, Sp, igp, wx, gcot, grad_wt,
+                                                       grad_ie, (double *)partials);
+  count_launch();
+  BGW_CUDA_TRY(cudaGetLastError());
+  BGW_TRY(prof_mark(env, 2));
+  env->prof.main_launches = 1;
+  env->prof.main_bytes = 32.0 * (double)P * (double)G * (1.0 + (grad_wt ? 0.5 : 0.0) + (grad_ie ? 0.5 : 0.0));
+  std::snprintf(env->prof.main_kernel, sizeof(env->prof.main_kernel), "gpp_adjoint_kernel");
+  reduce_partials_kernel<6><<<1, 256, 0, stream>>>((const double *)partials, grid, domega);
+  count_launch();
+  BGW_CUDA_TRY(cudaGetLastError());
+  return BGW_OK;
+}
+
+}  // namespace bgw

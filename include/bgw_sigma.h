@@ -106,6 +106,34 @@ int bgw_noflagOCC_solver(int64_t number_bands, int64_t ngpown, int64_t ncouls,
                          const double *vcoul, double *achtemp,
                          const bgw_options *opt);
 
+/* ---------------------------------------------------------- GPP adjoint --
+ * Analytic adjoint of bgw_noflagOCC_solver (no counterpart in the
+ * reference, whose quasiparticle renormalisation uses the three-point finite
+ * difference over wx_array, GPP/gpp.cpp:271-275).  With q = 1/(wx - wtilde)
+ * Sigma is holomorphic in wtilde and I_eps; for cotangents
+ *   grad_achtemp[iw] = dL/dRe achtemp[iw] + i dL/dIm achtemp[iw]  (3 complex)
+ * it returns the complex gradients dL/dRe z + i dL/dIm z:
+ *   grad_wtilde [ngpown][ncouls] complex (includes wtilde[p][igp] inside
+ *                                         sch_store1), may be NULL
+ *   grad_I_eps  [ngpown][ncouls] complex, may be NULL
+ *   dachtemp_domega [3] complex: d achtemp[iw] / d wx[iw], may be NULL
+ * Quotients are recomputed, nothing of size bands x G' x G is stored.
+ * Requires the band-independent wx (wx_band_stride 0).  Same arguments as
+ * the forward otherwise. */
+int bgw_noflagOCC_solver_backward(int64_t number_bands, int64_t ngpown,
+                                  int64_t ncouls, const int32_t *inv_igp_index,
+                                  const int32_t *indinv, int64_t indinv_len,
+                                  const double *wx_array,
+                                  const double *wtilde_array,
+                                  const double *aqsmtemp,
+                                  const double *aqsntemp,
+                                  const double *I_eps_array,
+                                  const double *vcoul,
+                                  const double *grad_achtemp,
+                                  double *grad_wtilde, double *grad_I_eps,
+                                  double *dachtemp_domega,
+                                  const bgw_options *opt);
+
 /* --------------------------------------------------- GPP, no allocation --
  * No counterpart in the reference.  A variant of bgw_noflagOCC_solver for
  * callers that cannot allocate GPU memory: code whose device memory is all

@@ -13,6 +13,9 @@
  *   - FF   achsDtemp_Kernel             FF/ff.cpp:171-209
  *   - FF   asxDtemp_Kernel (+ssxDittt)  FF/ff.cpp:154-169, 211-293
  *   - FF   achDtemp_cor_Kernel (+schDttt_corKernel1/2)  FF/ff.cpp:295-451
+ * and the analytic gradient of the GPP sum (orc_gpp_backward), which the
+ * reference does not have; that gradient is pinned by central finite
+ * differences of the long-double forward (tests/test_adjoint.py).
  *
  * Every sum is accumulated in long double and combined in a fixed order, so
  * the result does not depend on the OpenMP thread count.  The oracle is
@@ -403,6 +406,150 @@ int orc_ff_cor(long nb, long nvband, long nfreqeval, long G, long P,
     out[2 * iw] = (double)tr;
     out[2 * iw + 1] = (double)ti;
   }
+  free(igp); free(part);
+  return 0;
+}
+
+/* ------------------------------------------------------------ GPP adjoint --
+ * Long-double reference gradient of the GPP sum for a band-independent wx.
+ * With q = 1/(wx - wtilde) (= conj(wdiff)/|wdiff|^2, gpp.cpp:374-378) the
+ * sum is holomorphic in wtilde and I_eps; for cotangents G_iw (gcot: 3
+ * complex) the complex gradient of L = sum_iw Re(conj(G_iw) Sigma_iw) is
+ * sum_iw G_iw conj(dSigma_iw/dz), with
+ *   dSigma/dI_eps[p][ig]  = S(p) q,   dSigma/dwtilde[p][ig] = S(p) I_eps q^2,
+ *   plus C(p) T(p) at ig = igp(p) (wtilde[p][igp] inside sch_store1),
+ *   dSigma_iw/dwx = - sum S(p) I_eps q^2.
+ * grad_wt / grad_ie: [P][G] complex or NULL; domega: 3 complex or NULL. */
+int orc_gpp_backward(long nb, long P, long G, const int *inv_igp_index,
+                     const int *indinv, long indinv_len, const double *wx,
+                     const double *wtilde, const double *aqsm,
+                     const double *aqsn, const double *I_eps,
+                     const double *vcoul, const double *gcot,
+                     double *grad_wt, double *grad_ie, double *domega) {
+  if (nb < 0 || P < 0 || G <= 0) return -1;
+  long *igp = (long *)malloc(sizeof(long) * (size_t)(P > 0 ? P : 1));
+  ld *part = (ld *)calloc((size_t)(P > 0 ? P : 1) * 6, sizeof(ld));
+  if (!igp || !part) { free(igp); free(part); return -1; }
+  if (resolve_igp(P, G, inv_igp_index, indinv, indinv_len, igp)) {
+    free(igp); free(part); return -1;
+  }
+  /* conj(G_iw) */
+  ld cgr[3], cgi[3];
+  for (int iw = 0; iw < 3; ++iw) { cgr[iw] = gcot[2 * iw]; cgi[iw] = -(ld)gcot[2 * iw + 1]; }
+#pragma omp parallel for schedule(dynamic, 4)
+  for (long p = 0; p < P; ++p) {
+    long g = igp[p];
+    ld Cr = 0, Ci = 0;
+    for (long n1 = 0; n1 < nb; ++n1) {
+      ld ar = aqsm[2 * (n1 * G + g)], ai = -(ld)aqsm[2 * (n1 * G + g) + 1];
+      ld br = aqsn[2 * (n1 * G + g)], bi = aqsn[2 * (n1 * G + g) + 1];
+      ld v = 0.5L * (ld)vcoul[g];
+      Cr += (ar * br - ai * bi) * v;
+      Ci += (ar * bi + ai * br) * v;
+    }
+    ld wgr = wtilde[2 * (p * G + g)], wgi = wtilde[2 * (p * G + g) + 1];
+    ld Sr = Cr * wgr - Ci * wgi, Si = Cr * wgi + Ci * wgr;
+    ld Tr[3] = {0, 0, 0}, Ti[3] = {0, 0, 0}, Ur[3] = {0, 0, 0}, Ui[3] = {0, 0, 0};
+    for (long ig = 0; ig < G; ++ig) {
+      ld wr = wtilde[2 * (p * G + ig)], wi = wtilde[2 * (p * G + ig) + 1];
+      ld er = I_eps[2 * (p * G + ig)], ei = I_eps[2 * (p * G + ig) + 1];
+      ld hIr = 0, hIi = 0, hWr = 0, hWi = 0;
+      for (int iw = 0; iw < 3; ++iw) {
+        ld dr = (ld)wx[iw] - wr, di = -wi;          /* d = wx - w        */
+        ld den = dr * dr + di * di;
+        ld qr = dr / den, qi = -di / den;           /* q = 1/d           */
+        ld iqr = er * qr - ei * qi, iqi = er * qi + ei * qr;       /* I q   */
+        ld q2r = iqr * qr - iqi * qi, q2i = iqr * qi + iqi * qr;   /* I q^2 */
+        Tr[iw] += iqr; Ti[iw] += iqi;
+        Ur[iw] += q2r; Ui[iw] += q2i;
+        hIr += cgr[iw] * qr - cgi[iw] * qi;  hIi += cgr[iw] * qi + cgi[iw] * qr;
+        hWr += cgr[iw] * q2r - cgi[iw] * q2i; hWi += cgr[iw] * q2i + cgi[iw] * q2r;
+      }
+      if (grad_ie) {  /* conj(S hI) */
+        grad_ie[2 * (p * G + ig)] = (double)(Sr * hIr - Si * hIi);
+        grad_ie[2 * (p * G + ig) + 1] = (double)(-(Sr * hIi + Si * hIr));
+      }
+      if (grad_wt) {  /* the (p, igp) entry is redone below with both terms */
+        ld xr = Sr * hWr - Si * hWi, xi = Sr * hWi + Si * hWr;
+        grad_wt[2 * (p * G + ig)] = (double)xr;
+        grad_wt[2 * (p * G + ig) + 1] = (double)(-xi);
+      }
+    }
+    if (grad_wt) {
+      /* recompute the (p, igp) entry in long double with both terms */
+      ld wr = wgr, wi = wgi;
+      ld er = I_eps[2 * (p * G + g)], ei = I_eps[2 * (p * G + g) + 1];
+      ld hWr = 0, hWi = 0, hCr = 0, hCi = 0;
+      for (int iw = 0; iw < 3; ++iw) {
+        ld dr = (ld)wx[iw] - wr, di = -wi;
+        ld den = dr * dr + di * di;
+        ld qr = dr / den, qi = -di / den;
+        ld iqr = er * qr - ei * qi, iqi = er * qi + ei * qr;
+        ld q2r = iqr * qr - iqi * qi, q2i = iqr * qi + iqi * qr;
+        hWr += cgr[iw] * q2r - cgi[iw] * q2i; hWi += cgr[iw] * q2i + cgi[iw] * q2r;
+        hCr += cgr[iw] * Tr[iw] - cgi[iw] * Ti[iw]; hCi += cgr[iw] * Ti[iw] + cgi[iw] * Tr[iw];
+      }
+      ld xr = (Sr * hWr - Si * hWi) + (Cr * hCr - Ci * hCi);
+      ld xi = (Sr * hWi + Si * hWr) + (Cr * hCi + Ci * hCr);
+      grad_wt[2 * (p * G + g)] = (double)xr;
+      grad_wt[2 * (p * G + g) + 1] = (double)(-xi);
+    }
+    for (int iw = 0; iw < 3; ++iw) {
+      part[6 * p + 2 * iw] = -(Sr * Ur[iw] - Si * Ui[iw]);
+      part[6 * p + 2 * iw + 1] = -(Sr * Ui[iw] + Si * Ur[iw]);
+    }
+  }
+  if (domega) {
+    ld tot[6] = {0, 0, 0, 0, 0, 0};
+    for (long p = 0; p < P; ++p)
+      for (int k = 0; k < 6; ++k) tot[k] += part[6 * p + k];
+    for (int k = 0; k < 6; ++k) domega[k] = (double)tot[k];
+  }
+  free(igp); free(part);
+  return 0;
+}
+
+/* orc_gpp_factored with long-double outputs (6 values), for finite
+ * differences whose step is far below double resolution of the sum. */
+int orc_gpp_factored_ld(long nb, long P, long G, const int *inv_igp_index,
+                        const int *indinv, long indinv_len, const double *wx,
+                        const double *wtilde, const double *aqsm,
+                        const double *aqsn, const double *I_eps,
+                        const double *vcoul, long double *achtemp) {
+  if (nb < 0 || P < 0 || G <= 0) return -1;
+  long *igp = (long *)malloc(sizeof(long) * (size_t)(P > 0 ? P : 1));
+  ld *part = (ld *)calloc((size_t)(P > 0 ? P : 1) * 6, sizeof(ld));
+  if (!igp || !part) { free(igp); free(part); return -1; }
+  if (resolve_igp(P, G, inv_igp_index, indinv, indinv_len, igp)) {
+    free(igp); free(part); return -1;
+  }
+#pragma omp parallel for schedule(dynamic, 4)
+  for (long p = 0; p < P; ++p) {
+    long g = igp[p];
+    ld Sr = 0, Si = 0;
+    for (long n1 = 0; n1 < nb; ++n1) {
+      ld sr, si;
+      gpp_store1(aqsm + 2 * (n1 * G + g), aqsn + 2 * (n1 * G + g), vcoul[g],
+                 wtilde + 2 * (p * G + g), &sr, &si);
+      Sr += sr; Si += si;
+    }
+    ld T[6] = {0, 0, 0, 0, 0, 0};
+    for (long ig = 0; ig < G; ++ig) {
+      for (int iw = 0; iw < 3; ++iw) {
+        ld qr, qi;
+        gpp_quot(wx[iw], wtilde + 2 * (p * G + ig), I_eps + 2 * (p * G + ig), &qr, &qi);
+        T[2 * iw] += qr;
+        T[2 * iw + 1] += qi;
+      }
+    }
+    for (int iw = 0; iw < 3; ++iw) {
+      part[6 * p + 2 * iw] = T[2 * iw] * Sr - T[2 * iw + 1] * Si;
+      part[6 * p + 2 * iw + 1] = T[2 * iw] * Si + T[2 * iw + 1] * Sr;
+    }
+  }
+  for (int k = 0; k < 6; ++k) achtemp[k] = 0;
+  for (long p = 0; p < P; ++p)
+    for (int k = 0; k < 6; ++k) achtemp[k] += part[6 * p + k];
   free(igp); free(part);
   return 0;
 }

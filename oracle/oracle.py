@@ -54,6 +54,8 @@ class Oracle:
         lib.orc_compute_fact.argtypes = [_D, ctypes.c_int, _P, ctypes.c_int, ctypes.c_int,
                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(_D), ctypes.POINTER(_D)]
         lib.orc_compute_fact.restype = None
+        lib.orc_gpp_backward.argtypes = [_L, _L, _L, _P, _P, _L, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]
+        lib.orc_gpp_factored_ld.argtypes = [_L, _L, _L, _P, _P, _L, _P, _P, _P, _P, _P, _P, _P]
         lib.orc_ff_achs.argtypes = [_L, _L, _L, _L, _P, _P, _L, _P, _P, _P, _P, _P]
         lib.orc_ff_asx.argtypes = [_L, _L, _L, _L, _L, _D, _D, _D, _P, _P, _P, _P, _L, _P, _P, _P, _P, _P, _P]
         lib.orc_ff_cor.argtypes = [_L, _L, _L, _L, _L, _L, _D, _D, _P, _P, _P, _P, _L, _P, _P, _P, _P, _P, _P]
@@ -73,6 +75,30 @@ class Oracle:
         if st != 0:
             raise ValueError("oracle rejected the GPP inputs")
         return out
+
+    def gpp_ld(self, g) -> np.ndarray:
+        """Factored GPP sum with long-double outputs: 6 np.longdouble (re, im per iw)."""
+        out = np.zeros(6, dtype=np.longdouble)
+        st = self.lib.orc_gpp_factored_ld(g.number_bands, g.ngpown, g.ncouls, _p(g.inv_igp_index), _p(g.indinv),
+                                          len(g.indinv), _p(g.wx_array), _p(g.wtilde_array), _p(g.aqsmtemp),
+                                          _p(g.aqsntemp), _p(g.I_eps_array), _p(g.vcoul), out.ctypes.data)
+        if st != 0:
+            raise ValueError("oracle rejected the GPP inputs")
+        return out
+
+    def gpp_backward(self, g, gcot):
+        """(grad_wtilde [P][G], grad_I_eps [P][G], dachtemp/domega [3]) complex128."""
+        gc = np.ascontiguousarray(np.asarray(gcot, dtype=np.complex128).reshape(3))
+        gw = np.zeros((g.ngpown, g.ncouls), np.complex128)
+        gi = np.zeros((g.ngpown, g.ncouls), np.complex128)
+        dw = np.zeros(3, np.complex128)
+        st = self.lib.orc_gpp_backward(g.number_bands, g.ngpown, g.ncouls, _p(g.inv_igp_index), _p(g.indinv),
+                                       len(g.indinv), _p(g.wx_array), _p(g.wtilde_array), _p(g.aqsmtemp),
+                                       _p(g.aqsntemp), _p(g.I_eps_array), _p(g.vcoul), _p(gc), _p(gw), _p(gi),
+                                       _p(dw))
+        if st != 0:
+            raise ValueError("oracle rejected the GPP inputs")
+        return gw, gi, dw
 
     def compute_fact(self, wx: float, grid: np.ndarray, loop: int, flag_occ: bool):
         i, f1, f2 = ctypes.c_int(0), _D(0.0), _D(0.0)

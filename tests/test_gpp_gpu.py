@@ -132,3 +132,33 @@ def test_ctypes_invalid_option_struct(bgw, cuda):
                                          p(g.wtilde_array), p(g.aqsmtemp), p(g.aqsntemp), p(g.I_eps_array),
                                          p(g.vcoul), p(out), ctypes.byref(o))
     assert st == -1
+
+
+# Mixed precision: FP32 per-term quotients, TwoSum-compensated FP64
+# accumulation.  Tolerance: the FP32 quotient rounding (~2^-24 per term)
+# propagates into the sum; 2e-6 relative is the bar written here.
+MIXED_RTOL = 2e-6
+
+
+@pytest.mark.parametrize("name", ["gpp_small_seeded", "gpp_ragged", "gpp_many_bands", "gpp_small_uniform"])
+def test_mixed_precision_golden(bgw, golden, cuda, name):
+    g = GPP_CASES[name]()
+    got = bgw.noflagOCC_solver(g, precision="mixed")
+    assert rel_err(got, l2c(golden["gpp"][name]["reference"])) < MIXED_RTOL
+
+
+def test_mixed_precision_band_dependent_wx(bgw, oracle, cuda):
+    g = I.gpp_seeded(40, 2, 1500, 15, seed=17, wx_per_band=True)
+    assert rel_err(bgw.noflagOCC_solver(g, precision="mixed"), oracle.gpp(g)) < MIXED_RTOL
+
+
+def test_mixed_precision_factored_unsupported(bgw, cuda):
+    with pytest.raises(bgw.BgwError) as e:
+        bgw.noflagOCC_solver(I.gpp_seeded(4, 2, 256, 16), precision="mixed", algorithm="factored")
+    assert e.value.status == -7
+
+
+def test_mixed_precision_benchmark_size(bgw, oracle, cuda):
+    g = I.gpp_seeded(512, 2, 32768, 20, seed=1234)
+    got = bgw.noflagOCC_solver(bgw.to_device(g, cuda), precision="mixed").cpu().numpy()
+    assert rel_err(got, oracle.gpp(g, factored=True)) < MIXED_RTOL
