@@ -78,6 +78,9 @@ struct Workspace {
   size_t cap[SLOT_COUNT] = {};
   cudaEvent_t last_use = nullptr;
   cudaEvent_t prof[4] = {};  // call start, main start, main stop, call stop
+  cudaStream_t copy_stream = nullptr;  // host-input staging (non-blocking)
+  cudaEvent_t copy_start = nullptr;
+  cudaEvent_t chunk_ready[16] = {};
   int sm_count = 0;
   int device = -1;
 };
@@ -89,6 +92,8 @@ int ws_reserve(Workspace *ws, int s, size_t bytes, void **out);
 // Makes `stream` wait for the previous user of the workspace, and records
 // this call as the new last user (call after enqueuing).
 int ws_acquire(Workspace *ws, cudaStream_t stream);
+// The workspace's copy stream and its events (created on first use).
+int ws_copy_stream(Workspace *ws, cudaStream_t *out);
 int ws_release(Workspace *ws, cudaStream_t stream);
 
 // ------------------------------------------------------ call environment --

@@ -16,6 +16,9 @@ struct FFPlan;
 int gpp_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *inv, const int32_t *indinv,
                 int64_t indinv_len, const double *wx, int64_t wx_stride, const double2 *wt, const double2 *am,
                 const double2 *an, const double2 *ie, const double *vc, double *achtemp_dev);
+int gpp_run_host(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *inv, const int32_t *indinv,
+                 int64_t indinv_len, const double *wx, size_t wx_n, int64_t wx_stride, const double *wt,
+                 const double *am, const double *an, const double *ie, const double *vc, double *achtemp_dev);
 
 int gpp_adjoint_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *inv, const int32_t *indinv,
                         int64_t indinv_len, const double *wx, const double2 *wt, const double2 *am,
@@ -86,22 +89,29 @@ extern "C" int bgw_noflagOCC_solver(int64_t number_bands, int64_t ngpown, int64_
   const int64_t stride = env->opt.wx_band_stride;
   if (stride != 0 && stride < 3) return BGW_ERR_INVALID_ARG;
   const size_t wx_n = stride == 0 ? 3 : (size_t)(nb > 0 ? (nb - 1) * stride + 3 : 3);
-  const void *inv = nullptr, *ind = nullptr, *wx = nullptr, *wt = nullptr, *am = nullptr, *an = nullptr,
-             *ie = nullptr, *vc = nullptr;
-  const size_t pg = (size_t)P * (size_t)G * 16, ng = (size_t)nb * (size_t)G * 16;
-  BGW_TRY(stage_input(env, SLOT_IN0, inv_igp_index, sizeof(int32_t) * (size_t)P, &inv));
-  BGW_TRY(stage_input(env, SLOT_IN1, indinv, sizeof(int32_t) * (size_t)indinv_len, &ind));
-  BGW_TRY(stage_input(env, SLOT_IN2, wx_array, sizeof(double) * wx_n, &wx));
-  BGW_TRY(stage_input(env, SLOT_IN3, wtilde_array, pg, &wt));
-  BGW_TRY(stage_input(env, SLOT_IN4, aqsmtemp, ng, &am));
-  BGW_TRY(stage_input(env, SLOT_IN5, aqsntemp, ng, &an));
-  BGW_TRY(stage_input(env, SLOT_IN6, I_eps_array, pg, &ie));
-  BGW_TRY(stage_input(env, SLOT_IN7, vcoul, sizeof(double) * (size_t)G, &vc));
   double *out = nullptr;
   BGW_TRY(out_buffer(env, achtemp, 6 * sizeof(double), &out));
-  BGW_TRY(gpp_enqueue(env, nb, P, G, (const int32_t *)inv, (const int32_t *)ind, indinv_len, (const double *)wx,
-                      stride, (const double2 *)wt, (const double2 *)am, (const double2 *)an, (const double2 *)ie,
-                      (const double *)vc, out));
+  if (env->host) {
+    // Host inputs: staged in G'-row chunks on a copy stream, overlapped with
+    // the per-chunk kernels.
+    BGW_TRY(gpp_run_host(env, nb, P, G, inv_igp_index, indinv, indinv_len, wx_array, wx_n, stride, wtilde_array,
+                         aqsmtemp, aqsntemp, I_eps_array, vcoul, out));
+  } else {
+    const void *inv = nullptr, *ind = nullptr, *wx = nullptr, *wt = nullptr, *am = nullptr, *an = nullptr,
+               *ie = nullptr, *vc = nullptr;
+    const size_t pg = (size_t)P * (size_t)G * 16, ng = (size_t)nb * (size_t)G * 16;
+    BGW_TRY(stage_input(env, SLOT_IN0, inv_igp_index, sizeof(int32_t) * (size_t)P, &inv));
+    BGW_TRY(stage_input(env, SLOT_IN1, indinv, sizeof(int32_t) * (size_t)indinv_len, &ind));
+    BGW_TRY(stage_input(env, SLOT_IN2, wx_array, sizeof(double) * wx_n, &wx));
+    BGW_TRY(stage_input(env, SLOT_IN3, wtilde_array, pg, &wt));
+    BGW_TRY(stage_input(env, SLOT_IN4, aqsmtemp, ng, &am));
+    BGW_TRY(stage_input(env, SLOT_IN5, aqsntemp, ng, &an));
+    BGW_TRY(stage_input(env, SLOT_IN6, I_eps_array, pg, &ie));
+    BGW_TRY(stage_input(env, SLOT_IN7, vcoul, sizeof(double) * (size_t)G, &vc));
+    BGW_TRY(gpp_enqueue(env, nb, P, G, (const int32_t *)inv, (const int32_t *)ind, indinv_len, (const double *)wx,
+                        stride, (const double2 *)wt, (const double2 *)am, (const double2 *)an, (const double2 *)ie,
+                        (const double *)vc, out));
+  }
   if (env->host) BGW_CUDA_TRY(cudaMemcpyAsync(achtemp, out, 6 * sizeof(double), cudaMemcpyDeviceToHost, env->stream));
   env->prof.flops = 63.0 * (double)nb * (double)P * (double)G;
   return finish_call(env);

@@ -21,6 +21,7 @@
 // reruns are bitwise identical.
 #include <algorithm>
 #include <cstdio>
+#include <functional>
 #include <type_traits>
 
 #include "bgw_internal.cuh"
@@ -321,26 +322,30 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 template <int BCH, bool MIXED>
-int launch_bandloop(Workspace *ws, cudaStream_t stream, int nb, int G, const double2 *wt, const double2 *ie,
-                    const double2 *st, const double4 *wx4, int64_t P, double **partials_out, int *grid_out,
-                    int *status) {
+int bandloop_per_sm(int *per_sm) {
   using Smem = BandSmem<BCH, MIXED>;
   const size_t smem = sizeof(Smem);
   auto kfn = gpp_bandloop_kernel<BCH, MIXED>;
+  BGW_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  BGW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kfn, kThreads, smem));
+  return *per_sm >= 1 ? BGW_OK : BGW_ERR_UNSUPPORTED;
+}
+
+// Launches the band loop over rows [0, P) of the given (already offset)
+// arrays; writes `grid` partials (6 doubles each) starting at `partials`.
+template <int BCH, bool MIXED>
+int launch_bandloop(cudaStream_t stream, int max_grid, int nb, int G, const double2 *wt, const double2 *ie,
+                    const double2 *st, const double4 *wx4, int64_t P, double *partials, int *grid_out,
+                    int *status) {
+  using Smem = BandSmem<BCH, MIXED>;
+  const size_t smem = sizeof(Smem);
   const int nchunks_g = (int)((G + BandCfg<MIXED>::kCH - 1) / BandCfg<MIXED>::kCH);
   const long long items = (long long)P * nchunks_g;
-  BGW_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int per_sm = 0;
-  BGW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kThreads, smem));
-  if (per_sm < 1) return BGW_ERR_UNSUPPORTED;
-  long long grid = std::min<long long>(items, (long long)ws->sm_count * per_sm);
+  long long grid = std::min<long long>(items, (long long)max_grid);
   if (grid < 1) grid = 1;
-  void *partials = nullptr;
-  BGW_TRY(ws_reserve(ws, SLOT_PARTIALS, sizeof(double) * 6 * (size_t)grid, &partials));
   *grid_out = (int)grid;
-  *partials_out = (double *)partials;
-  kfn<<<(int)grid, kThreads, smem, stream>>>(nb, G, items, nchunks_g, wt, ie, st, wx4, (double *)partials,
-                                             status);
+  gpp_bandloop_kernel<BCH, MIXED><<<(int)grid, kThreads, smem, stream>>>(nb, G, items, nchunks_g, wt, ie, st, wx4,
+                                                                          partials, status);
   count_launch();
   BGW_CUDA_TRY(cudaGetLastError());
   return BGW_OK;
@@ -348,81 +353,183 @@ int launch_bandloop(Workspace *ws, cudaStream_t stream, int nb, int G, const dou
 
 }  // namespace
 
+// Rows [p0[c], p0[c + 1]) of wtilde / I_eps form chunk c; the compute stream
+// waits for ready[c] (may be null) before using chunk c.  One chunk with no
+// event covers device-resident inputs.
+struct RowChunks {
+  static constexpr int kMax = 16;
+  int n = 1;
+  int64_t p0[kMax + 1] = {};
+  cudaEvent_t ready[kMax] = {};
+};
+
 // Enqueues the GPP sum on env->stream.  All pointers are device pointers;
 // wx holds 3 doubles (wx_stride == 0) or nb rows of wx_stride doubles.
 // achtemp_dev receives 6 doubles (3 complex).
-int gpp_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *inv, const int32_t *indinv,
-                int64_t indinv_len, const double *wx, int64_t wx_stride, const double2 *wt, const double2 *am,
-                const double2 *an, const double2 *ie, const double *vc, double *achtemp_dev) {
+// `issue(c)` (optional) is called before chunk c is enqueued and may issue
+// chunk c's copies: with pageable host memory cudaMemcpyAsync returns only
+// after staging the source, so interleaving keeps the GPU busy on chunk c-1.
+int gpp_enqueue_chunks(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *inv, const int32_t *indinv,
+                       int64_t indinv_len, const double *wx, int64_t wx_stride, const double2 *wt,
+                       const double2 *am, const double2 *an, const double2 *ie, const double *vc,
+                       double *achtemp_dev, RowChunks &rc, const std::function<int(int)> &issue = nullptr) {
   Workspace *ws = env->ws;
   cudaStream_t stream = env->stream;
-  const int nchunks_g = (int)((G + kChunk - 1) / kChunk);
-  const long long items = (long long)P * nchunks_g;
   const bool factored = env->opt.gpp_algorithm == BGW_GPP_FACTORED ||
                         (env->opt.gpp_algorithm == BGW_GPP_AUTO && wx_stride == 0 &&
                          env->opt.precision == BGW_PRECISION_FP64);
   if (factored && env->opt.precision == BGW_PRECISION_MIXED) return BGW_ERR_UNSUPPORTED;
-  int prep_grid = (int)std::min<long long>((P + 7) / 8, (long long)ws->sm_count * 16);
-  if (prep_grid < 1) prep_grid = 1;
+  if (factored && wx_stride != 0) return BGW_ERR_UNSUPPORTED;  // needs a band-independent wx
+  const bool mixed = env->opt.precision == BGW_PRECISION_MIXED;
+  auto prep_grid_for = [&](int64_t rows) {
+    return (int)std::max<long long>(1, std::min<long long>((rows + 7) / 8, (long long)ws->sm_count * 16));
+  };
 
+  // Partials: an upper bound of every chunk's grid, reserved up front.
+  int per_launch = 0;
   if (factored) {
-    if (wx_stride != 0) return BGW_ERR_UNSUPPORTED;  // needs a band-independent wx
-    void *S = nullptr, *partials = nullptr;
-    BGW_TRY(ws_reserve(ws, SLOT_TABLE0, sizeof(double2) * (size_t)std::max<int64_t>(P, 1), &S));
-    gpp_prep_kernel<<<prep_grid, 256, 0, stream>>>((int)nb, (int)P, (int)G, inv, indinv, indinv_len, wt, am, an,
-                                                   vc, nullptr, (double2 *)S, env->d_status);
-    count_launch();
-    BGW_CUDA_TRY(cudaGetLastError());
-    int grid = (int)std::min<long long>(std::max<long long>(items, 1), (long long)ws->sm_count * 8);
-    BGW_TRY(ws_reserve(ws, SLOT_PARTIALS, sizeof(double) * 6 * (size_t)grid, &partials));
-    BGW_TRY(prof_mark(env, 1));
-    gpp_factored_kernel<<<grid, kThreads, 0, stream>>>((int)G, items, nchunks_g, wt, ie, (const double2 *)S, wx,
-                                                       (double *)partials);
-    count_launch();
-    BGW_CUDA_TRY(cudaGetLastError());
-    BGW_TRY(prof_mark(env, 2));
-    env->prof.main_bytes = 32.0 * (double)P * (double)G + 16.0 * (double)P;
-    env->prof.main_launches = 1;
-    std::snprintf(env->prof.main_kernel, sizeof(env->prof.main_kernel), "gpp_factored_kernel");
-    reduce_partials_kernel<6><<<1, 256, 0, stream>>>((const double *)partials, grid, achtemp_dev);
-    count_launch();
-    BGW_CUDA_TRY(cudaGetLastError());
-    return BGW_OK;
+    per_launch = ws->sm_count * 8;
+  } else {
+    int per_sm = 0;
+    if (mixed) BGW_TRY((bandloop_per_sm<256, true>(&per_sm)));
+    else BGW_TRY((bandloop_per_sm<256, false>(&per_sm)));
+    per_launch = ws->sm_count * per_sm;
+  }
+  void *partials_v = nullptr, *tab = nullptr, *wx4 = nullptr;
+  BGW_TRY(ws_reserve(ws, SLOT_PARTIALS, sizeof(double) * 6 * (size_t)per_launch * rc.n, &partials_v));
+  double *partials = static_cast<double *>(partials_v);
+  const size_t tab_elems = factored ? (size_t)std::max<int64_t>(P, 1) : (size_t)std::max<int64_t>(P * nb, 1);
+  BGW_TRY(ws_reserve(ws, SLOT_TABLE0, sizeof(double2) * tab_elems, &tab));
+  if (!factored) {
+    // Per-band frequency rows (stride 0: the one triple repeated per band).
+    BGW_TRY(ws_reserve(ws, SLOT_TABLE1, sizeof(double4) * (size_t)std::max<int64_t>(nb, 1), &wx4));
   }
 
-  void *st = nullptr, *wx4 = nullptr;
-  BGW_TRY(ws_reserve(ws, SLOT_TABLE0, sizeof(double2) * (size_t)std::max<int64_t>(P * nb, 1), &st));
-  gpp_prep_kernel<<<prep_grid, 256, 0, stream>>>((int)nb, (int)P, (int)G, inv, indinv, indinv_len, wt, am, an, vc,
-                                                 (double2 *)st, nullptr, env->d_status);
-  count_launch();
-  BGW_CUDA_TRY(cudaGetLastError());
-  // Per-band frequency rows (stride 0: the one triple repeated per band).
-  BGW_TRY(ws_reserve(ws, SLOT_TABLE1, sizeof(double4) * (size_t)std::max<int64_t>(nb, 1), &wx4));
-  if (nb > 0) {
-    int g = (int)std::min<int64_t>((nb + 255) / 256, 1024);
-    gpp_wx_kernel<<<std::max(g, 1), 256, 0, stream>>>((int)nb, wx, wx_stride, (double4 *)wx4);
-    count_launch();
-    BGW_CUDA_TRY(cudaGetLastError());
-  }
-  int grid = 0;
-  double *partials = nullptr;
-  BGW_TRY(prof_mark(env, 1));
-  if (env->opt.precision == BGW_PRECISION_MIXED) {
-    BGW_TRY((launch_bandloop<256, true>(ws, stream, (int)nb, (int)G, wt, ie, (const double2 *)st,
-                                        (const double4 *)wx4, P, &partials, &grid, env->d_status)));
-  } else {
-    BGW_TRY((launch_bandloop<256, false>(ws, stream, (int)nb, (int)G, wt, ie, (const double2 *)st,
-                                         (const double4 *)wx4, P, &partials, &grid, env->d_status)));
+  int total = 0;  // partials written so far
+  for (int c = 0; c < rc.n; ++c) {
+    if (issue) BGW_TRY(issue(c));
+    if (rc.ready[c]) BGW_CUDA_TRY(cudaStreamWaitEvent(stream, rc.ready[c], 0));
+    const int64_t p0 = rc.p0[c], rows = rc.p0[c + 1] - rc.p0[c];
+    if (c == 0 && !factored && nb > 0) {
+      int g = (int)std::min<int64_t>((nb + 255) / 256, 1024);
+      gpp_wx_kernel<<<std::max(g, 1), 256, 0, stream>>>((int)nb, wx, wx_stride, (double4 *)wx4);
+      count_launch();
+      BGW_CUDA_TRY(cudaGetLastError());
+    }
+    if (rows <= 0 && rc.n > 1) continue;
+    const double2 *wt_c = wt + (size_t)p0 * G, *ie_c = ie + (size_t)p0 * G;
+    double *part_c = partials + (size_t)total * 6;
+    if (factored) {
+      double2 *S_c = static_cast<double2 *>(tab) + p0;
+      gpp_prep_kernel<<<prep_grid_for(rows), 256, 0, stream>>>((int)nb, (int)rows, (int)G, inv + p0, indinv,
+                                                               indinv_len, wt_c, am, an, vc, nullptr, S_c,
+                                                               env->d_status);
+      count_launch();
+      BGW_CUDA_TRY(cudaGetLastError());
+      const int nchunks_g = (int)((G + kChunk - 1) / kChunk);
+      const long long items = (long long)rows * nchunks_g;
+      const int grid = (int)std::min<long long>(std::max<long long>(items, 1), (long long)per_launch);
+      if (c == 0) BGW_TRY(prof_mark(env, 1));
+      gpp_factored_kernel<<<grid, kThreads, 0, stream>>>((int)G, items, nchunks_g, wt_c, ie_c, S_c, wx, part_c);
+      count_launch();
+      BGW_CUDA_TRY(cudaGetLastError());
+      total += grid;
+    } else {
+      double2 *st_c = static_cast<double2 *>(tab) + (size_t)p0 * nb;
+      gpp_prep_kernel<<<prep_grid_for(rows), 256, 0, stream>>>((int)nb, (int)rows, (int)G, inv + p0, indinv,
+                                                               indinv_len, wt_c, am, an, vc, st_c, nullptr,
+                                                               env->d_status);
+      count_launch();
+      BGW_CUDA_TRY(cudaGetLastError());
+      if (c == 0) BGW_TRY(prof_mark(env, 1));
+      int grid = 0;
+      if (mixed) {
+        BGW_TRY((launch_bandloop<256, true>(stream, per_launch, (int)nb, (int)G, wt_c, ie_c, st_c,
+                                            (const double4 *)wx4, rows, part_c, &grid, env->d_status)));
+      } else {
+        BGW_TRY((launch_bandloop<256, false>(stream, per_launch, (int)nb, (int)G, wt_c, ie_c, st_c,
+                                             (const double4 *)wx4, rows, part_c, &grid, env->d_status)));
+      }
+      total += grid;
+    }
   }
   BGW_TRY(prof_mark(env, 2));
-  env->prof.main_bytes = 32.0 * (double)P * (double)G + 16.0 * (double)P * (double)nb + 32.0 * (double)nb;
-  env->prof.main_launches = 1;
-  std::snprintf(env->prof.main_kernel, sizeof(env->prof.main_kernel),
-                env->opt.precision == BGW_PRECISION_MIXED ? "gpp_bandloop_kernel<mixed>" : "gpp_bandloop_kernel");
-  reduce_partials_kernel<6><<<1, 256, 0, stream>>>(partials, grid, achtemp_dev);
+  if (factored) {
+    env->prof.main_bytes = 32.0 * (double)P * (double)G + 16.0 * (double)P;
+    std::snprintf(env->prof.main_kernel, sizeof(env->prof.main_kernel), "gpp_factored_kernel");
+  } else {
+    env->prof.main_bytes = 32.0 * (double)P * (double)G + 16.0 * (double)P * (double)nb + 32.0 * (double)nb;
+    std::snprintf(env->prof.main_kernel, sizeof(env->prof.main_kernel),
+                  mixed ? "gpp_bandloop_kernel<mixed>" : "gpp_bandloop_kernel");
+  }
+  env->prof.main_launches = rc.n;
+  reduce_partials_kernel<6><<<1, 256, 0, stream>>>(partials, std::max(total, 1), achtemp_dev);
   count_launch();
   BGW_CUDA_TRY(cudaGetLastError());
   return BGW_OK;
+}
+
+int gpp_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *inv, const int32_t *indinv,
+                int64_t indinv_len, const double *wx, int64_t wx_stride, const double2 *wt, const double2 *am,
+                const double2 *an, const double2 *ie, const double *vc, double *achtemp_dev) {
+  RowChunks rc;
+  rc.n = 1;
+  rc.p0[0] = 0;
+  rc.p0[1] = P;
+  return gpp_enqueue_chunks(env, nb, P, G, inv, indinv, indinv_len, wx, wx_stride, wt, am, an, ie, vc,
+                            achtemp_dev, rc);
+}
+
+// Host-resident inputs: the copies run on the workspace's copy stream in
+// G'-row chunks, and chunk c's kernels start as soon as its rows have landed,
+// so the H2D transfer of chunk c+1 overlaps the compute of chunk c.  The
+// chunking is a fixed function of the sizes, so results stay deterministic.
+int gpp_run_host(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *inv, const int32_t *indinv,
+                 int64_t indinv_len, const double *wx, size_t wx_n, int64_t wx_stride, const double *wt,
+                 const double *am, const double *an, const double *ie, const double *vc, double *achtemp_dev) {
+  Workspace *ws = env->ws;
+  cudaStream_t cs = nullptr;
+  BGW_TRY(ws_copy_stream(ws, &cs));
+  // The copy stream starts after everything already queued on the compute
+  // stream (earlier users of the staging buffers).
+  BGW_CUDA_TRY(cudaEventRecord(ws->copy_start, env->stream));
+  BGW_CUDA_TRY(cudaStreamWaitEvent(cs, ws->copy_start, 0));
+  const size_t pg = (size_t)P * (size_t)G * 16, ng = (size_t)nb * (size_t)G * 16;
+  void *d_inv, *d_ind, *d_wx, *d_vc, *d_am, *d_an, *d_wt, *d_ie;
+  BGW_TRY(ws_reserve(ws, SLOT_IN0, sizeof(int32_t) * (size_t)P, &d_inv));
+  BGW_TRY(ws_reserve(ws, SLOT_IN1, sizeof(int32_t) * (size_t)indinv_len, &d_ind));
+  BGW_TRY(ws_reserve(ws, SLOT_IN2, sizeof(double) * wx_n, &d_wx));
+  BGW_TRY(ws_reserve(ws, SLOT_IN7, sizeof(double) * (size_t)G, &d_vc));
+  BGW_TRY(ws_reserve(ws, SLOT_IN4, ng, &d_am));
+  BGW_TRY(ws_reserve(ws, SLOT_IN5, ng, &d_an));
+  BGW_TRY(ws_reserve(ws, SLOT_IN3, pg, &d_wt));
+  BGW_TRY(ws_reserve(ws, SLOT_IN6, pg, &d_ie));
+  auto h2d = [&](void *dst, const void *src, size_t bytes) -> int {
+    if (bytes) BGW_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, cs));
+    return BGW_OK;
+  };
+  BGW_TRY(h2d(d_inv, inv, sizeof(int32_t) * (size_t)P));
+  BGW_TRY(h2d(d_ind, indinv, sizeof(int32_t) * (size_t)indinv_len));
+  BGW_TRY(h2d(d_wx, wx, sizeof(double) * wx_n));
+  BGW_TRY(h2d(d_vc, vc, sizeof(double) * (size_t)G));
+  BGW_TRY(h2d(d_am, am, ng));
+  BGW_TRY(h2d(d_an, an, ng));
+  // About 8 chunks of at least 64 rows.
+  RowChunks rc;
+  rc.n = (int)std::max<int64_t>(1, std::min<int64_t>(8, P / 64));
+  for (int c = 0; c <= rc.n; ++c) rc.p0[c] = P * c / rc.n;
+  for (int c = 0; c < rc.n; ++c) rc.ready[c] = ws->chunk_ready[c];
+  auto issue = [&](int c) -> int {
+    const size_t off = (size_t)rc.p0[c] * G * 16, bytes = (size_t)(rc.p0[c + 1] - rc.p0[c]) * G * 16;
+    BGW_TRY(h2d(static_cast<char *>(d_wt) + off, reinterpret_cast<const char *>(wt) + off, bytes));
+    BGW_TRY(h2d(static_cast<char *>(d_ie) + off, reinterpret_cast<const char *>(ie) + off, bytes));
+    BGW_CUDA_TRY(cudaEventRecord(ws->chunk_ready[c], cs));
+    return BGW_OK;
+  };
+  return gpp_enqueue_chunks(env, nb, P, G, (const int32_t *)d_inv, (const int32_t *)d_ind, indinv_len,
+                            (const double *)d_wx, wx_stride, (const double2 *)d_wt, (const double2 *)d_am,
+                            (const double2 *)d_an, (const double2 *)d_ie, (const double *)d_vc, achtemp_dev, rc,
+                            issue);
 }
 
 // ------------------------------------------------------ no-allocation path --

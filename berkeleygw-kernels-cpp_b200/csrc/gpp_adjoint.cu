@@ -28,7 +28,7 @@ namespace bgw {
 namespace {
 
 constexpr int kAdjThreads = 256;
-constexpr int kAdjElems = 4;
+constexpr int kAdjElems = 2;
 
 // C(p), S(p) = C(p) wtilde[p][igp] and igp(p) (-1 if out of range).  One
 // warp per column, fixed-order band sum.
@@ -68,7 +68,7 @@ __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_doub
 
 // grad_wt / grad_ie may be null (not requested).  partials: 6 doubles per
 // CTA (dSigma_iw/domega, re/im).
-__global__ void __launch_bounds__(kAdjThreads)
+__global__ void __launch_bounds__(kAdjThreads, 2)
     gpp_adjoint_kernel(int P, int G, const double2 *__restrict__ wtilde, const double2 *__restrict__ ieps,
                        const double2 *__restrict__ Cp, const double2 *__restrict__ Sp, const int *__restrict__ igp,
                        const double *__restrict__ wx3, const double2 *__restrict__ gcot,
@@ -83,19 +83,26 @@ __global__ void __launch_bounds__(kAdjThreads)
     const double2 S = Sp[p];
     double t_r[3] = {0.0, 0.0, 0.0}, t_i[3] = {0.0, 0.0, 0.0};   // T(p, iw)
     double u_r[3] = {0.0, 0.0, 0.0}, u_i[3] = {0.0, 0.0, 0.0};   // sum_ig I q^2 (this thread)
-    for (int g0 = 0; g0 < G; g0 += kAdjThreads * kAdjElems) {
-      double2 w[kAdjElems], v[kAdjElems];
+    // Loads of chunk g0 + step are issued before chunk g0 is computed
+    // (register double buffering), so HBM traffic overlaps the FP64 work.
+    constexpr int kStep = kAdjThreads * kAdjElems;
+    double2 w[kAdjElems], v[kAdjElems], wn[kAdjElems], vn[kAdjElems];
+    auto load = [&](int g0, double2 (&ww)[kAdjElems], double2 (&vv)[kAdjElems]) {
 #pragma unroll
       for (int k = 0; k < kAdjElems; ++k) {
         const int ig = g0 + k * kAdjThreads + tid;
         if (ig < G) {
-          w[k] = __ldcs(wtilde + (size_t)p * G + ig);
-          v[k] = __ldcs(ieps + (size_t)p * G + ig);
+          ww[k] = __ldcs(wtilde + (size_t)p * G + ig);
+          vv[k] = __ldcs(ieps + (size_t)p * G + ig);
         } else {
-          w[k] = make_double2(0.0, 1.0);
-          v[k] = make_double2(0.0, 0.0);
+          ww[k] = make_double2(0.0, 1.0);
+          vv[k] = make_double2(0.0, 0.0);
         }
       }
+    };
+    load(0, w, v);
+    for (int g0 = 0; g0 < G; g0 += kStep) {
+      if (g0 + kStep < G) load(g0 + kStep, wn, vn);
 #pragma unroll
       for (int k = 0; k < kAdjElems; ++k) {
         const int ig = g0 + k * kAdjThreads + tid;
@@ -116,9 +123,14 @@ __global__ void __launch_bounds__(kAdjThreads)
         }
         if (ig < G) {
           // grad = conj(sum_iw conj(G_iw) dSigma_iw/dz)
-          if (grad_ie) grad_ie[(size_t)p * G + ig] = cconj(cmul(S, hI));
-          if (grad_wt) grad_wt[(size_t)p * G + ig] = cconj(cmul(S, hW));
+          if (grad_ie) __stcs(grad_ie + (size_t)p * G + ig, cconj(cmul(S, hI)));
+          if (grad_wt) __stcs(grad_wt + (size_t)p * G + ig, cconj(cmul(S, hW)));
         }
+      }
+#pragma unroll
+      for (int k = 0; k < kAdjElems; ++k) {
+        w[k] = wn[k];
+        v[k] = vn[k];
       }
     }
 #pragma unroll

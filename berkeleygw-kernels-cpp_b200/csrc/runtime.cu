@@ -66,6 +66,16 @@ int ws_acquire(Workspace *ws, cudaStream_t stream) {
   return BGW_OK;
 }
 
+int ws_copy_stream(Workspace *ws, cudaStream_t *out) {
+  if (!ws->copy_stream) {
+    BGW_CUDA_TRY(cudaStreamCreateWithFlags(&ws->copy_stream, cudaStreamNonBlocking));
+    BGW_CUDA_TRY(cudaEventCreateWithFlags(&ws->copy_start, cudaEventDisableTiming));
+    for (auto &e : ws->chunk_ready) BGW_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  *out = ws->copy_stream;
+  return BGW_OK;
+}
+
 int ws_release(Workspace *ws, cudaStream_t stream) {
   BGW_CUDA_TRY(cudaEventRecord(ws->last_use, stream));
   return BGW_OK;
