@@ -365,6 +365,12 @@ def run_ours(args, world, rank, local):
     del d
     torch.cuda.empty_cache()
 
+    # Batched uneven GPP: 64 q-point instances in one graph-replayed launch
+    # against 64 sequential single-instance calls (same inputs, on the GPU).
+    if not args.quick and not args.no_batch:
+        extra["gpp_batched"] = bench_batched(bgw, I, dev, sh, stream, dfma_peak, rank)
+        torch.cuda.empty_cache()
+
     # FF sums.
     if not args.quick:
         f = I.ff_seeded(**FF_DIMS, seed=1234 + rank)
@@ -436,6 +442,86 @@ def run_ours(args, world, rank, local):
     return 0
 
 
+def make_batch_device(I, dev, n=64, seed=4321):
+    """The batched workload generated on the GPU (seeded torch generator):
+    ncouls uniform in {4096, 4608, ..., 32768}, number_bands uniform in
+    [128, 512], nodes_per_group 20, the benchmark distributions."""
+    import torch
+    rng = np.random.default_rng(seed)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    out = []
+    for _ in range(n):
+        G = int(rng.choice(np.arange(4096, 32768 + 1, 512)))
+        nb = int(rng.integers(128, 513))
+        P = G // 20
+
+        def cu(rows, lo, hi):
+            t = torch.rand((rows, G, 2), generator=gen, device=dev, dtype=torch.float64)
+            t.mul_(hi - lo).add_(lo)
+            return torch.view_as_complex(t)
+        wt = torch.rand((P, G, 2), generator=gen, device=dev, dtype=torch.float64)
+        wt[..., 0].mul_(1.5).add_(0.5)
+        wt[..., 1].mul_(0.02).sub_(0.01)
+        indinv = torch.cat([torch.randperm(G, generator=gen, device=dev), torch.tensor([G - 1], device=dev)])
+        out.append(I.GppInputs(
+            number_bands=nb, nvband=2, ncouls=G, ngpown=P,
+            inv_igp_index=(torch.arange(P, device=dev) * 20).to(torch.int32), indinv=indinv.to(torch.int32),
+            wx_array=torch.tensor([9.5, 10.0, 10.5], device=dev, dtype=torch.float64),
+            wtilde_array=torch.view_as_complex(wt), aqsmtemp=cu(nb, -1.0, 1.0), aqsntemp=cu(nb, -1.0, 1.0),
+            I_eps_array=cu(P, -0.5, 0.5), vcoul=1.0 / (1.0 + torch.arange(G, device=dev, dtype=torch.float64))))
+    return out
+
+
+def bench_batched(bgw, I, dev, sh, stream, dfma_peak, rank):
+    import torch
+    insts = make_batch_device(I, dev)
+    nbytes = sum(g.nbytes() for g in insts)
+    flops = sum(63.0 * g.number_bands * g.ngpown * g.ncouls for g in insts)
+    stream_bytes = sum(32.0 * g.ngpown * g.ncouls for g in insts)
+    res = {"workload": "64 instances, ncouls uniform in {4096..32768 step 512}, number_bands in [128, 512], "
+                       "nodes_per_group 20; inputs generated on the GPU", "device_bytes": nbytes}
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize(dev)
+        ev0.record(stream)
+        for _ in range(reps):
+            fn()
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        return ev0.elapsed_time(ev1) / 1e3 / reps
+
+    for alg in ("bandloop", "factored"):
+        t0 = time.perf_counter()
+        b = bgw.GppBatch(insts, algorithm=alg, stream=sh)
+        create_s = time.perf_counter() - t0
+        t_batch = timed(lambda: b.execute(stream=sh), 3)
+        batch_out = b.execute(stream=sh).cpu().numpy().copy()
+        seq_out = np.zeros_like(batch_out)
+
+        def seq():
+            for k, g in enumerate(insts):
+                r = bgw.noflagOCC_solver(g, algorithm=alg, stream=sh)
+                seq_out[k] = r.cpu().numpy()
+        t_seq = timed(seq, 1)
+        err = max(rel_err(batch_out[k], seq_out[k]) for k in range(len(insts)))
+        entry = {"batched_s": t_batch, "sequential_s": t_seq, "speedup_vs_sequential": t_seq / t_batch,
+                 "instances_per_s": len(insts) / t_batch, "tuned": b.info(), "create_s": create_s,
+                 "max_rel_diff_vs_sequential": err}
+        if alg == "bandloop":
+            entry["roofline"] = {"bound": "fp64", "achieved": flops / t_batch / 1e12, "unit": "TFLOP/s",
+                                 "peak": dfma_peak, "frac": flops / t_batch / 1e12 / dfma_peak}
+        else:
+            entry["roofline"] = {"bound": "hbm", "achieved": stream_bytes / t_batch / 1e9, "unit": "GB/s",
+                                 "peak": _hbm_peak(), "frac": stream_bytes / t_batch / 1e9 / _hbm_peak()}
+        res[alg] = entry
+        b.close()
+    del insts
+    return res
+
+
 def run_only(args, local):
     """Diagnostic mode for profilers: runs one kernel path W + K times on the
     benchmark shapes (GPP bands optionally reduced with --bands) and prints a
@@ -495,6 +581,7 @@ def main():
     ap.add_argument("--quick", action="store_true", help="GPP band loop + e2e only")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and oracle check")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-instances extra")
     ap.add_argument("--only", choices=["gpp_bandloop", "gpp_mixed", "gpp_factored", "gpp_adjoint", "ff"],
                     default=None,
                     help="diagnostic: time one kernel path only (for profilers)")

@@ -39,7 +39,8 @@ FLAG_PROFILE = 2
 EXPORTS = ("bgw_options_init", "bgw_noflagOCC_solver", "bgw_achsDtemp_Kernel", "bgw_asxDtemp_Kernel",
            "bgw_achDtemp_cor_Kernel", "bgw_ff_sigma", "bgw_status_string", "bgw_abi_version",
            "bgw_launch_count", "bgw_measure_fp64_peak", "bgw_release_workspace", "bgw_last_profile",
-           "bgw_noflagOCC_solver_noalloc", "bgw_noflagOCC_solver_backward")
+           "bgw_noflagOCC_solver_noalloc", "bgw_noflagOCC_solver_backward", "bgw_gpp_batch_create",
+           "bgw_gpp_batch_execute", "bgw_gpp_batch_info", "bgw_gpp_batch_destroy")
 
 
 class BgwError(RuntimeError):
@@ -63,6 +64,14 @@ class Profile(ctypes.Structure):
         return {"main_kernel": self.main_kernel.decode(), "main_kernel_ms": self.main_kernel_ms,
                 "device_ms": self.device_ms, "flops": self.flops, "main_bytes": self.main_bytes,
                 "main_launches": self.main_launches, "total_launches": self.total_launches}
+
+
+class GppInstance(ctypes.Structure):
+    _fields_ = [("number_bands", ctypes.c_int64), ("ngpown", ctypes.c_int64), ("ncouls", ctypes.c_int64),
+                ("inv_igp_index", ctypes.c_void_p), ("indinv", ctypes.c_void_p), ("indinv_len", ctypes.c_int64),
+                ("wx_array", ctypes.c_void_p), ("wx_band_stride", ctypes.c_int64), ("wtilde_array", ctypes.c_void_p),
+                ("aqsmtemp", ctypes.c_void_p), ("aqsntemp", ctypes.c_void_p), ("I_eps_array", ctypes.c_void_p),
+                ("vcoul", ctypes.c_void_p), ("achtemp", ctypes.c_void_p)]
 
 
 _LIB = None
@@ -101,6 +110,11 @@ def load(build_if_needed: bool = True) -> ctypes.CDLL:
                                                  ctypes.c_int32, _P]
     lib.bgw_noflagOCC_solver_backward.argtypes = [_I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P,
                                                   _P, _P, opt]
+    lib.bgw_gpp_batch_create.argtypes = [ctypes.POINTER(GppInstance), _I64, opt, ctypes.POINTER(_P)]
+    lib.bgw_gpp_batch_execute.argtypes = [_P, opt]
+    lib.bgw_gpp_batch_info.argtypes = [_P, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
+                                       ctypes.POINTER(ctypes.c_int64)]
+    lib.bgw_gpp_batch_destroy.argtypes = [_P]
     lib.bgw_achsDtemp_Kernel.argtypes = [_I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _I64, _P, _P, opt]
     lib.bgw_asxDtemp_Kernel.argtypes = [_I64, _I64, _I64, _I64, _I64, _D, _D, _D, _P, _P, _P, _P, _I64, _P, _P,
                                         _I64, _P, _P, _P, _P, opt]
@@ -233,6 +247,55 @@ def noflagOCC_solver_backward(inp: GppInputs, grad_achtemp, *, want_wtilde=True,
                                            _ptr(inp.vcoul), _ptr(gc), _nz(gw), _nz(gi), _nz(dw), ctypes.byref(o))
     _check("bgw_noflagOCC_solver_backward", st)
     return gw, gi, dw
+
+
+class GppBatch:
+    """Many device-resident GPP instances in one persistent launch (a CUDA
+    graph replayed by execute()).  `instances`: GppInputs with CUDA tensors."""
+
+    def __init__(self, instances, *, precision="fp64", algorithm="auto", stream=None):
+        import torch
+        lib = load()
+        self.instances = list(instances)
+        dev = self.instances[0].wtilde_array.device
+        self.out = torch.zeros((len(self.instances), 3), dtype=torch.complex128, device=dev)
+        arr = (GppInstance * len(self.instances))()
+        for k, g in enumerate(self.instances):
+            if _where(g) != "device":
+                raise ValueError("batched instances must be CUDA tensors")
+            arr[k] = GppInstance(g.number_bands, g.ngpown, g.ncouls, _ptr(g.inv_igp_index), _ptr(g.indinv),
+                                 len(g.indinv), _ptr(g.wx_array), g.wx_band_stride, _ptr(g.wtilde_array),
+                                 _ptr(g.aqsmtemp), _ptr(g.aqsntemp), _ptr(g.I_eps_array), _ptr(g.vcoul),
+                                 self.out[k].data_ptr())
+        self._arr = arr
+        o = make_options("device", precision, algorithm, stream=_stream_handle(None, stream),
+                         device=dev.index if dev.index is not None else -1)
+        h = _P()
+        _check("bgw_gpp_batch_create", lib.bgw_gpp_batch_create(arr, len(self.instances), ctypes.byref(o),
+                                                                ctypes.byref(h)))
+        self.handle = h
+
+    def execute(self, stream=None, flags=0):
+        o = make_options("device", stream=_stream_handle(None, stream), flags=flags)
+        _check("bgw_gpp_batch_execute", load().bgw_gpp_batch_execute(self.handle, ctypes.byref(o)))
+        return self.out
+
+    def info(self):
+        ke, grid, items = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64()
+        _check("bgw_gpp_batch_info", load().bgw_gpp_batch_info(self.handle, ctypes.byref(ke), ctypes.byref(grid),
+                                                                ctypes.byref(items)))
+        return {"elems_per_thread": ke.value, "grid": grid.value, "items": items.value}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            load().bgw_gpp_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _ff_out(inp: FFInputs, n: int, mem: str):

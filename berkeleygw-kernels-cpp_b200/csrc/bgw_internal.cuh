@@ -111,6 +111,8 @@ struct CallEnv {
 
 // Profiling marks (no-ops unless BGW_FLAG_PROFILE).
 int prof_mark(CallEnv *env, int which);
+// Stores `p` as this thread's last profile (bgw_last_profile).
+void set_last_profile(const bgw_profile &p);
 
 // Validates options, selects the device, fetches the workspace.
 int begin_call(const bgw_options *user, CallEnv *env);

@@ -80,15 +80,17 @@ extern "C" int bgw_noflagOCC_solver(int64_t number_bands, int64_t ngpown, int64_
   const int64_t nb = number_bands, P = ngpown, G = ncouls;
   if (nb < 0 || P < 0 || G <= 0 || G > INT32_MAX || nb > INT32_MAX || P > INT32_MAX) return BGW_ERR_INVALID_ARG;
   if (!dims_ok(nb, G) || !dims_ok(P, G) || indinv_len <= 0 || indinv_len > INT32_MAX) return BGW_ERR_INVALID_ARG;
-  if (!achtemp || !wx_array || !vcoul || !indinv) return BGW_ERR_INVALID_ARG;
+  if (!achtemp || !vcoul || !indinv) return BGW_ERR_INVALID_ARG;
   if (P > 0 && (!inv_igp_index || !wtilde_array || !I_eps_array)) return BGW_ERR_INVALID_ARG;
   if (nb > 0 && P > 0 && (!aqsmtemp || !aqsntemp)) return BGW_ERR_INVALID_ARG;
   Call c(opt);
   if (c.st != BGW_OK) return c.st;
   CallEnv *env = &c.env;
   const int64_t stride = env->opt.wx_band_stride;
+  // wx may be absent only when nothing reads it: no bands and per-band rows.
+  if (!wx_array && (nb > 0 || stride == 0)) return BGW_ERR_INVALID_ARG;
   if (stride != 0 && stride < 3) return BGW_ERR_INVALID_ARG;
-  const size_t wx_n = stride == 0 ? 3 : (size_t)(nb > 0 ? (nb - 1) * stride + 3 : 3);
+  const size_t wx_n = !wx_array ? 0 : stride == 0 ? 3 : (size_t)(nb > 0 ? (nb - 1) * stride + 3 : 3);
   double *out = nullptr;
   BGW_TRY(out_buffer(env, achtemp, 6 * sizeof(double), &out));
   if (env->host) {

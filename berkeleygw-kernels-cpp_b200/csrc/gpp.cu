@@ -80,11 +80,6 @@ __global__ void gpp_wx_kernel(int nb, const double *__restrict__ wx, long long s
 // a frequency x:
 //   dr  = x - wr,  |wdiff|^2 = dr^2 + wi^2,
 //   conj(wdiff) * I_eps = (dr*Ir + a) + i (dr*Ii + b).
-template <typename T>
-struct Elem {
-  T wr, wi2, Ir, Ii, a, b;
-};
-
 // Elements per thread: FP64 4, mixed 8 (the FP32 quotients are cheap, so a
 // longer run per band amortises the FP64 band combination).
 template <bool MIXED>
@@ -102,22 +97,6 @@ struct BandSmem {
   unsigned long long bar[2];
   double red[(kThreads / 32) * 6];
 };
-
-__device__ __forceinline__ float rcp_approx_f32(float d) {
-  float y;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(d));
-  return y;
-}
-
-// Error-free transformation of a + b (Knuth's TwoSum, TAOCP vol. 2,
-// 4.2.2): hi + lo == a + b exactly, no ordering assumption.
-__device__ __forceinline__ void two_sum_acc(double &hi, double &lo, double b) {
-  const double s = hi + b;
-  const double bb = s - hi;
-  const double err = (hi - (s - bb)) + (b - bb);
-  hi = s;
-  lo += err;
-}
 
 // Every band reads its own frequencies from the staged wx4 rows (for the
 // reference's band-independent wx the rows repeat one triple), so each
@@ -192,61 +171,8 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 1 : 2)
     const int nbv = min(BCH, nb - b0);
 
     Elem<T> e[kE];
-#pragma unroll
-    for (int k = 0; k < kE; ++k) {
-      const int idx = k * kThreads + tid;
-      if (idx < nvalid) {
-        double2 w = sm.wt[buf][idx], v = sm.ie[buf][idx];
-        e[k].wr = (T)w.x;
-        e[k].wi2 = (T)(w.y * w.y);
-        e[k].Ir = (T)v.x;
-        e[k].Ii = (T)v.y;
-        e[k].a = (T)(-w.y * v.y);
-        e[k].b = (T)(w.y * v.x);
-      } else {  // padding: contributes exactly zero, keeps |wdiff|^2 >= 1
-        e[k].wr = (T)0;
-        e[k].wi2 = (T)1;
-        e[k].Ir = e[k].Ii = e[k].a = e[k].b = (T)0;
-      }
-    }
-
-    for (int bb = 0; bb < nbv; ++bb) {
-      const double4 w4 = sm.wx[buf][bb];
-      const T x[3] = {(T)w4.x, (T)w4.y, (T)w4.z};
-      const double2 s = sm.st[buf][bb];
-      T tr[3] = {(T)0, (T)0, (T)0}, ti[3] = {(T)0, (T)0, (T)0};
-#pragma unroll
-      for (int k = 0; k < kE; ++k) {
-#pragma unroll
-        for (int iw = 0; iw < 3; ++iw) {
-          const T dr = x[iw] - e[k].wr;
-          const T den = fma(dr, dr, e[k].wi2);
-          T r;
-          if constexpr (MIXED) {
-            r = rcp_approx_f32(den);
-          } else {
-            r = rcp_refined(den);
-          }
-          const T nr = fma(dr, e[k].Ir, e[k].a);
-          const T ni = fma(dr, e[k].Ii, e[k].b);
-          tr[iw] = fma(nr, r, tr[iw]);
-          ti[iw] = fma(ni, r, ti[iw]);
-        }
-      }
-#pragma unroll
-      for (int iw = 0; iw < 3; ++iw) {
-        const double trd = (double)tr[iw], tid_ = (double)ti[iw];
-        if constexpr (MIXED) {
-          two_sum_acc(acc_r[iw], lo_r[iw], fma(trd, s.x, -tid_ * s.y));
-          two_sum_acc(acc_i[iw], lo_i[iw], fma(trd, s.y, tid_ * s.x));
-        } else {
-          acc_r[iw] = fma(trd, s.x, acc_r[iw]);
-          acc_r[iw] = fma(-tid_, s.y, acc_r[iw]);
-          acc_i[iw] = fma(trd, s.y, acc_i[iw]);
-          acc_i[iw] = fma(tid_, s.x, acc_i[iw]);
-        }
-      }
-    }
+    load_elems<T, kE>(e, sm.wt[buf], sm.ie[buf], nvalid, kThreads, tid);
+    band_sweep<MIXED, kE>(e, sm.wx[buf], sm.st[buf], nbv, acc_r, acc_i, lo_r, lo_i);
     __syncthreads();  // buffer `buf` is free for step j + 2
   }
   if (!ok && tid == 0) {

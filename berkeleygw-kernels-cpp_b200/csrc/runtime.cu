@@ -85,6 +85,8 @@ namespace {
 thread_local bgw_profile t_last_profile = {};
 }
 
+void set_last_profile(const bgw_profile &p) { t_last_profile = p; }
+
 int prof_mark(CallEnv *env, int which) {
   if (!env->profile) return BGW_OK;
   BGW_CUDA_TRY(cudaEventRecord(env->ws->prof[which], env->stream));

@@ -134,6 +134,45 @@ int bgw_noflagOCC_solver_backward(int64_t number_bands, int64_t ngpown,
                                   double *dachtemp_domega,
                                   const bgw_options *opt);
 
+/* ---------------------------------------------------------- GPP batched --
+ * No counterpart in the reference (one instance per process).  Many GPP
+ * instances -- q-points of uneven ncouls and number_bands -- evaluated by one
+ * persistent launch: the work list of all instances is cut into equal-cost
+ * ranges, one per CTA, and the prep / sum / finalize kernels are captured
+ * once into a CUDA graph that bgw_gpp_batch_execute replays.  The elements
+ * per thread (tile width and occupancy) are chosen at creation by timing the
+ * candidate kernels on a sample of the work list (cached per batch shape).
+ * Algorithm / precision as bgw_noflagOCC_solver (opt->gpp_algorithm,
+ * opt->precision); FACTORED needs every wx_band_stride == 0.  All pointers
+ * are device memory of the selected device and must stay valid while the
+ * batch exists; the results go to each instance's achtemp. */
+typedef struct bgw_gpp_instance {
+  int64_t number_bands, ngpown, ncouls;
+  const int32_t *inv_igp_index; /* [ngpown]                          */
+  const int32_t *indinv;        /* [indinv_len]                      */
+  int64_t indinv_len;
+  const double *wx_array;       /* [3] or [number_bands][stride]     */
+  int64_t wx_band_stride;
+  const double *wtilde_array;   /* complex [ngpown][ncouls]          */
+  const double *aqsmtemp;       /* complex [number_bands][ncouls]    */
+  const double *aqsntemp;
+  const double *I_eps_array;    /* complex [ngpown][ncouls]          */
+  const double *vcoul;          /* [ncouls]                          */
+  double *achtemp;              /* output, complex [3]               */
+} bgw_gpp_instance;
+
+typedef struct bgw_gpp_batch bgw_gpp_batch;
+/* opt->memory must be BGW_MEMORY_DEVICE; opt->stream is used for tuning. */
+int bgw_gpp_batch_create(const bgw_gpp_instance *instances, int64_t n,
+                         const bgw_options *opt, bgw_gpp_batch **batch);
+/* Replays the graph on opt->stream (NULL options: default stream,
+ * synchronous).  With BGW_FLAG_ASYNC the status goes to
+ * opt->device_status; with BGW_FLAG_PROFILE the replay is timed. */
+int bgw_gpp_batch_execute(bgw_gpp_batch *batch, const bgw_options *opt);
+int bgw_gpp_batch_info(const bgw_gpp_batch *batch, int32_t *elems_per_thread,
+                       int32_t *grid, int64_t *total_items);
+int bgw_gpp_batch_destroy(bgw_gpp_batch *batch);
+
 /* --------------------------------------------------- GPP, no allocation --
  * No counterpart in the reference.  A variant of bgw_noflagOCC_solver for
  * callers that cannot allocate GPU memory: code whose device memory is all
