@@ -394,6 +394,23 @@ def run_ours(args, world, rank, local):
                          "algorithmic_bytes_per_launch": p["main_bytes"],
                          "achieved_GBps": p["main_bytes"] / (fk * 1e-3) / 1e9,
                          "traffic": traffic_from_profiles("ff_contract_kernel")}}
+        # Mixed precision: integer-slice products on the tcgen05 tensor cores.
+        for _ in range(2):
+            bgw.ff_sigma(fd, stream=sh, precision="mixed", flags=bgw.FLAG_PROFILE)
+        mks, mds = [], []
+        for _ in range(args.steps):
+            mix_out = bgw.ff_sigma(fd, stream=sh, precision="mixed", flags=bgw.FLAG_PROFILE)
+            pm = bgw.last_profile()
+            mks.append(pm["main_kernel_ms"])
+            mds.append(pm["device_ms"])
+        mk = statistics.mean(mks)
+        extra["ff_mixed"] = {
+            "precision": "mixed: 6 int8 digits per operand, levels 2..7 (21 digit pairs), FP64 recombination",
+            "s_per_sigma": statistics.mean(mds) / 1e3, "kernel": pm["main_kernel"], "contraction_ms": mk,
+            "speedup_vs_fp64": statistics.mean(dms) / statistics.mean(mds),
+            "effective_TFLOPs": pm["flops"] / (mk * 1e-3) / 1e12,
+            "rel_err_vs_fp64": {k: rel_err(a.cpu().numpy(), b.cpu().numpy())
+                                for k, a, b in zip(("achsDtemp", "asxDtemp", "achDtemp_cor"), mix_out, ff_out)}}
         if rank == 0 and not args.no_cpu:
             from oracle.oracle import Reference
             if Reference.available():
@@ -413,6 +430,10 @@ def run_ours(args, world, rank, local):
                     "achsDtemp": rel_err(ff_out[0].cpu().numpy(), ra),
                     "asxDtemp": rel_err(ff_out[1].cpu().numpy(), rs),
                     "achDtemp_cor": rel_err(ff_out[2].cpu().numpy(), rc)}
+                extra["ff_mixed"]["rel_err_vs_reference"] = {
+                    "achsDtemp": rel_err(mix_out[0].cpu().numpy(), ra),
+                    "asxDtemp": rel_err(mix_out[1].cpu().numpy(), rs),
+                    "achDtemp_cor": rel_err(mix_out[2].cpu().numpy(), rc)}
         del fd
 
     # Accuracy against the long-double oracle (exact factored identity).
@@ -548,8 +569,12 @@ def run_only(args, local):
         dims = dict(FF_DIMS)
         if args.bands:
             dims["number_bands"] = args.bands
+        if args.freqs:
+            dims["nFreq"] = args.freqs
         d = bgw.to_device(I.ff_seeded(**dims, seed=1234), dev)
-        call = lambda: bgw.ff_sigma(d, flags=bgw.FLAG_PROFILE)  # noqa: E731
+        prec = "mixed" if args.only.startswith("ff_mixed") else "fp64"
+        fl = bgw.FLAG_PROFILE | (bgw.FLAG_FF_SLICE_ALL if args.only == "ff_mixed_all" else 0)
+        call = lambda: bgw.ff_sigma(d, precision=prec, flags=fl)  # noqa: E731
     for _ in range(args.warmup):
         call()
     profs = []
@@ -582,10 +607,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and oracle check")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-instances extra")
-    ap.add_argument("--only", choices=["gpp_bandloop", "gpp_mixed", "gpp_factored", "gpp_adjoint", "ff"],
+    ap.add_argument("--only", choices=["gpp_bandloop", "gpp_mixed", "gpp_factored", "gpp_adjoint", "ff", "ff_mixed",
+                                       "ff_mixed_all"],
                     default=None,
                     help="diagnostic: time one kernel path only (for profilers)")
     ap.add_argument("--bands", type=int, default=0, help="with --only: number_bands override")
+    ap.add_argument("--freqs", type=int, default=0, help="with --only ff*: nFreq override")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

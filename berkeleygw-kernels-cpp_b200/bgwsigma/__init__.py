@@ -34,6 +34,7 @@ PRECISION = {"fp64": 0, "mixed": 1}
 GPP_ALGO = {"bandloop": 0, "factored": 1, "auto": 2}
 FLAG_ASYNC = 1
 FLAG_PROFILE = 2
+FLAG_FF_SLICE_ALL = 4
 
 # Every extern "C" symbol include/bgw_sigma.h declares.
 EXPORTS = ("bgw_options_init", "bgw_noflagOCC_solver", "bgw_achsDtemp_Kernel", "bgw_asxDtemp_Kernel",

@@ -208,7 +208,6 @@ int ff_call(int64_t nb, int64_t nvband, int64_t nE, int64_t G, int64_t P, int64_
   Call c(opt);
   if (c.st != BGW_OK) return c.st;
   CallEnv *env = &c.env;
-  if (env->opt.precision != BGW_PRECISION_FP64) return BGW_ERR_UNSUPPORTED;
 
   // Band classification needs ekq and dFreqGrid on the host.
   const int64_t ne = (want_asx || want_cor) ? nb : 0;
@@ -272,9 +271,14 @@ int ff_call(int64_t nb, int64_t nvband, int64_t nE, int64_t G, int64_t P, int64_
     o_cor = cor;
   }
   const int64_t nb_w = (want_achs || want_cor) ? nb : nvband;
-  BGW_TRY(ff_launch(env, plan, nb_w, nE, G, P, (const int32_t *)d_inv, (const int32_t *)d_ind, indinv_len,
-                    (const double2 *)d_am, (const double2 *)d_an, (const double *)d_vc, (const double2 *)d_R, r_f0,
-                    (const double2 *)d_A, a_f0, o_achs, o_asx, o_cor));
+  if (env->opt.precision == BGW_PRECISION_MIXED)
+    BGW_TRY(ff_launch_mixed(env, plan, nb, nb_w, nE, G, P, (const int32_t *)d_inv, (const int32_t *)d_ind,
+                            indinv_len, (const double2 *)d_am, (const double2 *)d_an, (const double *)d_vc,
+                            (const double2 *)d_R, r_f0, (const double2 *)d_A, a_f0, o_achs, o_asx, o_cor));
+  else
+    BGW_TRY(ff_launch(env, plan, nb_w, nE, G, P, (const int32_t *)d_inv, (const int32_t *)d_ind, indinv_len,
+                      (const double2 *)d_am, (const double2 *)d_an, (const double *)d_vc, (const double2 *)d_R,
+                      r_f0, (const double2 *)d_A, a_f0, o_achs, o_asx, o_cor));
   if (env->host) {
     if (want_achs)
       BGW_CUDA_TRY(cudaMemcpyAsync(achs, o_achs, 2 * sizeof(double), cudaMemcpyDeviceToHost, env->stream));

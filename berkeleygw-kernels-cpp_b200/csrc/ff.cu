@@ -134,45 +134,29 @@ int build_plan(int64_t nb, int64_t nvband, int64_t P, int64_t G, int64_t nFreq, 
       groups[{OUT_COR, SRC_RA, fc.ifreq + 1}].push_back({(int32_t)n1, 0, fc.f2 * s});
     }
   }
-  // Base tiles (no k split), then a k split that fills the GPU.
-  const int64_t ptiles = (P + kTN - 1) / kTN;
-  int64_t base = 0;
-  for (auto &kv : groups) base += ((int64_t)kv.second.size() + kTM - 1) / kTM * ptiles;
-  const int64_t kblocks = (G + kBK - 1) / kBK;
-  int64_t ksplit = base > 0 ? (target_ctas + base - 1) / base : 1;
-  ksplit = std::max<int64_t>(1, std::min<int64_t>(ksplit, std::max<int64_t>(1, kblocks / 8)));
-  const int64_t kb_per = (kblocks + ksplit - 1) / ksplit;
-  ksplit = (kblocks + kb_per - 1) / kb_per;
-
   plan->rows.clear();
   plan->tiles.clear();
+  plan->groups.clear();
   plan->useful_cmacs = 0.0;
-  int cur_out = 0;
-  plan->seg[0] = 0;
   for (auto &kv : groups) {
     const GroupKey &key = kv.first;
-    while (cur_out < key.out) plan->seg[++cur_out] = (int)plan->tiles.size();
     const int32_t rb = (int32_t)plan->rows.size();
     const int64_t nrows = (int64_t)kv.second.size();
     plan->rows.insert(plan->rows.end(), kv.second.begin(), kv.second.end());
+    plan->groups.push_back({key.out, key.src, key.f, rb, (int32_t)nrows});
     plan->useful_cmacs += (double)nrows * (double)P * (double)G;
-    for (int64_t r0 = 0; r0 < nrows; r0 += kTM)
-      for (int64_t p0 = 0; p0 < P; p0 += kTN)
-        for (int64_t ks = 0; ks < ksplit; ++ks) {
-          FFTile t;
-          t.src = key.src;
-          t.f = key.f;
-          t.row_begin = rb + (int32_t)r0;
-          t.row_count = (int32_t)std::min<int64_t>(kTM, nrows - r0);
-          t.p_begin = (int32_t)p0;
-          t.k_begin = (int32_t)(ks * kb_per * kBK);
-          const int64_t kend = std::min<int64_t>(G, (ks + 1) * kb_per * kBK);
-          t.k_count = (int32_t)std::max<int64_t>(0, kend - t.k_begin);
-          t.out = key.out;
-          plan->tiles.push_back(t);
-        }
   }
-  while (cur_out < OUT_COUNT) plan->seg[++cur_out] = (int)plan->tiles.size();
+  // Tiles in group (= output) order; seg[o] = first tile of output o.
+  ff_fp64_tiles(plan->groups, P, G, target_ctas, &plan->tiles);
+  for (int o = 0; o <= OUT_COUNT; ++o) {
+    int first = (int)plan->tiles.size();
+    for (int i = 0; i < (int)plan->tiles.size(); ++i)
+      if (plan->tiles[i].out >= o) {
+        first = i;
+        break;
+      }
+    plan->seg[o] = first;
+  }
   // Distinct (array, slice) pairs read: 1 per R or A slice, 2 per R - A slice.
   {
     std::map<std::pair<int, int>, int> seen;
@@ -224,10 +208,12 @@ __global__ void ff_w_kernel(int nb, int P, int G, const int *__restrict__ inv, c
 }
 
 // ------------------------------------------------------- DMMA contraction --
+// Not volatile: the MMA has no side effects, so the compiler may interleave
+// independent accumulators to hide the DMMA latency.
 __device__ __forceinline__ void dmma_f64(double &c0, double &c1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
-               : "+d"(c0), "+d"(c1)
-               : "d"(a), "d"(b));
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+      : "+d"(c0), "+d"(c1)
+      : "d"(a), "d"(b));
 }
 
 // cp.async (16-byte, L2-only) global -> shared copies.  `valid` false
@@ -261,14 +247,14 @@ struct FFSmem {
 // (rows gathered by band index, out-of-range rows / k zero-filled); for the
 // COR sum the I_epsR and I_epsA rows are staged separately and R - A is
 // formed when the B fragments are read.
-__global__ void __launch_bounds__(kFFThreads, 2)
-    ff_contract_kernel(const FFTile *__restrict__ tiles, const FFRow *__restrict__ rows, int P, int G,
-                       const double2 *__restrict__ aqsn, const double2 *__restrict__ R, int r_f0,
-                       const double2 *__restrict__ A, int a_f0, const double2 *__restrict__ W,
-                       double *__restrict__ partials) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  FFSmem &sm = *reinterpret_cast<FFSmem *>(smem_raw);
-  const FFTile t = tiles[blockIdx.x];
+// MC = 8-row blocks of the tile that hold real rows (1..4): the all-padding
+// blocks of a partly filled tile are neither copied nor multiplied.
+template <int MC>
+__device__ __forceinline__ void contract_tile(FFSmem &sm, const FFTile &t, const FFRow *__restrict__ rows, int P,
+                                              int G, const double2 *__restrict__ aqsn,
+                                              const double2 *__restrict__ R, int r_f0,
+                                              const double2 *__restrict__ A, int a_f0,
+                                              const double2 *__restrict__ W, double *__restrict__ partials) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g8 = lane >> 2, t4 = lane & 3;
 
@@ -309,6 +295,7 @@ __global__ void __launch_bounds__(kFFThreads, 2)
     const size_t off = (size_t)kb * kBK;
 #pragma unroll
     for (int q = 0; q < kAq; ++q) {
+      if (q * (kFFThreads / kBK) >= MC * 8) continue;  // rows of this copy are all padding
       const int idx = q * kFFThreads + tid;
       const bool v = kin && a_ok[q];
       cp_async16(&s.a[(idx / kBK) * kLds + kc], v ? a_src[q] + off : aqsn, v);
@@ -347,7 +334,7 @@ __global__ void __launch_bounds__(kFFThreads, 2)
     for (int ks = 0; ks < kBK / 4; ++ks) {
       double ar[4], ai[4], br[2], bi[2], bn[2];
 #pragma unroll
-      for (int m = 0; m < 4; ++m) {
+      for (int m = 0; m < MC; ++m) {
         const double2 v = sa[(m * 8 + g8) * kLds + ks * 4 + t4];
         ar[m] = v.x;
         ai[m] = v.y;
@@ -364,13 +351,20 @@ __global__ void __launch_bounds__(kFFThreads, 2)
         bi[n] = v.y;
         bn[n] = -v.y;
       }
+      // Two sweeps over the 4 MC independent accumulators, so that the two
+      // MMAs into one accumulator are 4 MC instructions apart.
 #pragma unroll
-      for (int m = 0; m < 4; ++m)
+      for (int m = 0; m < MC; ++m)
 #pragma unroll
         for (int n = 0; n < 2; ++n) {
           dmma_f64(cr[m][n][0], cr[m][n][1], ar[m], br[n]);
-          dmma_f64(cr[m][n][0], cr[m][n][1], ai[m], bn[n]);
           dmma_f64(ci[m][n][0], ci[m][n][1], ar[m], bi[n]);
+        }
+#pragma unroll
+      for (int m = 0; m < MC; ++m)
+#pragma unroll
+        for (int n = 0; n < 2; ++n) {
+          dmma_f64(cr[m][n][0], cr[m][n][1], ai[m], bn[n]);
           dmma_f64(ci[m][n][0], ci[m][n][1], ai[m], br[n]);
         }
     }
@@ -381,7 +375,7 @@ __global__ void __launch_bounds__(kFFThreads, 2)
   // accumulator entries (row m*8+g8, column warp*16 + n*8 + 2*t4 + j).
   double vr = 0.0, vi = 0.0;
 #pragma unroll
-  for (int m = 0; m < 4; ++m) {
+  for (int m = 0; m < MC; ++m) {
     const int r = m * 8 + g8;
     if (r >= t.row_count) continue;
     const FFRow row = rows[t.row_begin + r];
@@ -402,6 +396,22 @@ __global__ void __launch_bounds__(kFFThreads, 2)
   if (tid == 0) {
     partials[(size_t)blockIdx.x * 2 + 0] = v[0];
     partials[(size_t)blockIdx.x * 2 + 1] = v[1];
+  }
+}
+
+__global__ void __launch_bounds__(kFFThreads, 2)
+    ff_contract_kernel(const FFTile *__restrict__ tiles, const FFRow *__restrict__ rows, int P, int G,
+                       const double2 *__restrict__ aqsn, const double2 *__restrict__ R, int r_f0,
+                       const double2 *__restrict__ A, int a_f0, const double2 *__restrict__ W,
+                       double *__restrict__ partials) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  FFSmem &sm = *reinterpret_cast<FFSmem *>(smem_raw);
+  const FFTile t = tiles[blockIdx.x];
+  switch (min(4, (t.row_count + 7) >> 3)) {  // uniform per CTA
+    case 1: contract_tile<1>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
+    case 2: contract_tile<2>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
+    case 3: contract_tile<3>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
+    default: contract_tile<4>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
   }
 }
 
@@ -455,6 +465,71 @@ int ff_make_plan(CallEnv *env, int64_t nb, int64_t nvband, int64_t P, int64_t G,
   BGW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ff_contract_kernel, kFFThreads, smem));
   return build_plan(nb, nvband, P, G, nFreq, fmin, fstep, occ, ekq_h, grid_h, want_achs, want_asx, want_cor,
                     2 * env->ws->sm_count * std::max(per_sm, 1), plan);
+}
+
+int ff_build_w(CallEnv *env, int64_t nb_w, int64_t G, int64_t P, const int32_t *inv, const int32_t *indinv,
+               int64_t indinv_len, const double2 *am, const double *vc, double2 **W_out) {
+  void *W = nullptr;
+  BGW_TRY(ws_reserve(env->ws, SLOT_TABLE2, sizeof(double2) * (size_t)std::max<int64_t>(nb_w * P, 1), &W));
+  if (nb_w * P > 0) {
+    int g = (int)std::min<long long>((nb_w * P + 255) / 256, (long long)env->ws->sm_count * 8);
+    ff_w_kernel<<<g, 256, 0, env->stream>>>((int)nb_w, (int)P, (int)G, inv, indinv, indinv_len, am, vc,
+                                            (double2 *)W, env->d_status);
+    count_launch();
+    BGW_CUDA_TRY(cudaGetLastError());
+  }
+  *W_out = static_cast<double2 *>(W);
+  return BGW_OK;
+}
+
+void ff_fp64_tiles(const std::vector<FFGroup> &groups, int64_t P, int64_t G, int target_ctas,
+                   std::vector<FFTile> *tiles) {
+  const int64_t ptiles = (P + kTN - 1) / kTN;
+  int64_t base = 0;
+  for (const auto &g : groups) base += ((int64_t)g.row_count + kTM - 1) / kTM * ptiles;
+  const int64_t kblocks = (G + kBK - 1) / kBK;
+  int64_t ksplit = base > 0 ? (target_ctas + base - 1) / base : 1;
+  ksplit = std::max<int64_t>(1, std::min<int64_t>(ksplit, std::max<int64_t>(1, kblocks / 8)));
+  const int64_t kb_per = (kblocks + ksplit - 1) / ksplit;
+  ksplit = (kblocks + kb_per - 1) / kb_per;
+  // Row tiles innermost: the tiles that read the same X block (p0, k range)
+  // are launched next to each other and share it through L2.
+  for (const auto &g : groups)
+    for (int64_t p0 = 0; p0 < P; p0 += kTN)
+      for (int64_t ks = 0; ks < ksplit; ++ks)
+        for (int64_t r0 = 0; r0 < g.row_count; r0 += kTM) {
+          FFTile t;
+          t.src = g.src;
+          t.f = g.f;
+          t.row_begin = g.row_begin + (int32_t)r0;
+          t.row_count = (int32_t)std::min<int64_t>(kTM, g.row_count - r0);
+          t.p_begin = (int32_t)p0;
+          t.k_begin = (int32_t)(ks * kb_per * kBK);
+          const int64_t kend = std::min<int64_t>(G, (ks + 1) * kb_per * kBK);
+          t.k_count = (int32_t)std::max<int64_t>(0, kend - t.k_begin);
+          t.out = g.out;
+          tiles->push_back(t);
+        }
+}
+
+int ff_fp64_per_sm(int *per_sm) {
+  const size_t smem = sizeof(FFSmem);
+  BGW_CUDA_TRY(cudaFuncSetAttribute(ff_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  BGW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, ff_contract_kernel, kFFThreads, smem));
+  return BGW_OK;
+}
+
+int ff_launch_fp64_tiles(cudaStream_t stream, const FFTile *d_tiles, int ntiles, const FFRow *d_rows, int64_t P,
+                         int64_t G, const double2 *an, const double2 *R, int r_f0, const double2 *A, int a_f0,
+                         const double2 *W, double *partials) {
+  if (ntiles <= 0) return BGW_OK;
+  int per_sm = 0;
+  BGW_TRY(ff_fp64_per_sm(&per_sm));
+  ff_contract_kernel<<<ntiles, kFFThreads, sizeof(FFSmem), stream>>>(d_tiles, d_rows, (int)P, (int)G, an, R, r_f0,
+                                                                      A, a_f0, W, partials);
+  count_launch();
+  BGW_CUDA_TRY(cudaGetLastError());
+  return BGW_OK;
 }
 
 // Enqueues a planned FF evaluation.  Device pointers; R / A point at

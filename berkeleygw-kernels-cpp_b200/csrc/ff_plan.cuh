@@ -21,7 +21,14 @@ struct FFTile {
   int32_t p_begin, k_begin, k_count, out;
 };
 
+// One band group: rows [row_begin, row_begin + row_count) of FFPlan::rows,
+// all contracted with the same slice f of source `src`, summed into `out`.
+struct FFGroup {
+  int32_t out, src, f, row_begin, row_count;
+};
+
 struct FFPlan {
+  std::vector<FFGroup> groups;
   std::vector<FFRow> rows;
   std::vector<FFTile> tiles;
   int seg[OUT_COUNT + 1] = {0, 0, 0, 0};  // tile range of each output
@@ -36,6 +43,25 @@ struct FFPlan {
 int ff_make_plan(CallEnv *env, int64_t nb, int64_t nvband, int64_t P, int64_t G, int64_t nFreq, double fmin,
                  double fstep, double occ, const double *ekq_h, const double *grid_h, bool want_achs,
                  bool want_asx, bool want_cor, FFPlan *plan);
+
+// Builds W[n1][p] = conj(aqsm[n1][igp]) vcoul[igp] for n1 < nb_w on `stream`.
+int ff_build_w(CallEnv *env, int64_t nb_w, int64_t G, int64_t P, const int32_t *inv, const int32_t *indinv,
+               int64_t indinv_len, const double2 *am, const double *vc, double2 **W_out);
+// FP64 (DMMA) tiles of the given groups, appended to `tiles` (k split sized
+// for `target_ctas` together with `base_tiles` tiles already planned).
+void ff_fp64_tiles(const std::vector<FFGroup> &groups, int64_t P, int64_t G, int target_ctas,
+                   std::vector<FFTile> *tiles);
+// Launches the DMMA contraction over device tiles; one complex partial per
+// tile at `partials`.
+int ff_launch_fp64_tiles(cudaStream_t stream, const FFTile *d_tiles, int ntiles, const FFRow *d_rows, int64_t P,
+                         int64_t G, const double2 *an, const double2 *R, int r_f0, const double2 *A, int a_f0,
+                         const double2 *W, double *partials);
+int ff_fp64_per_sm(int *per_sm);
+// Mixed precision (integer slices on tcgen05) evaluation of a plan.
+int ff_launch_mixed(CallEnv *env, const FFPlan &plan, int64_t nb, int64_t nb_w, int64_t nE, int64_t G, int64_t P,
+                    const int32_t *inv, const int32_t *indinv, int64_t indinv_len, const double2 *am,
+                    const double2 *an, const double *vc, const double2 *R, int r_f0, const double2 *A, int a_f0,
+                    double *achs_dev, double *asx_dev, double *cor_dev);
 
 // Enqueues a planned FF evaluation.  Device pointers; R / A point at
 // frequency slice r_f0 / a_f0.  Outputs are device pointers (nullptr skips).

@@ -61,9 +61,15 @@ enum {
   BGW_FLAG_ASYNC = 1,  /* device memory only: enqueue on `stream` and return
                           without synchronising; the device-side status is
                           written to options->device_status (required).   */
-  BGW_FLAG_PROFILE = 2 /* time the call's dominant kernel and all its device
+  BGW_FLAG_PROFILE = 2, /* time the call's dominant kernel and all its device
                           work with CUDA events on `stream`; read back with
                           bgw_last_profile() (synchronous calls only).     */
+  BGW_FLAG_FF_SLICE_ALL = 4 /* FF with BGW_PRECISION_MIXED: integer-slice
+                          tensor-core products for every band group of more
+                          than 16 rows.  Default: only groups of at least
+                          128 rows (the sums over all bands), where they
+                          beat the FP64 tensor cores; smaller groups stay
+                          FP64.                                            */
 };
 
 typedef struct bgw_options {
