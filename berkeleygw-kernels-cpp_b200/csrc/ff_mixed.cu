@@ -25,7 +25,7 @@
 // issues the MMAs (M = 128 rows, N = 128 columns, K = 32 per instruction)
 // into two int32 TMEM accumulators (Re, Im) per level, double-buffered in the
 // 512 columns so that a level drains while the next one multiplies;
-// warps 2-5 drain each finished level (tcgen05.ld), convert to FP64 and fold
+// warps 2-9 drain each finished level (tcgen05.ld), convert to FP64 and fold
 // W(band, p) 2^eB(p) 128^-L into a per-row sum; the row factor coef 2^eA and
 // a fixed-order reduction give one partial per segment.  Every mbarrier wait
 // is bounded.  Groups of at most 16 rows (the SX sum's) go to the FP64 DMMA
@@ -58,7 +58,8 @@ constexpr int kAPlanes = 3;                  // Re, Im, -Im
 constexpr int kXPlanes = 2;                  // Re, Im
 constexpr int kStages = 5;
 constexpr int kAccBufs = 512 / (2 * kN);     // TMEM accumulator sets (Re + Im)
-constexpr int kMixThreads = 192;             // warp 0 copies, warp 1 MMAs, warps 2-5 epilogue
+constexpr int kEpiWarps = 8;                 // two per TMEM lane quarter (column halves)
+constexpr int kMixThreads = 64 + 32 * kEpiWarps;  // warp 0 copies, warp 1 MMAs, warps 2.. epilogue
 constexpr int kMixMinRows = 128;             // default: smaller groups use the FP64 kernel
 constexpr int kMixMinRowsAll = 17;           // with BGW_FLAG_FF_SLICE_ALL
 constexpr int kMaxSegBlocks = 128;           // 8192 k: every int32 accumulator stays below 2^31
@@ -239,7 +240,7 @@ struct __align__(128) MixSmem {
   int8_t x[kStages][kXPlanes][kXTile];
   uint64_t full[kStages], empty[kStages], acc_full[kAccBufs], acc_empty[kAccBufs], done;
   uint32_t tmem;
-  double red[4][2];
+  double red[kEpiWarps][2];
 };
 
 __device__ __forceinline__ bool wait_or_flag(uint64_t *bar, uint32_t parity, int *status) {
@@ -270,7 +271,7 @@ __global__ void __launch_bounds__(kMixThreads, 1)
     }
     for (int i = 0; i < kAccBufs; ++i) {
       mbar_init(&sm.acc_full[i], 1);
-      mbar_init(&sm.acc_empty[i], 4);
+      mbar_init(&sm.acc_empty[i], kEpiWarps);
     }
     mbar_init(&sm.done, 1);
     fence_mbar_init();
@@ -288,7 +289,8 @@ __global__ void __launch_bounds__(kMixThreads, 1)
   if (warp == 0) {
     // ---- producer: digit tiles in (segment, level, pair, k block) order.
     if (lane == 0) {
-      int step = 0;
+      int step = 0, st = 0;
+      uint32_t ph = 0;  // phase of the current pass over the stages
       bool ok = true;
       for (int sg = seg0; sg < seg1 && ok; ++sg) {
         const MixSeg S = segs[sg];
@@ -296,44 +298,55 @@ __global__ void __launch_bounds__(kMixThreads, 1)
         const MixX X = xs[Gp.xid];
         const long long a_plane = (long long)Gp.row_tiles * KB * kATile;
         const long long x_plane = (long long)PT * KB * kXTile;
-        const int8_t *a_base = pack + Gp.a_off + (long long)S.rt * KB * kATile;
-        const int8_t *x_base = pack + X.b_off + (long long)S.pt * KB * kXTile;
+        const int8_t *a_base = pack + Gp.a_off + ((long long)S.rt * KB + S.kb0) * kATile;
+        const int8_t *x_base = pack + X.b_off + ((long long)S.pt * KB + S.kb0) * kXTile;
         for (int li = 0; li < kLevels && ok; ++li) {
           const int L = li + 2;
           for (int s = pair_lo(L); s <= pair_hi(L) && ok; ++s) {
-            const int u = L - 2 - s;
+            const int8_t *ap = a_base + s * a_plane;
+            const int8_t *xp = x_base + (L - 2 - s) * x_plane;
             for (int kb = S.kb0; kb < S.kb1; ++kb) {
-              const int st = step % kStages;
-              if (step >= kStages && !wait_or_flag(&sm.empty[st], ((step / kStages) - 1) & 1, status)) {
+              if (step >= kStages && !wait_or_flag(&sm.empty[st], ph ^ 1u, status)) {
                 ok = false;
                 break;
               }
               mbar_expect_tx(&sm.full[st], kStageBytes);
+#pragma unroll
               for (int pl = 0; pl < kAPlanes; ++pl)
-                bulk_g2s(sm.a[st][pl], a_base + (pl * kS + s) * a_plane + (long long)kb * kATile, kATile,
-                         &sm.full[st]);
+                bulk_g2s(sm.a[st][pl], ap + pl * kS * a_plane, kATile, &sm.full[st]);
+#pragma unroll
               for (int pl = 0; pl < kXPlanes; ++pl)
-                bulk_g2s(sm.x[st][pl], x_base + (pl * kS + u) * x_plane + (long long)kb * kXTile, kXTile,
-                         &sm.full[st]);
+                bulk_g2s(sm.x[st][pl], xp + pl * kS * x_plane, kXTile, &sm.full[st]);
+              ap += kATile;
+              xp += kXTile;
               ++step;
+              if (++st == kStages) {
+                st = 0;
+                ph ^= 1u;
+              }
             }
           }
         }
       }
       // Copies still in flight (error paths only) land before the CTA exits:
       // wait for the last phase issued on every stage.
-      for (int st = 0; st < kStages; ++st) {
-        if (step <= st) continue;
-        const int last = (step - 1) - ((step - 1 - st) % kStages);
-        (void)wait_or_flag(&sm.full[st], (last / kStages) & 1, status);
+      for (int t = 0; t < kStages; ++t) {
+        if (step <= t) continue;
+        const int last = (step - 1) - ((step - 1 - t) % kStages);
+        (void)wait_or_flag(&sm.full[t], (last / kStages) & 1, status);
       }
     }
     __syncwarp();
   } else if (warp == 1) {
-    // ---- MMA issuer (one thread).
+    // ---- MMA issuer (one thread).  Shared-memory descriptors are built
+    // once; a stage / k step only adds its 16-byte-unit offset to the start
+    // address field (addresses stay below 2^18, so the field never carries).
     if (lane == 0) {
       constexpr uint32_t idesc = tc::idesc_i8(kM, kN);
-      int step = 0, lvl = 0;
+      const uint64_t dA = tc::smem_desc(smem_u32(&sm.a[0][0][0]), kALbo, 128);
+      const uint64_t dX = tc::smem_desc(smem_u32(&sm.x[0][0][0]), kXLbo, 128);
+      int st = 0, lvl = 0;
+      uint32_t ph = 0;
       bool ok = true;
       for (int sg = seg0; sg < seg1 && ok; ++sg) {
         const MixSeg S = segs[sg];
@@ -347,21 +360,21 @@ __global__ void __launch_bounds__(kMixThreads, 1)
           const uint32_t d_re = tmem + (uint32_t)(buf * 2 * kN), d_im = d_re + kN;
           bool first = true;
           for (int s = pair_lo(L); s <= pair_hi(L) && ok; ++s) {
-            for (int kb = S.kb0; kb < S.kb1; ++kb, ++step) {
-              const int st = step % kStages;
-              if (!wait_or_flag(&sm.full[st], (step / kStages) & 1, status)) {
+            for (int kb = S.kb0; kb < S.kb1; ++kb) {
+              if (!wait_or_flag(&sm.full[st], ph, status)) {
                 ok = false;
                 break;
               }
               tc::fence_after();
-              const uint32_t a0 = smem_u32(sm.a[st][0]), a1 = smem_u32(sm.a[st][1]), a2 = smem_u32(sm.a[st][2]);
-              const uint32_t x0 = smem_u32(sm.x[st][0]), x1 = smem_u32(sm.x[st][1]);
+              const uint64_t a_st = dA + (uint64_t)(st * (kAPlanes * kATile / 16));
+              const uint64_t x_st = dX + (uint64_t)(st * (kXPlanes * kXTile / 16));
 #pragma unroll
-              for (int j = 0; j < kBK / 32; ++j) {
-                const uint32_t ka = j * 2 * kALbo, kx = j * 2 * kXLbo;  // 16-k column groups 2j, 2j + 1
-                const uint64_t ar = tc::smem_desc(a0 + ka, kALbo, 128), ai = tc::smem_desc(a1 + ka, kALbo, 128);
-                const uint64_t an = tc::smem_desc(a2 + ka, kALbo, 128);
-                const uint64_t xr = tc::smem_desc(x0 + kx, kXLbo, 128), xi = tc::smem_desc(x1 + kx, kXLbo, 128);
+              for (int j = 0; j < kBK / 32; ++j) {  // 16-k column groups 2j, 2j + 1
+                const uint64_t ar = a_st + (0 * kATile + j * 2 * kALbo) / 16;
+                const uint64_t ai = a_st + (1 * kATile + j * 2 * kALbo) / 16;
+                const uint64_t an = a_st + (2 * kATile + j * 2 * kALbo) / 16;
+                const uint64_t xr = x_st + (0 * kXTile + j * 2 * kXLbo) / 16;
+                const uint64_t xi = x_st + (1 * kXTile + j * 2 * kXLbo) / 16;
                 tc::mma_i8(d_re, ar, xr, idesc, !first);
                 tc::mma_i8(d_re, an, xi, idesc, true);
                 tc::mma_i8(d_im, ar, xi, idesc, !first);
@@ -369,6 +382,10 @@ __global__ void __launch_bounds__(kMixThreads, 1)
                 first = false;
               }
               tc::commit(&sm.empty[st]);  // stage reusable once these MMAs have read it
+              if (++st == kStages) {
+                st = 0;
+                ph ^= 1u;
+              }
             }
           }
           tc::commit(&sm.acc_full[buf]);  // level complete
@@ -378,8 +395,10 @@ __global__ void __launch_bounds__(kMixThreads, 1)
     }
     __syncwarp();
   } else {
-    // ---- epilogue: warps 2-5 own TMEM lane quarters (warp % 4).
-    const int q = warp & 3;
+    // ---- epilogue: warps 2..9; warp w reads TMEM lane quarter w % 4 and
+    // column half (w - 2) / 4.  The W row values of a 16-column chunk are
+    // loaded before the chunk's tensor-memory loads so both latencies overlap.
+    const int e = warp - 2, q = warp & 3, half = e >> 2;
     const int row = q * 32 + lane;
     int lvl = 0;
     bool ok = true;
@@ -391,7 +410,8 @@ __global__ void __launch_bounds__(kMixThreads, 1)
       const MixRow ar = arows[prow];
       const double2 *wrow = W + (size_t)ar.band * P;
       const double *sb = sB + X.sb_off + (size_t)S.w * x_rows_padded;
-      const int p0 = S.pt * kN;
+      const int c0 = half * (kN / 2);  // first tile column of this warp
+      const int p0 = S.pt * kN + c0;
       double tr = 0.0, ti = 0.0;
       for (int li = 0; li < kLevels; ++li, ++lvl) {
         const int buf = lvl % kAccBufs;
@@ -400,19 +420,24 @@ __global__ void __launch_bounds__(kMixThreads, 1)
         if (!ok) continue;
         tc::fence_after();
         double vr = 0.0, vi = 0.0;
-        const uint32_t tb = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * 2 * kN);
-        for (int cc = 0; cc < kN / 16; ++cc) {
+        const uint32_t tb = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * 2 * kN + c0);
+        for (int cc = 0; cc < kN / 32; ++cc) {
+          double2 w[16];
+          double sc[16];
+#pragma unroll
+          for (int c = 0; c < 16; ++c) {
+            const int p = min(p0 + cc * 16 + c, P - 1);
+            w[c] = wrow[p];
+            sc[c] = sb[p];
+          }
           int32_t re[16], im[16];
           tc::ld16(tb + cc * 16, re);
           tc::ld16(tb + kN + cc * 16, im);
           tc::wait_ld();
 #pragma unroll
           for (int c = 0; c < 16; ++c) {
-            const int p = p0 + cc * 16 + c;
-            if (p < P) {
-              const double2 w = wrow[p];
-              const double sc = sb[p];
-              const double wr = w.x * sc, wi = w.y * sc;
+            if (p0 + cc * 16 + c < P) {
+              const double wr = w[c].x * sc[c], wi = w[c].y * sc[c];
               const double cr = (double)re[c], ci = (double)im[c];
               vr = fma(wr, cr, fma(-wi, ci, vr));
               vi = fma(wr, ci, fma(wi, cr, vi));
@@ -435,15 +460,20 @@ __global__ void __launch_bounds__(kMixThreads, 1)
         ti += __shfl_xor_sync(0xffffffffu, ti, o);
       }
       if (lane == 0) {
-        sm.red[q][0] = tr;
-        sm.red[q][1] = ti;
+        sm.red[e][0] = tr;
+        sm.red[e][1] = ti;
       }
-      asm volatile("bar.sync 1, 128;" ::: "memory");  // epilogue warps only
-      if (warp == 2 && lane == 0) {
-        partials[(size_t)sg * 2 + 0] = ((sm.red[0][0] + sm.red[1][0]) + sm.red[2][0]) + sm.red[3][0];
-        partials[(size_t)sg * 2 + 1] = ((sm.red[0][1] + sm.red[1][1]) + sm.red[2][1]) + sm.red[3][1];
+      asm volatile("bar.sync 1, %0;" ::"n"(kEpiWarps * 32) : "memory");  // epilogue warps only
+      if (e == 0 && lane == 0) {
+        double pr = 0.0, pi = 0.0;
+        for (int k = 0; k < kEpiWarps; ++k) {
+          pr += sm.red[k][0];
+          pi += sm.red[k][1];
+        }
+        partials[(size_t)sg * 2 + 0] = pr;
+        partials[(size_t)sg * 2 + 1] = pi;
       }
-      asm volatile("bar.sync 1, 128;" ::: "memory");
+      asm volatile("bar.sync 1, %0;" ::"n"(kEpiWarps * 32) : "memory");
     }
   }
   tc::fence_before();
