@@ -35,6 +35,7 @@ GPP_ALGO = {"bandloop": 0, "factored": 1, "auto": 2}
 FLAG_ASYNC = 1
 FLAG_PROFILE = 2
 FLAG_FF_SLICE_ALL = 4
+FLAG_FF_WX_PER_IW = 8
 
 # Every extern "C" symbol include/bgw_sigma.h declares.
 EXPORTS = ("bgw_options_init", "bgw_noflagOCC_solver", "bgw_achsDtemp_Kernel", "bgw_asxDtemp_Kernel",
@@ -327,11 +328,11 @@ def ff_sigma(inp: FFInputs, *, achs=True, asx=True, cor=True, precision="fp64", 
     return o_achs, o_asx, o_cor
 
 
-def achsDtemp_Kernel(inp: FFInputs, *, precision="fp64", stream=None):
+def achsDtemp_Kernel(inp: FFInputs, *, precision="fp64", stream=None, flags=0):
     lib = load()
     mem = _where(inp)
     out = _ff_out(inp, 1, mem)
-    o = make_options(mem, precision, stream=_stream_handle(inp, stream))
+    o = make_options(mem, precision, stream=_stream_handle(inp, stream), flags=flags)
     st = lib.bgw_achsDtemp_Kernel(inp.number_bands, inp.ngpown, inp.ncouls, _ptr(inp.inv_igp_index),
                                   _ptr(inp.indinv), len(inp.indinv), _ptr(inp.aqsntemp), _ptr(inp.aqsmtemp),
                                   _ptr(inp.I_epsR_array), inp.nFreq, _ptr(inp.vcoul), _ptr(out), ctypes.byref(o))
@@ -339,11 +340,11 @@ def achsDtemp_Kernel(inp: FFInputs, *, precision="fp64", stream=None):
     return out
 
 
-def asxDtemp_Kernel(inp: FFInputs, *, precision="fp64", stream=None):
+def asxDtemp_Kernel(inp: FFInputs, *, precision="fp64", stream=None, flags=0):
     lib = load()
     mem = _where(inp)
     out = _ff_out(inp, max(inp.nfreqeval, 1), mem)
-    o = make_options(mem, precision, stream=_stream_handle(inp, stream))
+    o = make_options(mem, precision, stream=_stream_handle(inp, stream), flags=flags)
     st = lib.bgw_asxDtemp_Kernel(inp.nvband, inp.nfreqeval, inp.ncouls, inp.ngpown, inp.nFreq, inp.freqevalmin,
                                  inp.freqevalstep, inp.occ, _ptr(inp.ekq), _ptr(inp.dFreqGrid),
                                  _ptr(inp.inv_igp_index), _ptr(inp.indinv), len(inp.indinv), _ptr(inp.aqsmtemp),
@@ -353,11 +354,11 @@ def asxDtemp_Kernel(inp: FFInputs, *, precision="fp64", stream=None):
     return out
 
 
-def achDtemp_cor_Kernel(inp: FFInputs, *, precision="fp64", stream=None):
+def achDtemp_cor_Kernel(inp: FFInputs, *, precision="fp64", stream=None, flags=0):
     lib = load()
     mem = _where(inp)
     out = _ff_out(inp, max(inp.nfreqeval, 1), mem)
-    o = make_options(mem, precision, stream=_stream_handle(inp, stream))
+    o = make_options(mem, precision, stream=_stream_handle(inp, stream), flags=flags)
     st = lib.bgw_achDtemp_cor_Kernel(inp.number_bands, inp.nvband, inp.nfreqeval, inp.ncouls, inp.ngpown,
                                      inp.nFreq, inp.freqevalmin, inp.freqevalstep, _ptr(inp.ekq),
                                      _ptr(inp.dFreqGrid), _ptr(inp.inv_igp_index), _ptr(inp.indinv),

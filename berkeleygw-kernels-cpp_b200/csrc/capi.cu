@@ -226,8 +226,9 @@ int ff_call(int64_t nb, int64_t nvband, int64_t nE, int64_t G, int64_t P, int64_
     }
   }
   FFPlan plan;
+  const bool per_iw = (env->opt.flags & BGW_FLAG_FF_WX_PER_IW) != 0;
   BGW_TRY(ff_make_plan(env, nb, nvband, P, G, nFreq, fmin, fstep, occ, ekq_h.data(), grid_h.data(), want_achs,
-                       want_asx, want_cor, &plan));
+                       want_asx, want_cor, per_iw, nE, &plan));
 
   const size_t slice = (size_t)P * (size_t)G * 16;
   const size_t ng = (size_t)nb * (size_t)G * 16;

@@ -101,25 +101,33 @@ struct GroupKey {
 // Builds rows and tiles.  ekq/grid are host copies.
 int build_plan(int64_t nb, int64_t nvband, int64_t P, int64_t G, int64_t nFreq, double fmin, double fstep,
                double occ, const double *ekq, const double *grid, bool want_achs, bool want_asx, bool want_cor,
-               int target_ctas, FFPlan *plan) {
+               bool per_iw, int64_t nE, int target_ctas, FFPlan *plan) {
+  // Evaluation points with a distinct wx: iw = 0 .. nE - 1 with
+  // wx = fmin - ekq + iw fstep, or the reference's single wx = fmin - ekq +
+  // fstep (ff.cpp:245, 337) in slot 0.  Rows of every iw that read the same
+  // slice share one group (one GEMM over that slice).
+  const int64_t n_iw = per_iw ? nE : 1;
+  auto wx_of = [&](int64_t n1, int64_t iw) { return fmin - ekq[n1] + (per_iw ? (double)iw : 1.0) * fstep; };
   std::map<GroupKey, std::vector<FFRow>> groups;
   if (want_achs) {
     auto &g = groups[{OUT_ACHS, SRC_R, 1}];
     for (int64_t n1 = 0; n1 < nb; ++n1) g.push_back({(int32_t)n1, 0, -0.5});
   }
   if (want_asx) {
+    for (int64_t iw = 0; iw < n_iw; ++iw)
     for (int64_t n1 = 0; n1 < nvband; ++n1) {
-      const double wx = fmin - ekq[n1] + fstep;
+      const double wx = wx_of(n1, iw);
       const Fact fc = compute_fact_host(wx, (int)nFreq, grid, 1, false);
       const int src = wx > 0 ? SRC_R : SRC_A;
-      groups[{OUT_ASX, src, fc.ifreq}].push_back({(int32_t)n1, 0, fc.f1 * occ});
-      groups[{OUT_ASX, src, fc.ifreq + 1}].push_back({(int32_t)n1, 0, fc.f2 * occ});
+      groups[{OUT_ASX, src, fc.ifreq}].push_back({(int32_t)n1, (int32_t)iw, fc.f1 * occ});
+      groups[{OUT_ASX, src, fc.ifreq + 1}].push_back({(int32_t)n1, (int32_t)iw, fc.f2 * occ});
     }
   }
   if (want_cor) {
+    for (int64_t iw = 0; iw < n_iw; ++iw)
     for (int64_t n1 = 0; n1 < nb; ++n1) {
       const bool flag_occ = n1 < nvband;
-      const double wx = fmin - ekq[n1] + fstep;
+      const double wx = wx_of(n1, iw);
       const Fact fc = compute_fact_host(wx, (int)nFreq, grid, 2, flag_occ);
       double s;
       if (wx > 0) {
@@ -130,14 +138,15 @@ int build_plan(int64_t nb, int64_t nvband, int64_t P, int64_t G, int64_t nFreq, 
       } else {
         continue;
       }
-      groups[{OUT_COR, SRC_RA, fc.ifreq}].push_back({(int32_t)n1, 0, fc.f1 * s});
-      groups[{OUT_COR, SRC_RA, fc.ifreq + 1}].push_back({(int32_t)n1, 0, fc.f2 * s});
+      groups[{OUT_COR, SRC_RA, fc.ifreq}].push_back({(int32_t)n1, (int32_t)iw, fc.f1 * s});
+      groups[{OUT_COR, SRC_RA, fc.ifreq + 1}].push_back({(int32_t)n1, (int32_t)iw, fc.f2 * s});
     }
   }
   plan->rows.clear();
   plan->tiles.clear();
   plan->groups.clear();
   plan->useful_cmacs = 0.0;
+  plan->per_iw = per_iw;
   for (auto &kv : groups) {
     const GroupKey &key = kv.first;
     const int32_t rb = (int32_t)plan->rows.size();
@@ -237,6 +246,7 @@ struct FFStage {
 struct FFSmem {
   FFStage st[kStages];
   double red[(kFFThreads / 32) * 2];
+  double row_red[kFFThreads / 32][kTM][2];  // per-row partials of each warp
 };
 
 // One CTA per tile.  4 warps; warp w owns G' columns [16w, 16w + 16) of the
@@ -249,7 +259,7 @@ struct FFSmem {
 // formed when the B fragments are read.
 // MC = 8-row blocks of the tile that hold real rows (1..4): the all-padding
 // blocks of a partly filled tile are neither copied nor multiplied.
-template <int MC>
+template <int MC, bool ROWS>
 __device__ __forceinline__ void contract_tile(FFSmem &sm, const FFTile &t, const FFRow *__restrict__ rows, int P,
                                               int G, const double2 *__restrict__ aqsn,
                                               const double2 *__restrict__ R, int r_f0,
@@ -373,9 +383,13 @@ __device__ __forceinline__ void contract_tile(FFSmem &sm, const FFTile &t, const
 
   // Epilogue: sum_r coef(r) sum_p W(band(r), p) C(r, p) over this thread's
   // accumulator entries (row m*8+g8, column warp*16 + n*8 + 2*t4 + j).
+  // ROWS: one partial per tile row instead (rows of one tile may feed
+  // different outputs), reduced over the 4 lanes and 4 warps sharing a row.
   double vr = 0.0, vi = 0.0;
+  double rv[MC][2];
 #pragma unroll
   for (int m = 0; m < MC; ++m) {
+    rv[m][0] = rv[m][1] = 0.0;
     const int r = m * 8 + g8;
     if (r >= t.row_count) continue;
     const FFRow row = rows[t.row_begin + r];
@@ -387,9 +401,41 @@ __device__ __forceinline__ void contract_tile(FFSmem &sm, const FFTile &t, const
         if (p >= P) continue;
         const double2 w = W[(size_t)row.band * P + p];
         const double xr = cr[m][n][j], xi = ci[m][n][j];
-        vr = fma(row.coef, xr * w.x - xi * w.y, vr);
-        vi = fma(row.coef, xr * w.y + xi * w.x, vi);
+        if (ROWS) {
+          rv[m][0] = fma(row.coef, xr * w.x - xi * w.y, rv[m][0]);
+          rv[m][1] = fma(row.coef, xr * w.y + xi * w.x, rv[m][1]);
+        } else {
+          vr = fma(row.coef, xr * w.x - xi * w.y, vr);
+          vi = fma(row.coef, xr * w.y + xi * w.x, vi);
+        }
       }
+  }
+  if (ROWS) {
+#pragma unroll
+    for (int m = 0; m < MC; ++m)
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        rv[m][k] += __shfl_xor_sync(0xffffffffu, rv[m][k], 1);
+        rv[m][k] += __shfl_xor_sync(0xffffffffu, rv[m][k], 2);
+      }
+    if (t4 == 0)
+#pragma unroll
+      for (int m = 0; m < MC; ++m) {
+        sm.row_red[warp][m * 8 + g8][0] = rv[m][0];
+        sm.row_red[warp][m * 8 + g8][1] = rv[m][1];
+      }
+    __syncthreads();
+    if (tid < kTM) {
+      double pr = 0.0, pi = 0.0;
+      if (tid < MC * 8)
+        for (int w = 0; w < kFFThreads / 32; ++w) {
+          pr += sm.row_red[w][tid][0];
+          pi += sm.row_red[w][tid][1];
+        }
+      partials[((size_t)blockIdx.x * kTM + tid) * 2 + 0] = pr;
+      partials[((size_t)blockIdx.x * kTM + tid) * 2 + 1] = pi;
+    }
+    return;
   }
   double v[2] = {vr, vi};
   block_sum<2, kFFThreads>(v, sm.red);
@@ -403,15 +449,25 @@ __global__ void __launch_bounds__(kFFThreads, 2)
     ff_contract_kernel(const FFTile *__restrict__ tiles, const FFRow *__restrict__ rows, int P, int G,
                        const double2 *__restrict__ aqsn, const double2 *__restrict__ R, int r_f0,
                        const double2 *__restrict__ A, int a_f0, const double2 *__restrict__ W,
-                       double *__restrict__ partials) {
+                       double *__restrict__ partials, int per_row) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   FFSmem &sm = *reinterpret_cast<FFSmem *>(smem_raw);
   const FFTile t = tiles[blockIdx.x];
-  switch (min(4, (t.row_count + 7) >> 3)) {  // uniform per CTA
-    case 1: contract_tile<1>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
-    case 2: contract_tile<2>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
-    case 3: contract_tile<3>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
-    default: contract_tile<4>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
+  const int mc = min(4, (t.row_count + 7) >> 3);  // uniform per CTA
+  if (per_row) {
+    switch (mc) {
+      case 1: contract_tile<1, true>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
+      case 2: contract_tile<2, true>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
+      case 3: contract_tile<3, true>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
+      default: contract_tile<4, true>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
+    }
+    return;
+  }
+  switch (mc) {
+    case 1: contract_tile<1, false>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
+    case 2: contract_tile<2, false>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
+    case 3: contract_tile<3, false>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
+    default: contract_tile<4, false>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
   }
 }
 
@@ -452,19 +508,42 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// Block o sums the partials whose out_of entry is o, in index order (fixed
+// thread-strided order, then block_sum): bitwise reproducible.  Output o is
+// achsDtemp (o = 0), asxDtemp[o - 1] (o <= nE) or achDtemp_cor[o - 1 - nE].
+__global__ void __launch_bounds__(256)
+    ff_slot_finalize_kernel(const double *__restrict__ partials, const int *__restrict__ out_of, int n, int nE,
+                            double *__restrict__ achs, double *__restrict__ asx, double *__restrict__ cor) {
+  __shared__ double red[8 * 2];
+  const int o = blockIdx.x;
+  double v[2] = {0.0, 0.0};
+  for (int i = threadIdx.x; i < n; i += 256)
+    if (out_of[i] == o) {
+      v[0] += partials[(size_t)i * 2];
+      v[1] += partials[(size_t)i * 2 + 1];
+    }
+  block_sum<2, 256>(v, red);
+  if (threadIdx.x != 0) return;
+  double *dst = o == 0 ? achs : o <= nE ? (asx ? asx + 2 * (o - 1) : nullptr) : (cor ? cor + 2 * (o - 1 - nE) : nullptr);
+  if (dst) {
+    dst[0] = v[0];
+    dst[1] = v[1];
+  }
+}
+
 }  // namespace
 
 // Builds the plan of the requested sums (host copies of ekq[0..nb) and
 // dFreqGrid); sizes the k split for the device.
 int ff_make_plan(CallEnv *env, int64_t nb, int64_t nvband, int64_t P, int64_t G, int64_t nFreq, double fmin,
                  double fstep, double occ, const double *ekq_h, const double *grid_h, bool want_achs,
-                 bool want_asx, bool want_cor, FFPlan *plan) {
+                 bool want_asx, bool want_cor, bool per_iw, int64_t nE, FFPlan *plan) {
   const size_t smem = sizeof(FFSmem);
   BGW_CUDA_TRY(cudaFuncSetAttribute(ff_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   BGW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ff_contract_kernel, kFFThreads, smem));
   return build_plan(nb, nvband, P, G, nFreq, fmin, fstep, occ, ekq_h, grid_h, want_achs, want_asx, want_cor,
-                    2 * env->ws->sm_count * std::max(per_sm, 1), plan);
+                    per_iw, nE, 2 * env->ws->sm_count * std::max(per_sm, 1), plan);
 }
 
 int ff_build_w(CallEnv *env, int64_t nb_w, int64_t G, int64_t P, const int32_t *inv, const int32_t *indinv,
@@ -521,12 +600,30 @@ int ff_fp64_per_sm(int *per_sm) {
 
 int ff_launch_fp64_tiles(cudaStream_t stream, const FFTile *d_tiles, int ntiles, const FFRow *d_rows, int64_t P,
                          int64_t G, const double2 *an, const double2 *R, int r_f0, const double2 *A, int a_f0,
-                         const double2 *W, double *partials) {
+                         const double2 *W, double *partials, bool per_row) {
   if (ntiles <= 0) return BGW_OK;
   int per_sm = 0;
   BGW_TRY(ff_fp64_per_sm(&per_sm));
   ff_contract_kernel<<<ntiles, kFFThreads, sizeof(FFSmem), stream>>>(d_tiles, d_rows, (int)P, (int)G, an, R, r_f0,
-                                                                      A, a_f0, W, partials);
+                                                                      A, a_f0, W, partials, per_row ? 1 : 0);
+  count_launch();
+  BGW_CUDA_TRY(cudaGetLastError());
+  return BGW_OK;
+}
+
+int ff_fp64_tile_rows() { return kTM; }
+
+void ff_fp64_row_outputs(const std::vector<FFTile> &tiles, const std::vector<FFRow> &rows, int64_t nE,
+                         std::vector<int> *out_of) {
+  for (const auto &t : tiles)
+    for (int r = 0; r < kTM; ++r)
+      out_of->push_back(r < t.row_count ? ff_out_index(t.out, rows[t.row_begin + r].slot, nE) : -1);
+}
+
+int ff_launch_slot_finalize(cudaStream_t stream, const double *partials, const int *out_of, int n, int64_t nE,
+                            double *achs, double *asx, double *cor) {
+  const int n_out = 1 + 2 * (int)nE;
+  ff_slot_finalize_kernel<<<n_out, 256, 0, stream>>>(partials, out_of, n, (int)nE, achs, asx, cor);
   count_launch();
   BGW_CUDA_TRY(cudaGetLastError());
   return BGW_OK;
@@ -565,11 +662,24 @@ int ff_launch(CallEnv *env, const FFPlan &plan, int64_t nb_w, int64_t nE, int64_
     BGW_CUDA_TRY(cudaGetLastError());
   }
   const int ntiles = (int)plan.tiles.size();
-  BGW_TRY(ws_reserve(ws, SLOT_PARTIALS, sizeof(double) * 2 * (size_t)std::max(ntiles, 1), &partials));
+  // Distinct outputs per iw: one partial per tile row, routed by row slot.
+  const bool per_row = plan.per_iw;
+  std::vector<int> out_of;
+  if (per_row) ff_fp64_row_outputs(plan.tiles, plan.rows, nE, &out_of);
+  const size_t n_part = per_row ? out_of.size() : (size_t)ntiles;
+  BGW_TRY(ws_reserve(ws, SLOT_PARTIALS, sizeof(double) * 2 * std::max<size_t>(n_part, 1), &partials));
+  void *d_out_of = nullptr;
+  if (per_row) {
+    BGW_TRY(ws_reserve(ws, SLOT_TABLE1, sizeof(int) * std::max<size_t>(out_of.size(), 1), &d_out_of));
+    if (!out_of.empty())
+      BGW_CUDA_TRY(cudaMemcpyAsync(d_out_of, out_of.data(), sizeof(int) * out_of.size(), cudaMemcpyHostToDevice,
+                                   stream));
+  }
   BGW_TRY(prof_mark(env, 1));
   if (ntiles > 0) {
     ff_contract_kernel<<<ntiles, kFFThreads, smem, stream>>>(d_tiles, d_rows, (int)P, (int)G, an, R, r_f0, A, a_f0,
-                                                             (const double2 *)W, (double *)partials);
+                                                             (const double2 *)W, (double *)partials,
+                                                             per_row ? 1 : 0);
     count_launch();
     BGW_CUDA_TRY(cudaGetLastError());
   }
@@ -585,10 +695,15 @@ int ff_launch(CallEnv *env, const FFPlan &plan, int64_t nb_w, int64_t nE, int64_
     env->prof.main_launches = ntiles > 0 ? 1 : 0;
     std::snprintf(env->prof.main_kernel, sizeof(env->prof.main_kernel), "ff_contract_kernel");
   }
-  ff_finalize_kernel<<<1, 256, 0, stream>>>((const double *)partials, plan.seg[0], plan.seg[1], plan.seg[2],
-                                            plan.seg[3], (int)nE, achs_dev, asx_dev, cor_dev);
-  count_launch();
-  BGW_CUDA_TRY(cudaGetLastError());
+  if (per_row) {
+    BGW_TRY(ff_launch_slot_finalize(stream, (const double *)partials, (const int *)d_out_of, (int)n_part, nE,
+                                    achs_dev, asx_dev, cor_dev));
+  } else {
+    ff_finalize_kernel<<<1, 256, 0, stream>>>((const double *)partials, plan.seg[0], plan.seg[1], plan.seg[2],
+                                              plan.seg[3], (int)nE, achs_dev, asx_dev, cor_dev);
+    count_launch();
+    BGW_CUDA_TRY(cudaGetLastError());
+  }
   // The pageable plan buffer must outlive its (staged) upload.
   BGW_CUDA_TRY(cudaStreamSynchronize(stream));
   return BGW_OK;

@@ -81,6 +81,7 @@ struct MixGroup {       // one integer-slice band group
 };
 struct MixRow {         // packed A row
   int band, g;
+  int slot, pad;        // evaluation point iw of the row
   double coef;          // 0 for padding rows
 };
 struct MixX {           // one distinct X = slice f of R, A or R - A
@@ -253,6 +254,9 @@ __device__ __forceinline__ bool wait_or_flag(uint64_t *bar, uint32_t parity, int
 __device__ __forceinline__ int pair_lo(int L) { return max(0, L - 2 - (kS - 1)); }
 __device__ __forceinline__ int pair_hi(int L) { return min(kS - 1, L - 2); }
 
+// ROWS: one partial per (segment, column half, row) instead of one per
+// segment (rows of one tile may feed different outputs).
+template <bool ROWS>
 __global__ void __launch_bounds__(kMixThreads, 1)
     ff_mix_gemm_kernel(const MixSeg *__restrict__ segs, const int *__restrict__ cta_seg,
                        const MixGroup *__restrict__ groups, const MixRow *__restrict__ arows,
@@ -454,6 +458,11 @@ __global__ void __launch_bounds__(kMixThreads, 1)
       const double f = ar.coef * sA[(size_t)S.w * n_arows + prow];
       tr *= f;
       ti *= f;
+      if (ROWS) {
+        partials[(((size_t)sg * 2 + half) * kM + row) * 2 + 0] = tr;
+        partials[(((size_t)sg * 2 + half) * kM + row) * 2 + 1] = ti;
+        continue;
+      }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
         tr += __shfl_xor_sync(0xffffffffu, tr, o);
@@ -636,12 +645,15 @@ int ff_launch_mixed(CallEnv *env, const FFPlan &plan, int64_t nb, int64_t nb_w, 
     for (int r = 0; r < m.row_tiles * kM; ++r) {
       MixRow mr;
       mr.g = (int)mg.size();
+      mr.pad = 0;
       if (r < g.row_count) {
         const FFRow &fr = plan.rows[g.row_begin + r];
         mr.band = fr.band;
+        mr.slot = fr.slot;
         mr.coef = fr.coef;
       } else {
         mr.band = 0;
+        mr.slot = 0;
         mr.coef = 0.0;
       }
       arows.push_back(mr);
@@ -662,9 +674,25 @@ int ff_launch_mixed(CallEnv *env, const FFPlan &plan, int64_t nb, int64_t nb_w, 
     ff_fp64_tiles(small, P, G, 2 * ws->sm_count * std::max(per_sm, 1), &ft);
   }
   const int nft = (int)ft.size(), nseg = (int)segs.size();
-  std::vector<int> out_of(nft + nseg);
-  for (int i = 0; i < nft; ++i) out_of[i] = ft[i].out;
-  for (int i = 0; i < nseg; ++i) out_of[nft + i] = segs[i].out;
+  // Partials: one per FP64 tile then one per segment; with distinct outputs
+  // per iw, one per FP64 tile row then one per (segment, column half, row).
+  const bool per_row = plan.per_iw;
+  std::vector<int> out_of;
+  if (per_row) {
+    ff_fp64_row_outputs(ft, plan.rows, nE, &out_of);
+    for (int i = 0; i < nseg; ++i)
+      for (int h = 0; h < 2; ++h)
+        for (int r = 0; r < kM; ++r) {
+          const MixRow &mr = arows[(size_t)mg[segs[i].g].prow0 + (size_t)segs[i].rt * kM + r];
+          out_of.push_back(mr.coef != 0.0 ? ff_out_index(segs[i].out, mr.slot, nE) : -1);
+        }
+  } else {
+    out_of.resize(nft + nseg);
+    for (int i = 0; i < nft; ++i) out_of[i] = ft[i].out;
+    for (int i = 0; i < nseg; ++i) out_of[nft + i] = segs[i].out;
+  }
+  const size_t n_part = out_of.size();
+  const size_t seg_part0 = per_row ? (size_t)nft * ff_fp64_tile_rows() : (size_t)nft;  // first segment partial
 
   // Device buffers: packed digits (TABLE0); plan arrays and row scales in
   // one upload (PLAN).
@@ -679,7 +707,7 @@ int ff_launch_mixed(CallEnv *env, const FFPlan &plan, int64_t nb, int64_t nb_w, 
   const size_t o_xs = o_cta + al(sizeof(int) * std::max<size_t>(cta_seg.size(), 1));
   const size_t o_ar = o_xs + al(sizeof(MixX) * std::max<size_t>(xs.size(), 1));
   const size_t o_out = o_ar + al(sizeof(MixRow) * std::max<size_t>(arows.size(), 1));
-  const size_t o_sa = o_out + al(sizeof(int) * std::max(nft + nseg, 1));
+  const size_t o_sa = o_out + al(sizeof(int) * std::max<size_t>(n_part, 1));
   const size_t o_sb = o_sa + al(sizeof(double) * std::max<size_t>(arows.size() * (size_t)NW, 1));
   const size_t total = o_sb + al(sizeof(double) * std::max<size_t>(xs.size() * (size_t)NW * x_rows_padded, 1));
   std::vector<unsigned char> host(total, 0);
@@ -693,11 +721,11 @@ int ff_launch_mixed(CallEnv *env, const FFPlan &plan, int64_t nb, int64_t nb_w, 
   put(o_cta, cta_seg.data(), sizeof(int) * cta_seg.size());
   put(o_xs, xs.data(), sizeof(MixX) * xs.size());
   put(o_ar, arows.data(), sizeof(MixRow) * arows.size());
-  put(o_out, out_of.data(), sizeof(int) * (nft + nseg));
+  put(o_out, out_of.data(), sizeof(int) * n_part);
   BGW_TRY(ws_reserve(ws, SLOT_PLAN, total, &small_buf));
   BGW_CUDA_TRY(cudaMemcpyAsync(small_buf, host.data(), total, cudaMemcpyHostToDevice, stream));
   unsigned char *sb = static_cast<unsigned char *>(small_buf);
-  BGW_TRY(ws_reserve(ws, SLOT_PARTIALS, sizeof(double) * 2 * (size_t)std::max(nft + nseg, 1), &partials));
+  BGW_TRY(ws_reserve(ws, SLOT_PARTIALS, sizeof(double) * 2 * std::max<size_t>(n_part, 1), &partials));
   double *part = static_cast<double *>(partials);
 
   BGW_TRY(prof_mark(env, 1));
@@ -730,20 +758,26 @@ int ff_launch_mixed(CallEnv *env, const FFPlan &plan, int64_t nb, int64_t nb_w, 
       BGW_CUDA_TRY(cudaGetLastError());
     }
     const int smem = (int)sizeof(MixSmem);
-    BGW_CUDA_TRY(cudaFuncSetAttribute(ff_mix_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    ff_mix_gemm_kernel<<<nctas, kMixThreads, smem, stream>>>(
+    auto gemm = per_row ? ff_mix_gemm_kernel<true> : ff_mix_gemm_kernel<false>;
+    BGW_CUDA_TRY(cudaFuncSetAttribute(gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    gemm<<<nctas, kMixThreads, smem, stream>>>(
         (const MixSeg *)(sb + o_seg), (const int *)(sb + o_cta), d_mg, d_ar, d_xs, (const int8_t *)pack, d_sa, d_sb,
-        na, x_rows_padded, W, (int)P, KB, PT, part + 2 * (size_t)nft, env->d_status);
+        na, x_rows_padded, W, (int)P, KB, PT, part + 2 * seg_part0, env->d_status);
     count_launch();
     BGW_CUDA_TRY(cudaGetLastError());
   }
   BGW_TRY(ff_launch_fp64_tiles(stream, (const FFTile *)(sb + o_ft), nft, (const FFRow *)(sb + o_rows), P, G, an, R,
-                               r_f0, A, a_f0, W, part));
+                               r_f0, A, a_f0, W, part, per_row));
   BGW_TRY(prof_mark(env, 2));
-  ff_mix_finalize_kernel<<<1, 256, 0, stream>>>(part, (const int *)(sb + o_out), nft + nseg, (int)nE, achs_dev,
-                                                asx_dev, cor_dev);
-  count_launch();
-  BGW_CUDA_TRY(cudaGetLastError());
+  if (per_row) {
+    BGW_TRY(ff_launch_slot_finalize(stream, part, (const int *)(sb + o_out), (int)n_part, nE, achs_dev, asx_dev,
+                                    cor_dev));
+  } else {
+    ff_mix_finalize_kernel<<<1, 256, 0, stream>>>(part, (const int *)(sb + o_out), (int)n_part, (int)nE, achs_dev,
+                                                  asx_dev, cor_dev);
+    count_launch();
+    BGW_CUDA_TRY(cudaGetLastError());
+  }
   {
     // Useful work as in the FP64 path; bytes = the packed digits written
     // once and the operands read once.

@@ -12,9 +12,15 @@ enum { OUT_ACHS = 0, OUT_ASX = 1, OUT_COR = 2, OUT_COUNT = 3 };
 
 struct FFRow {
   int32_t band;
-  int32_t pad;
+  int32_t slot;  // evaluation point iw of the row (0 unless wx depends on iw)
   double coef;
 };
+
+// Output index of (sum, slot): 0 = achsDtemp, 1 + iw = asxDtemp[iw],
+// 1 + nE + iw = achDtemp_cor[iw].
+inline int ff_out_index(int out, int slot, int64_t nE) {
+  return out == OUT_ACHS ? 0 : out == OUT_ASX ? 1 + slot : 1 + (int)nE + slot;
+}
 
 struct FFTile {
   int32_t src, f, row_begin, row_count;
@@ -36,13 +42,17 @@ struct FFPlan {
   // Frequency slices read from I_epsR / I_epsA: [lo, hi] (lo > hi: none).
   int r_lo = 1 << 30, r_hi = -1, a_lo = 1 << 30, a_hi = -1;
   std::vector<double> slice_reads;  // distinct [ngpown][ncouls] slices read
+  // wx = freqevalmin - ekq + iw * freqevalstep per evaluation point (rows
+  // carry their iw in `slot`; outputs are distinct per iw).  Otherwise the
+  // reference's single wx and every iw output gets the same value.
+  bool per_iw = false;
 };
 
 // Builds the plan of the requested sums from host copies of ekq[0..nb) and
 // dFreqGrid; sizes the k split for the device.
 int ff_make_plan(CallEnv *env, int64_t nb, int64_t nvband, int64_t P, int64_t G, int64_t nFreq, double fmin,
                  double fstep, double occ, const double *ekq_h, const double *grid_h, bool want_achs,
-                 bool want_asx, bool want_cor, FFPlan *plan);
+                 bool want_asx, bool want_cor, bool per_iw, int64_t nE, FFPlan *plan);
 
 // Builds W[n1][p] = conj(aqsm[n1][igp]) vcoul[igp] for n1 < nb_w on `stream`.
 int ff_build_w(CallEnv *env, int64_t nb_w, int64_t G, int64_t P, const int32_t *inv, const int32_t *indinv,
@@ -51,11 +61,21 @@ int ff_build_w(CallEnv *env, int64_t nb_w, int64_t G, int64_t P, const int32_t *
 // for `target_ctas` together with `base_tiles` tiles already planned).
 void ff_fp64_tiles(const std::vector<FFGroup> &groups, int64_t P, int64_t G, int target_ctas,
                    std::vector<FFTile> *tiles);
-// Launches the DMMA contraction over device tiles; one complex partial per
-// tile at `partials`.
+// Launches the DMMA contraction over device tiles: one complex partial per
+// tile at `partials`, or with `per_row` one per tile row (ntiles x
+// ff_fp64_tile_rows(), zero for padding rows).
 int ff_launch_fp64_tiles(cudaStream_t stream, const FFTile *d_tiles, int ntiles, const FFRow *d_rows, int64_t P,
                          int64_t G, const double2 *an, const double2 *R, int r_f0, const double2 *A, int a_f0,
-                         const double2 *W, double *partials);
+                         const double2 *W, double *partials, bool per_row = false);
+int ff_fp64_tile_rows();
+// Output index (ff_out_index) of every per-row partial of `tiles`, -1 for
+// padding rows, appended to `out_of`.
+void ff_fp64_row_outputs(const std::vector<FFTile> &tiles, const std::vector<FFRow> &rows, int64_t nE,
+                         std::vector<int> *out_of);
+// Sums partials[i] into output out_of[i] (index order, one block per output)
+// and writes achs, asx[nE], cor[nE] (null pointers skipped).
+int ff_launch_slot_finalize(cudaStream_t stream, const double *partials, const int *out_of, int n, int64_t nE,
+                            double *achs, double *asx, double *cor);
 int ff_fp64_per_sm(int *per_sm);
 // Mixed precision (integer slices on tcgen05) evaluation of a plan.
 int ff_launch_mixed(CallEnv *env, const FFPlan &plan, int64_t nb, int64_t nb_w, int64_t nE, int64_t G, int64_t P,

@@ -321,39 +321,50 @@ static void ff_band_sum(long n1, long P, long G, const long *igp,
   *out_i = acci;
 }
 
+/* The frequency argument of band n1 at evaluation point iw.  The reference
+ * uses wx = freqevalmin - ekq[n1] + freqevalstep for every iw (no iw term,
+ * ff.cpp:245, 337); per_iw selects wx = freqevalmin - ekq[n1] +
+ * iw * freqevalstep instead (a distinct value per iw; the reference's value is
+ * the one at iw = 1). */
+static double ff_wx(double freqevalmin, double freqevalstep, double ekq, long iw, int per_iw) {
+  return per_iw ? freqevalmin - ekq + (double)iw * freqevalstep : freqevalmin - ekq + freqevalstep;
+}
+
 /* asxDtemp_Kernel + ssxDittt_kernel, ff.cpp:154-169, 211-293.  For n1 <
- * nvband: wx = freqevalmin - ekq[n1] + freqevalstep (no iw term, :245),
- * compute_fact(loop 1), X = I_epsR if wx > 0 else I_epsA (:254-261), times
- * occ.  Every asxDtemp[iw] receives the same sum; out has nfreqeval complex
- * values. */
-int orc_ff_asx(long nvband, long nfreqeval, long G, long P, long nFreq,
-               double freqevalmin, double freqevalstep, double occ,
-               const double *ekq, const double *dFreqGrid,
-               const int *inv_igp_index, const int *indinv, long indinv_len,
-               const double *aqsm, const double *aqsn, const double *vcoul,
-               const double *I_epsR, const double *I_epsA, double *out) {
+ * nvband: wx (ff_wx), compute_fact(loop 1), X = I_epsR if wx > 0 else
+ * I_epsA (:254-261), times occ.  Without per_iw every asxDtemp[iw] receives
+ * the same sum; out has nfreqeval complex values. */
+static int ff_asx(long nvband, long nfreqeval, long G, long P, long nFreq,
+                  double freqevalmin, double freqevalstep, double occ,
+                  const double *ekq, const double *dFreqGrid,
+                  const int *inv_igp_index, const int *indinv, long indinv_len,
+                  const double *aqsm, const double *aqsn, const double *vcoul,
+                  const double *I_epsR, const double *I_epsA, double *out, int per_iw) {
   if (ff_check(nvband, P, G, nFreq) || nfreqeval < 0) return -1;
+  const long ne = per_iw ? nfreqeval : 1;
   long *igp = (long *)malloc(sizeof(long) * (size_t)(P > 0 ? P : 1));
-  ld *part = (ld *)calloc((size_t)(nvband > 0 ? nvband : 1) * 2, sizeof(ld));
+  ld *part = (ld *)calloc((size_t)(nvband > 0 ? nvband : 1) * (size_t)(ne > 0 ? ne : 1) * 2, sizeof(ld));
   if (!igp || !part) { free(igp); free(part); return -1; }
   if (resolve_igp(P, G, inv_igp_index, indinv, indinv_len, igp)) {
     free(igp); free(part); return -1;
   }
-#pragma omp parallel for schedule(dynamic, 1)
-  for (long n1 = 0; n1 < nvband; ++n1) {
-    double wx = freqevalmin - ekq[n1] + freqevalstep;
-    int ifreq = 0;
-    double f1 = 0, f2 = 0;
-    orc_compute_fact(wx, (int)nFreq, dFreqGrid, 1, 0, &ifreq, &f1, &f2);
-    ld r, i;
-    ff_band_sum(n1, P, G, igp, aqsn, aqsm, vcoul, wx > 0 ? I_epsR : I_epsA,
-                NULL, 0, ifreq, f1, f2, &r, &i);
-    part[2 * n1] = r * (ld)occ;
-    part[2 * n1 + 1] = i * (ld)occ;
-  }
-  ld tr = 0, ti = 0;
-  for (long n1 = 0; n1 < nvband; ++n1) { tr += part[2 * n1]; ti += part[2 * n1 + 1]; }
+#pragma omp parallel for schedule(dynamic, 1) collapse(2)
+  for (long n1 = 0; n1 < nvband; ++n1)
+    for (long e = 0; e < ne; ++e) {
+      double wx = ff_wx(freqevalmin, freqevalstep, ekq[n1], e, per_iw);
+      int ifreq = 0;
+      double f1 = 0, f2 = 0;
+      orc_compute_fact(wx, (int)nFreq, dFreqGrid, 1, 0, &ifreq, &f1, &f2);
+      ld r, i;
+      ff_band_sum(n1, P, G, igp, aqsn, aqsm, vcoul, wx > 0 ? I_epsR : I_epsA,
+                  NULL, 0, ifreq, f1, f2, &r, &i);
+      part[2 * (n1 * ne + e)] = r * (ld)occ;
+      part[2 * (n1 * ne + e) + 1] = i * (ld)occ;
+    }
   for (long iw = 0; iw < nfreqeval; ++iw) {
+    const long e = per_iw ? iw : 0;
+    ld tr = 0, ti = 0;
+    for (long n1 = 0; n1 < nvband; ++n1) { tr += part[2 * (n1 * ne + e)]; ti += part[2 * (n1 * ne + e) + 1]; }
     out[2 * iw] = (double)tr;
     out[2 * iw + 1] = (double)ti;
   }
@@ -361,53 +372,98 @@ int orc_ff_asx(long nvband, long nfreqeval, long G, long P, long nFreq,
   return 0;
 }
 
+int orc_ff_asx(long nvband, long nfreqeval, long G, long P, long nFreq,
+               double freqevalmin, double freqevalstep, double occ,
+               const double *ekq, const double *dFreqGrid,
+               const int *inv_igp_index, const int *indinv, long indinv_len,
+               const double *aqsm, const double *aqsn, const double *vcoul,
+               const double *I_epsR, const double *I_epsA, double *out) {
+  return ff_asx(nvband, nfreqeval, G, P, nFreq, freqevalmin, freqevalstep, occ, ekq, dFreqGrid, inv_igp_index,
+                indinv, indinv_len, aqsm, aqsn, vcoul, I_epsR, I_epsA, out, 0);
+}
+
+/* asxDtemp with wx = freqevalmin - ekq + iw * freqevalstep per iw. */
+int orc_ff_asx_iw(long nvband, long nfreqeval, long G, long P, long nFreq,
+                  double freqevalmin, double freqevalstep, double occ,
+                  const double *ekq, const double *dFreqGrid,
+                  const int *inv_igp_index, const int *indinv, long indinv_len,
+                  const double *aqsm, const double *aqsn, const double *vcoul,
+                  const double *I_epsR, const double *I_epsA, double *out) {
+  return ff_asx(nvband, nfreqeval, G, P, nFreq, freqevalmin, freqevalstep, occ, ekq, dFreqGrid, inv_igp_index,
+                indinv, indinv_len, aqsm, aqsn, vcoul, I_epsR, I_epsA, out, 1);
+}
+
 /* achDtemp_cor_Kernel + schDttt_corKernel1/2, ff.cpp:295-451.  For every
  * band: flag_occ = n1 < nvband (the intended per-iteration value; the
- * reference shares the variable across OpenMP threads, :310), wx as in SX,
+ * reference shares the variable across OpenMP threads, :310), wx (ff_wx),
  * compute_fact(loop 2).  wx > 0 and unoccupied -> Kernel1 with (f1, f2);
  * wx <= 0 and occupied -> Kernel2 with an extra -0.5 (:437-444); otherwise
- * nothing.  X = I_epsR - I_epsA.  Every achDtemp_cor[iw] receives the same
- * sum. */
+ * nothing.  X = I_epsR - I_epsA.  Without per_iw every achDtemp_cor[iw]
+ * receives the same sum. */
+static int ff_cor(long nb, long nvband, long nfreqeval, long G, long P,
+                  long nFreq, double freqevalmin, double freqevalstep,
+                  const double *ekq, const double *dFreqGrid,
+                  const int *inv_igp_index, const int *indinv, long indinv_len,
+                  const double *aqsm, const double *aqsn, const double *vcoul,
+                  const double *I_epsR, const double *I_epsA, double *out, int per_iw) {
+  if (ff_check(nb, P, G, nFreq) || nfreqeval < 0 || nvband < 0) return -1;
+  const long ne = per_iw ? nfreqeval : 1;
+  long *igp = (long *)malloc(sizeof(long) * (size_t)(P > 0 ? P : 1));
+  ld *part = (ld *)calloc((size_t)(nb > 0 ? nb : 1) * (size_t)(ne > 0 ? ne : 1) * 2, sizeof(ld));
+  if (!igp || !part) { free(igp); free(part); return -1; }
+  if (resolve_igp(P, G, inv_igp_index, indinv, indinv_len, igp)) {
+    free(igp); free(part); return -1;
+  }
+#pragma omp parallel for schedule(dynamic, 1) collapse(2)
+  for (long n1 = 0; n1 < nb; ++n1)
+    for (long e = 0; e < ne; ++e) {
+      int occ = n1 < nvband;
+      double wx = ff_wx(freqevalmin, freqevalstep, ekq[n1], e, per_iw);
+      int ifreq = 0;
+      double f1 = 0, f2 = 0;
+      orc_compute_fact(wx, (int)nFreq, dFreqGrid, 2, occ, &ifreq, &f1, &f2);
+      ld r = 0, i = 0;
+      if (wx > 0) {
+        if (!occ)
+          ff_band_sum(n1, P, G, igp, aqsn, aqsm, vcoul, I_epsR, I_epsA, 1,
+                      ifreq, f1, f2, &r, &i);
+      } else if (occ) {
+        ff_band_sum(n1, P, G, igp, aqsn, aqsm, vcoul, I_epsR, I_epsA, 1, ifreq,
+                    -0.5L * f1, -0.5L * f2, &r, &i);
+      }
+      part[2 * (n1 * ne + e)] = r;
+      part[2 * (n1 * ne + e) + 1] = i;
+    }
+  for (long iw = 0; iw < nfreqeval; ++iw) {
+    const long e = per_iw ? iw : 0;
+    ld tr = 0, ti = 0;
+    for (long n1 = 0; n1 < nb; ++n1) { tr += part[2 * (n1 * ne + e)]; ti += part[2 * (n1 * ne + e) + 1]; }
+    out[2 * iw] = (double)tr;
+    out[2 * iw + 1] = (double)ti;
+  }
+  free(igp); free(part);
+  return 0;
+}
+
 int orc_ff_cor(long nb, long nvband, long nfreqeval, long G, long P,
                long nFreq, double freqevalmin, double freqevalstep,
                const double *ekq, const double *dFreqGrid,
                const int *inv_igp_index, const int *indinv, long indinv_len,
                const double *aqsm, const double *aqsn, const double *vcoul,
                const double *I_epsR, const double *I_epsA, double *out) {
-  if (ff_check(nb, P, G, nFreq) || nfreqeval < 0 || nvband < 0) return -1;
-  long *igp = (long *)malloc(sizeof(long) * (size_t)(P > 0 ? P : 1));
-  ld *part = (ld *)calloc((size_t)(nb > 0 ? nb : 1) * 2, sizeof(ld));
-  if (!igp || !part) { free(igp); free(part); return -1; }
-  if (resolve_igp(P, G, inv_igp_index, indinv, indinv_len, igp)) {
-    free(igp); free(part); return -1;
-  }
-#pragma omp parallel for schedule(dynamic, 1)
-  for (long n1 = 0; n1 < nb; ++n1) {
-    int occ = n1 < nvband;
-    double wx = freqevalmin - ekq[n1] + freqevalstep;
-    int ifreq = 0;
-    double f1 = 0, f2 = 0;
-    orc_compute_fact(wx, (int)nFreq, dFreqGrid, 2, occ, &ifreq, &f1, &f2);
-    ld r = 0, i = 0;
-    if (wx > 0) {
-      if (!occ)
-        ff_band_sum(n1, P, G, igp, aqsn, aqsm, vcoul, I_epsR, I_epsA, 1,
-                    ifreq, f1, f2, &r, &i);
-    } else if (occ) {
-      ff_band_sum(n1, P, G, igp, aqsn, aqsm, vcoul, I_epsR, I_epsA, 1, ifreq,
-                  -0.5L * f1, -0.5L * f2, &r, &i);
-    }
-    part[2 * n1] = r;
-    part[2 * n1 + 1] = i;
-  }
-  ld tr = 0, ti = 0;
-  for (long n1 = 0; n1 < nb; ++n1) { tr += part[2 * n1]; ti += part[2 * n1 + 1]; }
-  for (long iw = 0; iw < nfreqeval; ++iw) {
-    out[2 * iw] = (double)tr;
-    out[2 * iw + 1] = (double)ti;
-  }
-  free(igp); free(part);
-  return 0;
+  return ff_cor(nb, nvband, nfreqeval, G, P, nFreq, freqevalmin, freqevalstep, ekq, dFreqGrid, inv_igp_index,
+                indinv, indinv_len, aqsm, aqsn, vcoul, I_epsR, I_epsA, out, 0);
+}
+
+/* achDtemp_cor with wx = freqevalmin - ekq + iw * freqevalstep per iw. */
+int orc_ff_cor_iw(long nb, long nvband, long nfreqeval, long G, long P,
+                  long nFreq, double freqevalmin, double freqevalstep,
+                  const double *ekq, const double *dFreqGrid,
+                  const int *inv_igp_index, const int *indinv, long indinv_len,
+                  const double *aqsm, const double *aqsn, const double *vcoul,
+                  const double *I_epsR, const double *I_epsA, double *out) {
+  return ff_cor(nb, nvband, nfreqeval, G, P, nFreq, freqevalmin, freqevalstep, ekq, dFreqGrid, inv_igp_index,
+                indinv, indinv_len, aqsm, aqsn, vcoul, I_epsR, I_epsA, out, 1);
 }
 
 /* ------------------------------------------------------------ GPP adjoint --

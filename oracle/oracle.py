@@ -59,6 +59,8 @@ class Oracle:
         lib.orc_ff_achs.argtypes = [_L, _L, _L, _L, _P, _P, _L, _P, _P, _P, _P, _P]
         lib.orc_ff_asx.argtypes = [_L, _L, _L, _L, _L, _D, _D, _D, _P, _P, _P, _P, _L, _P, _P, _P, _P, _P, _P]
         lib.orc_ff_cor.argtypes = [_L, _L, _L, _L, _L, _L, _D, _D, _P, _P, _P, _P, _L, _P, _P, _P, _P, _P, _P]
+        lib.orc_ff_asx_iw.argtypes = lib.orc_ff_asx.argtypes
+        lib.orc_ff_cor_iw.argtypes = lib.orc_ff_cor.argtypes
         self.lib = lib
 
     def gpp(self, g, factored: bool = False) -> np.ndarray:
@@ -115,22 +117,26 @@ class Oracle:
             raise ValueError("oracle rejected the FF inputs")
         return complex(out[0])
 
-    def asx(self, f) -> np.ndarray:
+    def asx(self, f, per_iw: bool = False) -> np.ndarray:
+        """asxDtemp; per_iw: wx = freqevalmin - ekq + iw * freqevalstep per iw."""
         out = np.zeros(max(f.nfreqeval, 1), dtype=np.complex128)
-        st = self.lib.orc_ff_asx(f.nvband, f.nfreqeval, f.ncouls, f.ngpown, f.nFreq, f.freqevalmin, f.freqevalstep,
-                                 f.occ, _p(f.ekq), _p(f.dFreqGrid), _p(f.inv_igp_index), _p(f.indinv),
-                                 len(f.indinv), _p(f.aqsmtemp), _p(f.aqsntemp), _p(f.vcoul), _p(f.I_epsR_array),
-                                 _p(f.I_epsA_array), _p(out))
+        fn = self.lib.orc_ff_asx_iw if per_iw else self.lib.orc_ff_asx
+        st = fn(f.nvband, f.nfreqeval, f.ncouls, f.ngpown, f.nFreq, f.freqevalmin, f.freqevalstep,
+                f.occ, _p(f.ekq), _p(f.dFreqGrid), _p(f.inv_igp_index), _p(f.indinv),
+                len(f.indinv), _p(f.aqsmtemp), _p(f.aqsntemp), _p(f.vcoul), _p(f.I_epsR_array),
+                _p(f.I_epsA_array), _p(out))
         if st != 0:
             raise ValueError("oracle rejected the FF inputs")
         return out[:f.nfreqeval]
 
-    def cor(self, f) -> np.ndarray:
+    def cor(self, f, per_iw: bool = False) -> np.ndarray:
+        """achDtemp_cor; per_iw as in asx."""
         out = np.zeros(max(f.nfreqeval, 1), dtype=np.complex128)
-        st = self.lib.orc_ff_cor(f.number_bands, f.nvband, f.nfreqeval, f.ncouls, f.ngpown, f.nFreq, f.freqevalmin,
-                                 f.freqevalstep, _p(f.ekq), _p(f.dFreqGrid), _p(f.inv_igp_index), _p(f.indinv),
-                                 len(f.indinv), _p(f.aqsmtemp), _p(f.aqsntemp), _p(f.vcoul), _p(f.I_epsR_array),
-                                 _p(f.I_epsA_array), _p(out))
+        fn = self.lib.orc_ff_cor_iw if per_iw else self.lib.orc_ff_cor
+        st = fn(f.number_bands, f.nvband, f.nfreqeval, f.ncouls, f.ngpown, f.nFreq, f.freqevalmin,
+                f.freqevalstep, _p(f.ekq), _p(f.dFreqGrid), _p(f.inv_igp_index), _p(f.indinv),
+                len(f.indinv), _p(f.aqsmtemp), _p(f.aqsntemp), _p(f.vcoul), _p(f.I_epsR_array),
+                _p(f.I_epsA_array), _p(out))
         if st != 0:
             raise ValueError("oracle rejected the FF inputs")
         return out[:f.nfreqeval]

@@ -105,3 +105,17 @@ def test_reference_live_if_built(oracle):
     assert rel_err(ref.achs(f), oracle.achs(f)) < FP64_RTOL
     assert rel_err(ref.asx(f), oracle.asx(f)) < FP64_RTOL
     assert rel_err(ref.cor(f), oracle.cor(f)) < FP64_RTOL
+
+
+@pytest.mark.parametrize("name", sorted(FF_CASES))
+def test_ff_per_iw_oracle_pinned_at_iw1(golden, oracle, name):
+    """With wx = freqevalmin - ekq + iw * freqevalstep per iw (an option the
+    reference lacks), the iw = 1 entry is the reference's value (its single
+    wx, FF/ff.cpp:245, 337); the other entries follow the same restatement."""
+    f = FF_CASES[name]()
+    if f.nfreqeval < 2:
+        pytest.skip("needs two evaluation points")
+    ref = golden["ff"][name]["reference"]
+    asx, cor = oracle.asx(f, per_iw=True), oracle.cor(f, per_iw=True)
+    assert rel_err(asx[1], l2c(ref["asx"])[1]) < 1e-14
+    assert rel_err(cor[1], l2c(ref["cor"])[1]) < 1e-14
