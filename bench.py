@@ -411,6 +411,29 @@ def run_ours(args, world, rank, local):
             "effective_TFLOPs": pm["flops"] / (mk * 1e-3) / 1e12,
             "rel_err_vs_fp64": {k: rel_err(a.cpu().numpy(), b.cpu().numpy())
                                 for k, a, b in zip(("achsDtemp", "asxDtemp", "achDtemp_cor"), mix_out, ff_out)}}
+        # Option: iw-dependent wx (nfreqeval distinct outputs), FP64 and mixed.
+        piw = {}
+        for prec in ("fp64", "mixed"):
+            fl = bgw.FLAG_PROFILE | bgw.FLAG_FF_WX_PER_IW
+            for _ in range(2):
+                bgw.ff_sigma(fd, stream=sh, precision=prec, flags=fl)
+            ks, ds = [], []
+            for _ in range(max(2, args.steps // 4)):
+                out = bgw.ff_sigma(fd, stream=sh, precision=prec, flags=fl)
+                pp = bgw.last_profile()
+                ks.append(pp["main_kernel_ms"])
+                ds.append(pp["device_ms"])
+            piw[prec] = (statistics.mean(ks), statistics.mean(ds), out, pp)
+        kf, df, of_, pf = piw["fp64"]
+        km, dm, om, _ = piw["mixed"]
+        extra["ff_per_iw"] = {
+            "option": "BGW_FLAG_FF_WX_PER_IW: wx = freqevalmin - ekq + iw*freqevalstep, 10 distinct outputs",
+            "fp64": {"s_per_sigma": df / 1e3, "contraction_ms": kf,
+                     "TFLOPs": pf["flops"] / (kf * 1e-3) / 1e12, "frac_of_dmma_peak": pf["flops"] / (kf * 1e-3) / 1e12
+                     / dmma_peak},
+            "mixed": {"s_per_sigma": dm / 1e3, "contraction_ms": km, "speedup_vs_fp64": df / dm,
+                      "rel_err_vs_fp64": {k: rel_err(a.cpu().numpy(), b.cpu().numpy())
+                                          for k, a, b in zip(("achsDtemp", "asxDtemp", "achDtemp_cor"), om, of_)}}}
         if rank == 0 and not args.no_cpu:
             from oracle.oracle import Reference
             if Reference.available():
@@ -572,8 +595,9 @@ def run_only(args, local):
         if args.freqs:
             dims["nFreq"] = args.freqs
         d = bgw.to_device(I.ff_seeded(**dims, seed=1234), dev)
-        prec = "mixed" if args.only.startswith("ff_mixed") else "fp64"
+        prec = "mixed" if "mixed" in args.only else "fp64"
         fl = bgw.FLAG_PROFILE | (bgw.FLAG_FF_SLICE_ALL if args.only == "ff_mixed_all" else 0)
+        fl |= bgw.FLAG_FF_WX_PER_IW if args.only.startswith("ff_per_iw") else 0
         call = lambda: bgw.ff_sigma(d, precision=prec, flags=fl)  # noqa: E731
     for _ in range(args.warmup):
         call()
@@ -608,7 +632,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-instances extra")
     ap.add_argument("--only", choices=["gpp_bandloop", "gpp_mixed", "gpp_factored", "gpp_adjoint", "ff", "ff_mixed",
-                                       "ff_mixed_all"],
+                                       "ff_mixed_all", "ff_per_iw", "ff_per_iw_mixed"],
                     default=None,
                     help="diagnostic: time one kernel path only (for profilers)")
     ap.add_argument("--bands", type=int, default=0, help="with --only: number_bands override")

@@ -104,8 +104,8 @@ int build_plan(int64_t nb, int64_t nvband, int64_t P, int64_t G, int64_t nFreq, 
                bool per_iw, int64_t nE, int target_ctas, FFPlan *plan) {
   // Evaluation points with a distinct wx: iw = 0 .. nE - 1 with
   // wx = fmin - ekq + iw fstep, or the reference's single wx = fmin - ekq +
-  // fstep (ff.cpp:245, 337) in slot 0.  Rows of every iw that read the same
-  // slice share one group (one GEMM over that slice).
+  // fstep (ff.cpp:245, 337).  Rows of every iw that read the same slice
+  // share one group (one GEMM over that slice).
   const int64_t n_iw = per_iw ? nE : 1;
   auto wx_of = [&](int64_t n1, int64_t iw) { return fmin - ekq[n1] + (per_iw ? (double)iw : 1.0) * fstep; };
   std::map<GroupKey, std::vector<FFRow>> groups;
@@ -113,14 +113,31 @@ int build_plan(int64_t nb, int64_t nvband, int64_t P, int64_t G, int64_t nFreq, 
     auto &g = groups[{OUT_ACHS, SRC_R, 1}];
     for (int64_t n1 = 0; n1 < nb; ++n1) g.push_back({(int32_t)n1, 0, -0.5});
   }
+  // Per-iw rows (band, iw, coef) of each group, before deduplication.
+  struct IwRow {
+    int32_t band, iw;
+    double coef;
+  };
+  // Rows are collected in dense (out, src, slice) buckets, then moved into
+  // the ordered maps (a map lookup per row costs more than the whole plan).
+  const int64_t nkeys = (int64_t)OUT_COUNT * 3 * (nFreq + 1);
+  auto kidx = [&](const GroupKey &k) { return ((int64_t)k.out * 3 + k.src) * (nFreq + 1) + k.f; };
+  std::vector<std::vector<FFRow>> dense_rows(per_iw ? 0 : nkeys);
+  std::vector<std::vector<IwRow>> dense_iw(per_iw ? nkeys : 0);
+  auto add = [&](const GroupKey &k, int64_t n1, int64_t iw, double coef) {
+    if (per_iw)
+      dense_iw[kidx(k)].push_back({(int32_t)n1, (int32_t)iw, coef});
+    else
+      dense_rows[kidx(k)].push_back({(int32_t)n1, 0, coef});
+  };
   if (want_asx) {
     for (int64_t iw = 0; iw < n_iw; ++iw)
     for (int64_t n1 = 0; n1 < nvband; ++n1) {
       const double wx = wx_of(n1, iw);
       const Fact fc = compute_fact_host(wx, (int)nFreq, grid, 1, false);
       const int src = wx > 0 ? SRC_R : SRC_A;
-      groups[{OUT_ASX, src, fc.ifreq}].push_back({(int32_t)n1, (int32_t)iw, fc.f1 * occ});
-      groups[{OUT_ASX, src, fc.ifreq + 1}].push_back({(int32_t)n1, (int32_t)iw, fc.f2 * occ});
+      add({OUT_ASX, src, fc.ifreq}, n1, iw, fc.f1 * occ);
+      add({OUT_ASX, src, fc.ifreq + 1}, n1, iw, fc.f2 * occ);
     }
   }
   if (want_cor) {
@@ -138,8 +155,33 @@ int build_plan(int64_t nb, int64_t nvband, int64_t P, int64_t G, int64_t nFreq, 
       } else {
         continue;
       }
-      groups[{OUT_COR, SRC_RA, fc.ifreq}].push_back({(int32_t)n1, (int32_t)iw, fc.f1 * s});
-      groups[{OUT_COR, SRC_RA, fc.ifreq + 1}].push_back({(int32_t)n1, (int32_t)iw, fc.f2 * s});
+      add({OUT_COR, SRC_RA, fc.ifreq}, n1, iw, fc.f1 * s);
+      add({OUT_COR, SRC_RA, fc.ifreq + 1}, n1, iw, fc.f2 * s);
+    }
+  }
+  std::map<GroupKey, std::vector<IwRow>> iw_rows;
+  for (int out = 0; out < OUT_COUNT; ++out)
+    for (int src = 0; src < 3; ++src)
+      for (int f = 0; f <= (int)nFreq; ++f) {
+        const GroupKey k{out, src, f};
+        const int64_t i = kidx(k);
+        if (per_iw && !dense_iw[i].empty()) iw_rows[k] = std::move(dense_iw[i]);
+        if (!per_iw && !dense_rows[i].empty()) groups[k] = std::move(dense_rows[i]);
+      }
+  // Per-iw: one row per distinct band of a group (coef 1, bands ascending);
+  // each (band, iw) becomes a term on output ff_out_index(out, iw).
+  if (per_iw) {
+    if (want_achs) {
+      auto &g = groups[{OUT_ACHS, SRC_R, 1}];
+      for (auto &r : g) r.coef = 1.0;
+    }
+    std::vector<char> used((size_t)std::max<int64_t>(nb, 1));
+    for (auto &kv : iw_rows) {
+      std::fill(used.begin(), used.end(), 0);
+      for (const auto &r : kv.second) used[r.band] = 1;
+      auto &g = groups[kv.first];
+      for (int64_t b = 0; b < nb; ++b)
+        if (used[b]) g.push_back({(int32_t)b, 0, 1.0});
     }
   }
   plan->rows.clear();
@@ -147,6 +189,9 @@ int build_plan(int64_t nb, int64_t nvband, int64_t P, int64_t G, int64_t nFreq, 
   plan->groups.clear();
   plan->useful_cmacs = 0.0;
   plan->per_iw = per_iw;
+  plan->terms.clear();
+  std::vector<int32_t> row_of_band;
+  std::vector<std::vector<FFTerm>> terms_of((size_t)(1 + 2 * std::max<int64_t>(nE, 0)));
   for (auto &kv : groups) {
     const GroupKey &key = kv.first;
     const int32_t rb = (int32_t)plan->rows.size();
@@ -154,7 +199,20 @@ int build_plan(int64_t nb, int64_t nvband, int64_t P, int64_t G, int64_t nFreq, 
     plan->rows.insert(plan->rows.end(), kv.second.begin(), kv.second.end());
     plan->groups.push_back({key.out, key.src, key.f, rb, (int32_t)nrows});
     plan->useful_cmacs += (double)nrows * (double)P * (double)G;
+    if (per_iw) {
+      if (key.out == OUT_ACHS) {
+        for (int64_t r = 0; r < nrows; ++r) terms_of[0].push_back({rb + (int32_t)r, 0, -0.5});
+      } else {
+        row_of_band.assign((size_t)std::max<int64_t>(nb, 1), -1);
+        for (int64_t r = 0; r < nrows; ++r) row_of_band[kv.second[r].band] = rb + (int32_t)r;
+        for (const auto &t : iw_rows[key]) {
+          const int o = ff_out_index(key.out, t.iw, nE);
+          terms_of[o].push_back({row_of_band[t.band], o, t.coef});
+        }
+      }
+    }
   }
+  for (auto &v : terms_of) plan->terms.insert(plan->terms.end(), v.begin(), v.end());  // sorted by output
   // Tiles in group (= output) order; seg[o] = first tile of output o.
   ff_fp64_tiles(plan->groups, P, G, target_ctas, &plan->tiles);
   for (int o = 0; o <= OUT_COUNT; ++o) {
@@ -508,20 +566,29 @@ __global__ void __launch_bounds__(256)
   }
 }
 
-// Block o sums the partials whose out_of entry is o, in index order (fixed
-// thread-strided order, then block_sum): bitwise reproducible.  Output o is
-// achsDtemp (o = 0), asxDtemp[o - 1] (o <= nE) or achDtemp_cor[o - 1 - nE].
+// Output o (0 = achsDtemp, 1 + iw = asxDtemp[iw], 1 + nE + iw =
+// achDtemp_cor[iw]) = sum over its terms t (thread-strided in order, then
+// block_sum) of coef_t * (sum of the partials of row_t, in order): bitwise
+// reproducible.
 __global__ void __launch_bounds__(256)
-    ff_slot_finalize_kernel(const double *__restrict__ partials, const int *__restrict__ out_of, int n, int nE,
+    ff_term_finalize_kernel(const double *__restrict__ partials, const int *__restrict__ row_ptr,
+                            const int *__restrict__ part_idx, const int *__restrict__ out_ptr,
+                            const int *__restrict__ term_row, const double *__restrict__ term_coef, int nE,
                             double *__restrict__ achs, double *__restrict__ asx, double *__restrict__ cor) {
   __shared__ double red[8 * 2];
   const int o = blockIdx.x;
   double v[2] = {0.0, 0.0};
-  for (int i = threadIdx.x; i < n; i += 256)
-    if (out_of[i] == o) {
-      v[0] += partials[(size_t)i * 2];
-      v[1] += partials[(size_t)i * 2 + 1];
+  for (int t = out_ptr[o] + threadIdx.x; t < out_ptr[o + 1]; t += 256) {
+    const int r = term_row[t];
+    double sr = 0.0, si = 0.0;
+    for (int j = row_ptr[r]; j < row_ptr[r + 1]; ++j) {
+      const int i = part_idx[j];
+      sr += partials[(size_t)i * 2];
+      si += partials[(size_t)i * 2 + 1];
     }
+    v[0] = fma(term_coef[t], sr, v[0]);
+    v[1] = fma(term_coef[t], si, v[1]);
+  }
   block_sum<2, 256>(v, red);
   if (threadIdx.x != 0) return;
   double *dst = o == 0 ? achs : o <= nE ? (asx ? asx + 2 * (o - 1) : nullptr) : (cor ? cor + 2 * (o - 1 - nE) : nullptr);
@@ -613,17 +680,57 @@ int ff_launch_fp64_tiles(cudaStream_t stream, const FFTile *d_tiles, int ntiles,
 
 int ff_fp64_tile_rows() { return kTM; }
 
-void ff_fp64_row_outputs(const std::vector<FFTile> &tiles, const std::vector<FFRow> &rows, int64_t nE,
-                         std::vector<int> *out_of) {
+void ff_fp64_row_ids(const std::vector<FFTile> &tiles, std::vector<int> *row_of) {
   for (const auto &t : tiles)
-    for (int r = 0; r < kTM; ++r)
-      out_of->push_back(r < t.row_count ? ff_out_index(t.out, rows[t.row_begin + r].slot, nE) : -1);
+    for (int r = 0; r < kTM; ++r) row_of->push_back(r < t.row_count ? t.row_begin + r : -1);
 }
 
-int ff_launch_slot_finalize(cudaStream_t stream, const double *partials, const int *out_of, int n, int64_t nE,
+void ff_build_term_tables(const FFPlan &plan, const std::vector<int> &row_of, int64_t nE, FFTermTables *tt) {
+  const int nrows = (int)plan.rows.size(), n_out = 1 + 2 * (int)nE;
+  tt->row_ptr.assign(nrows + 1, 0);
+  for (int r : row_of)
+    if (r >= 0) ++tt->row_ptr[r + 1];
+  for (int r = 0; r < nrows; ++r) tt->row_ptr[r + 1] += tt->row_ptr[r];
+  tt->part_idx.assign(tt->row_ptr[nrows], 0);
+  std::vector<int> fill(tt->row_ptr.begin(), tt->row_ptr.end() - 1);
+  for (int i = 0; i < (int)row_of.size(); ++i)
+    if (row_of[i] >= 0) tt->part_idx[fill[row_of[i]]++] = i;  // partials of a row in index order
+  tt->out_ptr.assign(n_out + 1, 0);
+  tt->term_row.clear();
+  tt->term_coef.clear();
+  for (const auto &t : plan.terms) {  // sorted by output
+    ++tt->out_ptr[t.out + 1];
+    tt->term_row.push_back(t.row);
+    tt->term_coef.push_back(t.coef);
+  }
+  for (int o = 0; o < n_out; ++o) tt->out_ptr[o + 1] += tt->out_ptr[o];
+}
+
+int ff_launch_term_finalize(CallEnv *env, int slot, const FFTermTables &tt, const double *partials, int64_t nE,
                             double *achs, double *asx, double *cor) {
+  auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const size_t o_rp = 0, o_pi = o_rp + al(sizeof(int) * tt.row_ptr.size());
+  const size_t o_op = o_pi + al(sizeof(int) * std::max<size_t>(tt.part_idx.size(), 1));
+  const size_t o_tr = o_op + al(sizeof(int) * tt.out_ptr.size());
+  const size_t o_tc = o_tr + al(sizeof(int) * std::max<size_t>(tt.term_row.size(), 1));
+  const size_t total = o_tc + al(sizeof(double) * std::max<size_t>(tt.term_coef.size(), 1));
+  std::vector<unsigned char> host(total, 0);
+  auto put = [&](size_t o, const void *src, size_t bytes) {
+    if (bytes) std::memcpy(host.data() + o, src, bytes);
+  };
+  put(o_rp, tt.row_ptr.data(), sizeof(int) * tt.row_ptr.size());
+  put(o_pi, tt.part_idx.data(), sizeof(int) * tt.part_idx.size());
+  put(o_op, tt.out_ptr.data(), sizeof(int) * tt.out_ptr.size());
+  put(o_tr, tt.term_row.data(), sizeof(int) * tt.term_row.size());
+  put(o_tc, tt.term_coef.data(), sizeof(double) * tt.term_coef.size());
+  void *d = nullptr;
+  BGW_TRY(ws_reserve(env->ws, slot, total, &d));
+  BGW_CUDA_TRY(cudaMemcpyAsync(d, host.data(), total, cudaMemcpyHostToDevice, env->stream));
+  const unsigned char *b = static_cast<const unsigned char *>(d);
   const int n_out = 1 + 2 * (int)nE;
-  ff_slot_finalize_kernel<<<n_out, 256, 0, stream>>>(partials, out_of, n, (int)nE, achs, asx, cor);
+  ff_term_finalize_kernel<<<n_out, 256, 0, env->stream>>>(
+      partials, (const int *)(b + o_rp), (const int *)(b + o_pi), (const int *)(b + o_op), (const int *)(b + o_tr),
+      (const double *)(b + o_tc), (int)nE, achs, asx, cor);
   count_launch();
   BGW_CUDA_TRY(cudaGetLastError());
   return BGW_OK;
@@ -662,19 +769,12 @@ int ff_launch(CallEnv *env, const FFPlan &plan, int64_t nb_w, int64_t nE, int64_
     BGW_CUDA_TRY(cudaGetLastError());
   }
   const int ntiles = (int)plan.tiles.size();
-  // Distinct outputs per iw: one partial per tile row, routed by row slot.
+  // Distinct outputs per iw: one partial per tile row, combined by the terms.
   const bool per_row = plan.per_iw;
-  std::vector<int> out_of;
-  if (per_row) ff_fp64_row_outputs(plan.tiles, plan.rows, nE, &out_of);
-  const size_t n_part = per_row ? out_of.size() : (size_t)ntiles;
+  std::vector<int> row_of;
+  if (per_row) ff_fp64_row_ids(plan.tiles, &row_of);
+  const size_t n_part = per_row ? row_of.size() : (size_t)ntiles;
   BGW_TRY(ws_reserve(ws, SLOT_PARTIALS, sizeof(double) * 2 * std::max<size_t>(n_part, 1), &partials));
-  void *d_out_of = nullptr;
-  if (per_row) {
-    BGW_TRY(ws_reserve(ws, SLOT_TABLE1, sizeof(int) * std::max<size_t>(out_of.size(), 1), &d_out_of));
-    if (!out_of.empty())
-      BGW_CUDA_TRY(cudaMemcpyAsync(d_out_of, out_of.data(), sizeof(int) * out_of.size(), cudaMemcpyHostToDevice,
-                                   stream));
-  }
   BGW_TRY(prof_mark(env, 1));
   if (ntiles > 0) {
     ff_contract_kernel<<<ntiles, kFFThreads, smem, stream>>>(d_tiles, d_rows, (int)P, (int)G, an, R, r_f0, A, a_f0,
@@ -696,8 +796,10 @@ int ff_launch(CallEnv *env, const FFPlan &plan, int64_t nb_w, int64_t nE, int64_
     std::snprintf(env->prof.main_kernel, sizeof(env->prof.main_kernel), "ff_contract_kernel");
   }
   if (per_row) {
-    BGW_TRY(ff_launch_slot_finalize(stream, (const double *)partials, (const int *)d_out_of, (int)n_part, nE,
-                                    achs_dev, asx_dev, cor_dev));
+    FFTermTables tt;
+    ff_build_term_tables(plan, row_of, nE, &tt);
+    BGW_TRY(ff_launch_term_finalize(env, SLOT_TABLE1, tt, (const double *)partials, nE, achs_dev, asx_dev,
+                                    cor_dev));
   } else {
     ff_finalize_kernel<<<1, 256, 0, stream>>>((const double *)partials, plan.seg[0], plan.seg[1], plan.seg[2],
                                               plan.seg[3], (int)nE, achs_dev, asx_dev, cor_dev);

@@ -81,7 +81,7 @@ struct MixGroup {       // one integer-slice band group
 };
 struct MixRow {         // packed A row
   int band, g;
-  int slot, pad;        // evaluation point iw of the row
+  int plan_row, pad;    // row of the plan (-1 for padding rows)
   double coef;          // 0 for padding rows
 };
 struct MixX {           // one distinct X = slice f of R, A or R - A
@@ -649,11 +649,11 @@ int ff_launch_mixed(CallEnv *env, const FFPlan &plan, int64_t nb, int64_t nb_w, 
       if (r < g.row_count) {
         const FFRow &fr = plan.rows[g.row_begin + r];
         mr.band = fr.band;
-        mr.slot = fr.slot;
+        mr.plan_row = g.row_begin + r;
         mr.coef = fr.coef;
       } else {
         mr.band = 0;
-        mr.slot = 0;
+        mr.plan_row = -1;
         mr.coef = 0.0;
       }
       arows.push_back(mr);
@@ -677,15 +677,13 @@ int ff_launch_mixed(CallEnv *env, const FFPlan &plan, int64_t nb, int64_t nb_w, 
   // Partials: one per FP64 tile then one per segment; with distinct outputs
   // per iw, one per FP64 tile row then one per (segment, column half, row).
   const bool per_row = plan.per_iw;
-  std::vector<int> out_of;
+  std::vector<int> out_of;  // per_row: plan row of each partial, else its output
   if (per_row) {
-    ff_fp64_row_outputs(ft, plan.rows, nE, &out_of);
+    ff_fp64_row_ids(ft, &out_of);
     for (int i = 0; i < nseg; ++i)
       for (int h = 0; h < 2; ++h)
-        for (int r = 0; r < kM; ++r) {
-          const MixRow &mr = arows[(size_t)mg[segs[i].g].prow0 + (size_t)segs[i].rt * kM + r];
-          out_of.push_back(mr.coef != 0.0 ? ff_out_index(segs[i].out, mr.slot, nE) : -1);
-        }
+        for (int r = 0; r < kM; ++r)
+          out_of.push_back(arows[(size_t)mg[segs[i].g].prow0 + (size_t)segs[i].rt * kM + r].plan_row);
   } else {
     out_of.resize(nft + nseg);
     for (int i = 0; i < nft; ++i) out_of[i] = ft[i].out;
@@ -770,8 +768,9 @@ int ff_launch_mixed(CallEnv *env, const FFPlan &plan, int64_t nb, int64_t nb_w, 
                                r_f0, A, a_f0, W, part, per_row));
   BGW_TRY(prof_mark(env, 2));
   if (per_row) {
-    BGW_TRY(ff_launch_slot_finalize(stream, part, (const int *)(sb + o_out), (int)n_part, nE, achs_dev, asx_dev,
-                                    cor_dev));
+    FFTermTables tt;
+    ff_build_term_tables(plan, out_of, nE, &tt);
+    BGW_TRY(ff_launch_term_finalize(env, SLOT_TABLE1, tt, part, nE, achs_dev, asx_dev, cor_dev));
   } else {
     ff_mix_finalize_kernel<<<1, 256, 0, stream>>>(part, (const int *)(sb + o_out), (int)n_part, (int)nE, achs_dev,
                                                   asx_dev, cor_dev);

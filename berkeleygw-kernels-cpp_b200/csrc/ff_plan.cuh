@@ -12,7 +12,14 @@ enum { OUT_ACHS = 0, OUT_ASX = 1, OUT_COR = 2, OUT_COUNT = 3 };
 
 struct FFRow {
   int32_t band;
-  int32_t slot;  // evaluation point iw of the row (0 unless wx depends on iw)
+  int32_t pad;
+  double coef;
+};
+
+// With per-iw outputs a group holds each band once (coef 1) and the terms
+// carry the coefficients: output `out` += coef * (row's contraction).
+struct FFTerm {
+  int32_t row, out;
   double coef;
 };
 
@@ -42,11 +49,27 @@ struct FFPlan {
   // Frequency slices read from I_epsR / I_epsA: [lo, hi] (lo > hi: none).
   int r_lo = 1 << 30, r_hi = -1, a_lo = 1 << 30, a_hi = -1;
   std::vector<double> slice_reads;  // distinct [ngpown][ncouls] slices read
-  // wx = freqevalmin - ekq + iw * freqevalstep per evaluation point (rows
-  // carry their iw in `slot`; outputs are distinct per iw).  Otherwise the
-  // reference's single wx and every iw output gets the same value.
+  // wx = freqevalmin - ekq + iw * freqevalstep per evaluation point:
+  // distinct outputs per iw, rows deduplicated per group, coefficients in
+  // `terms` (sorted by output).  Otherwise the reference's single wx and
+  // every iw output gets the same value.
   bool per_iw = false;
+  std::vector<FFTerm> terms;
 };
+
+// Host CSR tables of the per-iw finalize: the partials of each plan row and
+// the terms of each output.
+struct FFTermTables {
+  std::vector<int> row_ptr, part_idx, out_ptr, term_row;
+  std::vector<double> term_coef;
+};
+// row_of[i] = plan row of partial i (-1: none).
+void ff_build_term_tables(const FFPlan &plan, const std::vector<int> &row_of, int64_t nE, FFTermTables *tt);
+// Uploads the tables into workspace slot `slot` and enqueues the finalize:
+// output o = sum over its terms (in order) of coef * (sum of the row's
+// partials, in order); writes achs, asx[nE], cor[nE] (null skipped).
+int ff_launch_term_finalize(CallEnv *env, int slot, const FFTermTables &tt, const double *partials, int64_t nE,
+                            double *achs, double *asx, double *cor);
 
 // Builds the plan of the requested sums from host copies of ekq[0..nb) and
 // dFreqGrid; sizes the k split for the device.
@@ -68,14 +91,9 @@ int ff_launch_fp64_tiles(cudaStream_t stream, const FFTile *d_tiles, int ntiles,
                          int64_t G, const double2 *an, const double2 *R, int r_f0, const double2 *A, int a_f0,
                          const double2 *W, double *partials, bool per_row = false);
 int ff_fp64_tile_rows();
-// Output index (ff_out_index) of every per-row partial of `tiles`, -1 for
-// padding rows, appended to `out_of`.
-void ff_fp64_row_outputs(const std::vector<FFTile> &tiles, const std::vector<FFRow> &rows, int64_t nE,
-                         std::vector<int> *out_of);
-// Sums partials[i] into output out_of[i] (index order, one block per output)
-// and writes achs, asx[nE], cor[nE] (null pointers skipped).
-int ff_launch_slot_finalize(cudaStream_t stream, const double *partials, const int *out_of, int n, int64_t nE,
-                            double *achs, double *asx, double *cor);
+// Plan row of every per-row partial of `tiles` (-1 for padding rows),
+// appended to `row_of`.
+void ff_fp64_row_ids(const std::vector<FFTile> &tiles, std::vector<int> *row_of);
 int ff_fp64_per_sm(int *per_sm);
 // Mixed precision (integer slices on tcgen05) evaluation of a plan.
 int ff_launch_mixed(CallEnv *env, const FFPlan &plan, int64_t nb, int64_t nb_w, int64_t nE, int64_t G, int64_t P,
