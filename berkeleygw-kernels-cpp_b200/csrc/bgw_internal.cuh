@@ -83,12 +83,17 @@ struct Workspace {
   cudaEvent_t chunk_ready[16] = {};
   int sm_count = 0;
   int device = -1;
+  void *pinned = nullptr;  // page-locked host staging (grow-only)
+  size_t pinned_cap = 0;
 };
 
 // Returns the workspace of `device` (created on first use).
 Workspace *workspace_for(int device);
 // Ensures slot `s` holds at least `bytes` (256-byte aligned); grow-only.
 int ws_reserve(Workspace *ws, int s, size_t bytes, void **out);
+// Ensures the page-locked host staging buffer holds `bytes`; grow-only.  The
+// caller must not overwrite it while an earlier copy from it is in flight.
+int ws_reserve_pinned(Workspace *ws, size_t bytes, void **out);
 // Makes `stream` wait for the previous user of the workspace, and records
 // this call as the new last user (call after enqueuing).
 int ws_acquire(Workspace *ws, cudaStream_t stream);

@@ -22,7 +22,9 @@
 #include <algorithm>
 #include <cstdio>
 #include <functional>
+#include <thread>
 #include <type_traits>
+#include <vector>
 
 #include "bgw_internal.cuh"
 #include "gpp_common.cuh"
@@ -41,12 +43,14 @@ constexpr int kChunk = kThreads * kElems;  // ig per item
 // out-of-range inv_igp_index / indinv entry raises BGW_ERR_INDEX and that
 // column contributes zero (no out-of-bounds read is ever issued).
 // One warp per column p: st row (if st != nullptr) and S[p] (if S != nullptr).
+// gstride > 0: am / an / vc were gathered on the host to the columns
+// igp(p) (am[n1 * gstride + p], vc[p]); wtilde is always read at igp(p).
 __global__ void __launch_bounds__(256) gpp_prep_kernel(int nb, int P, int G, const int *__restrict__ inv,
                                                        const int *__restrict__ indinv, long long indinv_len,
                                                        const double2 *__restrict__ wt, const double2 *__restrict__ am,
                                                        const double2 *__restrict__ an, const double *__restrict__ vc,
                                                        double2 *__restrict__ st, double2 *__restrict__ S,
-                                                       int *status) {
+                                                       int *status, long long gstride) {
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
   for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < P; p += warps) {
@@ -54,7 +58,19 @@ __global__ void __launch_bounds__(256) gpp_prep_kernel(int nb, int P, int G, con
     double sr = 0.0, si = 0.0;
     for (int n1 = lane; n1 < nb; n1 += 32) {
       double2 s = make_double2(0.0, 0.0);
-      if (g >= 0) s = store1(am, an, vc, wt, n1, p, g, G);
+      if (g >= 0 && gstride > 0) {
+        double2 m = am[(size_t)n1 * gstride + p];
+        m.y = -m.y;
+        double2 r = cmul(m, an[(size_t)n1 * gstride + p]);  // same operation order as store1
+        r.x *= 0.5;
+        r.y *= 0.5;
+        const double v = vc[p];
+        r.x *= v;
+        r.y *= v;
+        s = cmul(r, wt[(size_t)p * G + g]);
+      } else if (g >= 0) {
+        s = store1(am, an, vc, wt, n1, p, g, G);
+      }
       if (st) st[(size_t)p * nb + n1] = s;
       sr += s.x;
       si += s.y;
@@ -298,7 +314,8 @@ struct RowChunks {
 int gpp_enqueue_chunks(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *inv, const int32_t *indinv,
                        int64_t indinv_len, const double *wx, int64_t wx_stride, const double2 *wt,
                        const double2 *am, const double2 *an, const double2 *ie, const double *vc,
-                       double *achtemp_dev, RowChunks &rc, const std::function<int(int)> &issue = nullptr) {
+                       double *achtemp_dev, RowChunks &rc, const std::function<int(int)> &issue = nullptr,
+                       long long gstride = 0) {
   Workspace *ws = env->ws;
   cudaStream_t stream = env->stream;
   const bool factored = env->opt.gpp_algorithm == BGW_GPP_FACTORED ||
@@ -347,9 +364,9 @@ int gpp_enqueue_chunks(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int
     double *part_c = partials + (size_t)total * 6;
     if (factored) {
       double2 *S_c = static_cast<double2 *>(tab) + p0;
-      gpp_prep_kernel<<<prep_grid_for(rows), 256, 0, stream>>>((int)nb, (int)rows, (int)G, inv + p0, indinv,
-                                                               indinv_len, wt_c, am, an, vc, nullptr, S_c,
-                                                               env->d_status);
+      gpp_prep_kernel<<<prep_grid_for(rows), 256, 0, stream>>>(
+          (int)nb, (int)rows, (int)G, inv + p0, indinv, indinv_len, wt_c, gstride ? am + p0 : am,
+          gstride ? an + p0 : an, gstride ? vc + p0 : vc, nullptr, S_c, env->d_status, gstride);
       count_launch();
       BGW_CUDA_TRY(cudaGetLastError());
       const int nchunks_g = (int)((G + kChunk - 1) / kChunk);
@@ -362,9 +379,9 @@ int gpp_enqueue_chunks(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int
       total += grid;
     } else {
       double2 *st_c = static_cast<double2 *>(tab) + (size_t)p0 * nb;
-      gpp_prep_kernel<<<prep_grid_for(rows), 256, 0, stream>>>((int)nb, (int)rows, (int)G, inv + p0, indinv,
-                                                               indinv_len, wt_c, am, an, vc, st_c, nullptr,
-                                                               env->d_status);
+      gpp_prep_kernel<<<prep_grid_for(rows), 256, 0, stream>>>(
+          (int)nb, (int)rows, (int)G, inv + p0, indinv, indinv_len, wt_c, gstride ? am + p0 : am,
+          gstride ? an + p0 : an, gstride ? vc + p0 : vc, st_c, nullptr, env->d_status, gstride);
       count_launch();
       BGW_CUDA_TRY(cudaGetLastError());
       if (c == 0) BGW_TRY(prof_mark(env, 1));
@@ -420,42 +437,97 @@ int gpp_run_host(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *
   // stream (earlier users of the staging buffers).
   BGW_CUDA_TRY(cudaEventRecord(ws->copy_start, env->stream));
   BGW_CUDA_TRY(cudaStreamWaitEvent(cs, ws->copy_start, 0));
-  const size_t pg = (size_t)P * (size_t)G * 16, ng = (size_t)nb * (size_t)G * 16;
+  const size_t pg = (size_t)P * (size_t)G * 16;
+  const size_t nbp = (size_t)nb * (size_t)P;
   void *d_inv, *d_ind, *d_wx, *d_vc, *d_am, *d_an, *d_wt, *d_ie;
   BGW_TRY(ws_reserve(ws, SLOT_IN0, sizeof(int32_t) * (size_t)P, &d_inv));
   BGW_TRY(ws_reserve(ws, SLOT_IN1, sizeof(int32_t) * (size_t)indinv_len, &d_ind));
   BGW_TRY(ws_reserve(ws, SLOT_IN2, sizeof(double) * wx_n, &d_wx));
-  BGW_TRY(ws_reserve(ws, SLOT_IN7, sizeof(double) * (size_t)G, &d_vc));
-  BGW_TRY(ws_reserve(ws, SLOT_IN4, ng, &d_am));
-  BGW_TRY(ws_reserve(ws, SLOT_IN5, ng, &d_an));
+  BGW_TRY(ws_reserve(ws, SLOT_IN7, sizeof(double) * (size_t)std::max<int64_t>(P, 1), &d_vc));
+  BGW_TRY(ws_reserve(ws, SLOT_IN4, nbp * 16, &d_am));
+  BGW_TRY(ws_reserve(ws, SLOT_IN5, nbp * 16, &d_an));
   BGW_TRY(ws_reserve(ws, SLOT_IN3, pg, &d_wt));
   BGW_TRY(ws_reserve(ws, SLOT_IN6, pg, &d_ie));
   auto h2d = [&](void *dst, const void *src, size_t bytes) -> int {
     if (bytes) BGW_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, cs));
     return BGW_OK;
   };
-  BGW_TRY(h2d(d_inv, inv, sizeof(int32_t) * (size_t)P));
-  BGW_TRY(h2d(d_ind, indinv, sizeof(int32_t) * (size_t)indinv_len));
-  BGW_TRY(h2d(d_wx, wx, sizeof(double) * wx_n));
-  BGW_TRY(h2d(d_vc, vc, sizeof(double) * (size_t)G));
-  BGW_TRY(h2d(d_am, am, ng));
-  BGW_TRY(h2d(d_an, an, ng));
-  // About 8 chunks of at least 64 rows.
+  // Up to 16 chunks of at least 64 rows.
   RowChunks rc;
-  rc.n = (int)std::max<int64_t>(1, std::min<int64_t>(8, P / 64));
+  rc.n = (int)std::max<int64_t>(1, std::min<int64_t>(RowChunks::kMax, P / 64));
   for (int c = 0; c <= rc.n; ++c) rc.p0[c] = P * c / rc.n;
   for (int c = 0; c < rc.n; ++c) rc.ready[c] = ws->chunk_ready[c];
-  auto issue = [&](int c) -> int {
+  auto copy_rows = [&](int c) -> int {
     const size_t off = (size_t)rc.p0[c] * G * 16, bytes = (size_t)(rc.p0[c + 1] - rc.p0[c]) * G * 16;
     BGW_TRY(h2d(static_cast<char *>(d_wt) + off, reinterpret_cast<const char *>(wt) + off, bytes));
     BGW_TRY(h2d(static_cast<char *>(d_ie) + off, reinterpret_cast<const char *>(ie) + off, bytes));
+    return BGW_OK;
+  };
+  // Chunk 0's wtilde / I_eps rows go first, so the copy engine works while
+  // the host gathers the aqs columns below.
+  BGW_TRY(copy_rows(0));
+
+  // The kernels read aqsmtemp / aqsntemp / vcoul only at the columns
+  // igp(p) = indinv[inv_igp_index[p]]: those are gathered here into a
+  // page-locked buffer ([nb][P] complex twice, then P doubles), so nb*P
+  // instead of nb*G values cross PCIe before the first chunk can start.  An
+  // out-of-range index gathers zeros; the device still resolves and checks
+  // every index and reports BGW_ERR_INDEX as for device-memory inputs.
+  const size_t gbytes = 2 * nbp * 16 + (size_t)P * 8;
+  void *pinned = nullptr;
+  BGW_TRY(ws_reserve_pinned(ws, gbytes, &pinned));
+  double2 *g_am = static_cast<double2 *>(pinned), *g_an = g_am + nbp;
+  double *g_vc = reinterpret_cast<double *>(g_an + nbp);
+  {
+    std::vector<int64_t> igp((size_t)P);
+    std::vector<int32_t> order;  // valid columns, ascending igp (monotone reads per band row)
+    order.reserve((size_t)P);
+    for (int64_t p = 0; p < P; ++p) {
+      const int32_t a = inv[p];
+      const int64_t g = (a >= 0 && (int64_t)a < indinv_len) ? (int64_t)indinv[a] : -1;
+      igp[(size_t)p] = (g >= 0 && g < G) ? g : -1;
+      g_vc[p] = igp[(size_t)p] >= 0 ? vc[igp[(size_t)p]] : 0.0;
+      if (igp[(size_t)p] >= 0) order.push_back((int32_t)p);
+      else
+        for (int64_t n1 = 0; n1 < nb; ++n1) g_am[(size_t)n1 * P + p] = g_an[(size_t)n1 * P + p] = double2{0.0, 0.0};
+    }
+    std::sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return igp[(size_t)x] < igp[(size_t)y]; });
+    const double2 *am2 = reinterpret_cast<const double2 *>(am), *an2 = reinterpret_cast<const double2 *>(an);
+    auto gather = [&](int64_t b0, int64_t b1) {
+      for (int64_t n1 = b0; n1 < b1; ++n1) {
+        const double2 *ra = am2 + (size_t)n1 * G, *rn = an2 + (size_t)n1 * G;
+        double2 *da = g_am + (size_t)n1 * P, *dn = g_an + (size_t)n1 * P;
+        for (int32_t p : order) {
+          const int64_t g = igp[(size_t)p];
+          da[p] = ra[g];
+          dn[p] = rn[g];
+        }
+      }
+    };
+    const int nthreads = (int)std::max<int64_t>(
+        1, std::min<int64_t>({16, (int64_t)std::thread::hardware_concurrency(), (int64_t)(nbp / 65536)}));
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nthreads; ++t) pool.emplace_back(gather, nb * t / nthreads, nb * (t + 1) / nthreads);
+    gather(0, nb / nthreads);
+    for (auto &th : pool) th.join();
+  }
+  BGW_TRY(h2d(d_inv, inv, sizeof(int32_t) * (size_t)P));
+  BGW_TRY(h2d(d_ind, indinv, sizeof(int32_t) * (size_t)indinv_len));
+  BGW_TRY(h2d(d_wx, wx, sizeof(double) * wx_n));
+  BGW_TRY(h2d(d_vc, g_vc, sizeof(double) * (size_t)P));
+  BGW_TRY(h2d(d_am, g_am, nbp * 16));
+  BGW_TRY(h2d(d_an, g_an, nbp * 16));
+  BGW_CUDA_TRY(cudaEventRecord(ws->chunk_ready[0], cs));  // chunk 0 and the per-band inputs
+  auto issue = [&](int c) -> int {
+    if (c == 0) return BGW_OK;
+    BGW_TRY(copy_rows(c));
     BGW_CUDA_TRY(cudaEventRecord(ws->chunk_ready[c], cs));
     return BGW_OK;
   };
   return gpp_enqueue_chunks(env, nb, P, G, (const int32_t *)d_inv, (const int32_t *)d_ind, indinv_len,
                             (const double *)d_wx, wx_stride, (const double2 *)d_wt, (const double2 *)d_am,
                             (const double2 *)d_an, (const double2 *)d_ie, (const double *)d_vc, achtemp_dev, rc,
-                            issue);
+                            issue, (long long)P);
 }
 
 // ------------------------------------------------------ no-allocation path --
@@ -550,7 +622,8 @@ extern "C" int bgw_noflagOCC_solver_noalloc(int64_t number_bands, int64_t ngpown
   gpp_prep_kernel<<<prep_grid, 256, 0, s>>>((int)nb, (int)P, (int)G, inv_igp_index, indinv, indinv_len,
                                             reinterpret_cast<const double2 *>(wtilde_array),
                                             reinterpret_cast<const double2 *>(aqsmtemp),
-                                            reinterpret_cast<const double2 *>(aqsntemp), vcoul, nullptr, S, status);
+                                            reinterpret_cast<const double2 *>(aqsntemp), vcoul, nullptr, S, status,
+                                            0LL);
   count_launch();
   BGW_CUDA_TRY(cudaGetLastError());
   int grid = (int)std::min<long long>(std::max<long long>(items, 1), (long long)sms * 8);

@@ -32,6 +32,27 @@ Workspace *workspace_for(int device) {
   return g_ws[device].get();
 }
 
+int ws_reserve_pinned(Workspace *ws, size_t bytes, void **out) {
+  if (bytes == 0) bytes = 256;
+  if (ws->pinned_cap < bytes) {
+    if (ws->pinned) {
+      BGW_CUDA_TRY(cudaDeviceSynchronize());
+      BGW_CUDA_TRY(cudaFreeHost(ws->pinned));
+      ws->pinned = nullptr;
+      ws->pinned_cap = 0;
+    }
+    cudaError_t e = cudaHostAlloc(&ws->pinned, bytes, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      ws->pinned = nullptr;
+      return BGW_ERR_ALLOC;
+    }
+    ws->pinned_cap = bytes;
+  }
+  *out = ws->pinned;
+  return BGW_OK;
+}
+
 int ws_reserve(Workspace *ws, int s, size_t bytes, void **out) {
   if (bytes == 0) bytes = 256;
   if (ws->cap[s] < bytes) {
@@ -225,6 +246,9 @@ int bgw_release_workspace(int32_t device) {
       ws->buf[s] = nullptr;
       ws->cap[s] = 0;
     }
+    if (ws->pinned) BGW_CUDA_TRY(cudaFreeHost(ws->pinned));
+    ws->pinned = nullptr;
+    ws->pinned_cap = 0;
   }
   return BGW_OK;
 }
