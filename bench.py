@@ -307,6 +307,11 @@ def run_ours(args, world, rank, local):
         extra["e2e_pageable"] = {"value": page_s, "unit": "s", "h2d_bytes_per_step": int(h2d),
                                  "d2h_bytes_per_step": 48, "steps": page_n,
                                  "note": "band loop, BGW_MEMORY_HOST on pageable numpy buffers"}
+        auto_page_s, _, _ = time_e2e("auto")
+        extra["e2e_auto_pageable"] = {"value": auto_page_s, "unit": "s", "h2d_bytes_per_step": int(h2d),
+                                      "d2h_bytes_per_step": 48,
+                                      "note": "default algorithm on pageable numpy buffers: what the reference's "
+                                              "own driver gets through the drop-in"}
         gp = gp_pinned
         auto_s, _, auto_res = time_e2e("auto")
         extra["e2e_auto"] = {"value": auto_s, "unit": "s", "h2d_bytes_per_step": int(h2d),

@@ -81,6 +81,7 @@ struct Workspace {
   cudaStream_t copy_stream = nullptr;  // host-input staging (non-blocking)
   cudaEvent_t copy_start = nullptr;
   cudaEvent_t chunk_ready[16] = {};
+  cudaEvent_t stage_free[2] = {};  // page-locked staging slot reusable
   int sm_count = 0;
   int device = -1;
   void *pinned = nullptr;  // page-locked host staging (grow-only)

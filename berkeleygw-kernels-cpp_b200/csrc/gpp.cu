@@ -21,6 +21,7 @@
 // reruns are bitwise identical.
 #include <algorithm>
 #include <cstdio>
+#include <cstring>
 #include <functional>
 #include <thread>
 #include <type_traits>
@@ -36,6 +37,31 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kElems = 4;                 // ig elements per thread
 constexpr int kChunk = kThreads * kElems;  // ig per item
+
+// Runs fn(i0, i1) over [0, n) split into `parts` contiguous ranges, one host
+// thread each (the calling thread takes the first).
+void parallel_ranges(int64_t n, int parts, const std::function<void(int64_t, int64_t)> &fn) {
+  parts = (int)std::max<int64_t>(1, std::min<int64_t>(parts, n));
+  std::vector<std::thread> pool;
+  for (int t = 1; t < parts; ++t) pool.emplace_back(fn, n * t / parts, n * (t + 1) / parts);
+  fn(0, n / parts);
+  for (auto &th : pool) th.join();
+}
+
+int host_threads(int64_t work_items, int64_t per_thread) {
+  return (int)std::max<int64_t>(
+      1, std::min<int64_t>({16, (int64_t)std::thread::hardware_concurrency(), work_items / per_thread}));
+}
+
+// True when `p` is host memory that CUDA has not page-locked.
+bool is_pageable(const void *p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return true;
+  }
+  return at.type == cudaMemoryTypeUnregistered;
+}
 
 // ---------------------------------------------------------------- prep --
 // st[p][n1] = sch_store1(n1, p); wx4[n1] = (wx[n1][0..2], 0); S[p] (if
@@ -457,10 +483,45 @@ int gpp_run_host(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *
   rc.n = (int)std::max<int64_t>(1, std::min<int64_t>(RowChunks::kMax, P / 64));
   for (int c = 0; c <= rc.n; ++c) rc.p0[c] = P * c / rc.n;
   for (int c = 0; c < rc.n; ++c) rc.ready[c] = ws->chunk_ready[c];
+  // Pageable wtilde / I_eps (the reference drivers' new[] buffers) are
+  // staged through two page-locked slots filled by several host threads:
+  // the memcpy of chunk c+1 overlaps the DMA of chunk c, instead of the
+  // driver's single-threaded staging of every byte.
+  const bool staged = P > 0 && G > 0 && (is_pageable(wt) || is_pageable(ie));
+  int64_t max_rows = 0;
+  for (int c = 0; c < rc.n; ++c) max_rows = std::max<int64_t>(max_rows, rc.p0[c + 1] - rc.p0[c]);
+  const size_t slot_bytes = staged ? 2 * (size_t)max_rows * G * 16 : 0;
+  const size_t gather_bytes = ((2 * nbp * 16 + (size_t)P * 8) + 255) & ~size_t(255);
+  void *pinned = nullptr;
+  BGW_TRY(ws_reserve_pinned(ws, gather_bytes + 2 * slot_bytes, &pinned));
+  unsigned char *slots = static_cast<unsigned char *>(pinned) + gather_bytes;
   auto copy_rows = [&](int c) -> int {
     const size_t off = (size_t)rc.p0[c] * G * 16, bytes = (size_t)(rc.p0[c + 1] - rc.p0[c]) * G * 16;
-    BGW_TRY(h2d(static_cast<char *>(d_wt) + off, reinterpret_cast<const char *>(wt) + off, bytes));
-    BGW_TRY(h2d(static_cast<char *>(d_ie) + off, reinterpret_cast<const char *>(ie) + off, bytes));
+    if (!staged) {
+      BGW_TRY(h2d(static_cast<char *>(d_wt) + off, reinterpret_cast<const char *>(wt) + off, bytes));
+      BGW_TRY(h2d(static_cast<char *>(d_ie) + off, reinterpret_cast<const char *>(ie) + off, bytes));
+      return BGW_OK;
+    }
+    const int slot = c & 1;
+    if (c >= 2) BGW_CUDA_TRY(cudaEventSynchronize(ws->stage_free[slot]));  // DMA of chunk c-2 done
+    unsigned char *dst = slots + (size_t)slot * slot_bytes;
+    const unsigned char *sw = reinterpret_cast<const unsigned char *>(wt) + off;
+    const unsigned char *si = reinterpret_cast<const unsigned char *>(ie) + off;
+    const int64_t blocks = (int64_t)((2 * bytes + (1 << 20) - 1) >> 20);  // 1 MiB pieces of wt | ie
+    parallel_ranges(blocks, host_threads(blocks, 4), [&](int64_t b0, int64_t b1) {
+      for (int64_t b = b0; b < b1; ++b) {
+        const size_t lo = (size_t)b << 20, hi = std::min<size_t>(2 * bytes, lo + (1 << 20));
+        for (size_t x = lo; x < hi;) {  // a piece may straddle the wt / ie boundary
+          const bool in_wt = x < bytes;
+          const size_t end = in_wt ? std::min(hi, bytes) : hi;
+          std::memcpy(dst + x, (in_wt ? sw + x : si + (x - bytes)), end - x);
+          x = end;
+        }
+      }
+    });
+    BGW_TRY(h2d(static_cast<char *>(d_wt) + off, dst, bytes));
+    BGW_TRY(h2d(static_cast<char *>(d_ie) + off, dst + bytes, bytes));
+    BGW_CUDA_TRY(cudaEventRecord(ws->stage_free[slot], cs));
     return BGW_OK;
   };
   // Chunk 0's wtilde / I_eps rows go first, so the copy engine works while
@@ -473,9 +534,6 @@ int gpp_run_host(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *
   // instead of nb*G values cross PCIe before the first chunk can start.  An
   // out-of-range index gathers zeros; the device still resolves and checks
   // every index and reports BGW_ERR_INDEX as for device-memory inputs.
-  const size_t gbytes = 2 * nbp * 16 + (size_t)P * 8;
-  void *pinned = nullptr;
-  BGW_TRY(ws_reserve_pinned(ws, gbytes, &pinned));
   double2 *g_am = static_cast<double2 *>(pinned), *g_an = g_am + nbp;
   double *g_vc = reinterpret_cast<double *>(g_an + nbp);
   {
@@ -504,12 +562,7 @@ int gpp_run_host(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *
         }
       }
     };
-    const int nthreads = (int)std::max<int64_t>(
-        1, std::min<int64_t>({16, (int64_t)std::thread::hardware_concurrency(), (int64_t)(nbp / 65536)}));
-    std::vector<std::thread> pool;
-    for (int t = 1; t < nthreads; ++t) pool.emplace_back(gather, nb * t / nthreads, nb * (t + 1) / nthreads);
-    gather(0, nb / nthreads);
-    for (auto &th : pool) th.join();
+    parallel_ranges(nb, host_threads((int64_t)nbp, 65536), gather);
   }
   BGW_TRY(h2d(d_inv, inv, sizeof(int32_t) * (size_t)P));
   BGW_TRY(h2d(d_ind, indinv, sizeof(int32_t) * (size_t)indinv_len));

@@ -92,6 +92,7 @@ int ws_copy_stream(Workspace *ws, cudaStream_t *out) {
     BGW_CUDA_TRY(cudaStreamCreateWithFlags(&ws->copy_stream, cudaStreamNonBlocking));
     BGW_CUDA_TRY(cudaEventCreateWithFlags(&ws->copy_start, cudaEventDisableTiming));
     for (auto &e : ws->chunk_ready) BGW_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto &e : ws->stage_free) BGW_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   }
   *out = ws->copy_stream;
   return BGW_OK;
