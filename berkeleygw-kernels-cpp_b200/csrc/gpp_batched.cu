@@ -18,6 +18,7 @@
 // prefix of the work list (bgw_gpp_batch_create); choices are cached per
 // batch signature for the process.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -226,7 +227,7 @@ __global__ void __launch_bounds__(kBThreads, (MIXED && KE == 8) ? 1 : 2)
 
 // Factored form over the CTA's item range: HBM-bound stream, 128-bit loads.
 template <int KE>
-__global__ void __launch_bounds__(kBThreads)
+__global__ void __launch_bounds__(kBThreads, 4)
     batch_factored_kernel(const BatchInst *__restrict__ inst, int n, const long long *__restrict__ range,
                           int max_seg, double *__restrict__ partials) {
   constexpr int kCH = kBThreads * KE;
@@ -238,32 +239,54 @@ __global__ void __launch_bounds__(kBThreads)
   const int inst_lo = i;
   double acc_r[3] = {0.0, 0.0, 0.0}, acc_i[3] = {0.0, 0.0, 0.0};
   double lo_r[3] = {0.0, 0.0, 0.0}, lo_i[3] = {0.0, 0.0, 0.0};
+  // The current instance's fields, kept in registers.
+  long long item0 = inst[i].item0, next0 = i + 1 < n ? inst[i + 1].item0 : LLONG_MAX;
+  int G = inst[i].G, nchunk = inst[i].nchunk;
+  const double2 *wt = inst[i].wt, *ie = inst[i].ie, *tab = inst[i].tab;
+  double x[3] = {inst[i].wx[0], inst[i].wx[1], inst[i].wx[2]};
   for (long long j = j0; j < j1; ++j) {
-    while (i + 1 < n && inst[i + 1].item0 <= j) ++i;
-    const BatchInst &I = inst[i];
-    const long long local = j - I.item0;
-    const int p = (int)(local / I.nchunk);
-    const int g0 = (int)(local % I.nchunk) * kCH;
-    const double x[3] = {I.wx[0], I.wx[1], I.wx[2]};
-    double tr[3] = {0.0, 0.0, 0.0}, ti[3] = {0.0, 0.0, 0.0};
+    if (next0 <= j) {
+      while (i + 1 < n && inst[i + 1].item0 <= j) ++i;
+      item0 = inst[i].item0;
+      next0 = i + 1 < n ? inst[i + 1].item0 : LLONG_MAX;
+      G = inst[i].G;
+      nchunk = inst[i].nchunk;
+      wt = inst[i].wt;
+      ie = inst[i].ie;
+      tab = inst[i].tab;
+      x[0] = inst[i].wx[0];
+      x[1] = inst[i].wx[1];
+      x[2] = inst[i].wx[2];
+    }
+    const long long local = j - item0;
+    const int p = (int)(local / nchunk);
+    const int g0 = (int)(local % nchunk) * kCH;
+    // All of the item's loads first (streamed once: evict-first), then the math.
+    double2 w[KE], v[KE];
 #pragma unroll
     for (int k = 0; k < KE; ++k) {
       const int ig = g0 + k * kBThreads + tid;
-      double2 w = make_double2(0.0, 1.0), v = make_double2(0.0, 0.0);
-      if (ig < I.G) {
-        w = __ldcs(I.wt + (size_t)p * I.G + ig);
-        v = __ldcs(I.ie + (size_t)p * I.G + ig);
-      }
-      const double wi2 = w.y * w.y, a = -w.y * v.y, b = w.y * v.x;
-#pragma unroll
-      for (int iw = 0; iw < 3; ++iw) {
-        const double dr = x[iw] - w.x;
-        const double r = rcp_refined(fma(dr, dr, wi2));
-        tr[iw] = fma(fma(dr, v.x, a), r, tr[iw]);
-        ti[iw] = fma(fma(dr, v.y, b), r, ti[iw]);
+      const size_t at = (size_t)p * G + min(ig, G - 1);
+      w[k] = __ldcs(wt + at);
+      v[k] = __ldcs(ie + at);
+      if (ig >= G) {
+        w[k] = make_double2(0.0, 1.0);
+        v[k] = make_double2(0.0, 0.0);
       }
     }
-    const double2 s = I.tab[p];
+    double tr[3] = {0.0, 0.0, 0.0}, ti[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < KE; ++k) {
+      const double wi2 = w[k].y * w[k].y, a = -w[k].y * v[k].y, b = w[k].y * v[k].x;
+#pragma unroll
+      for (int iw = 0; iw < 3; ++iw) {
+        const double dr = x[iw] - w[k].x;
+        const double r = rcp_refined(fma(dr, dr, wi2));
+        tr[iw] = fma(fma(dr, v[k].x, a), r, tr[iw]);
+        ti[iw] = fma(fma(dr, v[k].y, b), r, ti[iw]);
+      }
+    }
+    const double2 s = tab[p];
 #pragma unroll
     for (int iw = 0; iw < 3; ++iw) {
       acc_r[iw] = fma(tr[iw], s.x, acc_r[iw]);
@@ -271,7 +294,7 @@ __global__ void __launch_bounds__(kBThreads)
       acc_i[iw] = fma(tr[iw], s.y, acc_i[iw]);
       acc_i[iw] = fma(ti[iw], s.x, acc_i[iw]);
     }
-    const bool last = (j + 1 == j1) || (i + 1 < n && inst[i + 1].item0 <= j + 1);
+    const bool last = (j + 1 == j1) || next0 <= j + 1;
     if (last) flush(acc_r, acc_i, lo_r, lo_i, red, partials, max_seg, i - inst_lo);
   }
 }
