@@ -90,7 +90,7 @@ constexpr int kTM = 32;        // rows (bands) per tile
 constexpr int kTN = 64;        // G' columns per tile
 constexpr int kBK = 8;         // complex k per pipeline stage
 constexpr int kLds = kBK + 4;  // padded row stride (double2): 192 B, conflict-free fragment reads
-constexpr int kStages = 3;     // cp.async pipeline depth
+constexpr int kStages = 2;     // cp.async double buffer (3 CTAs / 12 warps per SM fit)
 constexpr int kFFThreads = 128;
 
 struct GroupKey {
