@@ -424,6 +424,17 @@ def run_ours(args, world, rank, local):
             "effective_TFLOPs": pm["flops"] / (mk * 1e-3) / 1e12,
             "rel_err_vs_fp64": {k: rel_err(a.cpu().numpy(), b.cpu().numpy())
                                 for k, a, b in zip(("achsDtemp", "asxDtemp", "achDtemp_cor"), mix_out, ff_out)}}
+        # Through host buffers (the drop-in's case): synchronous calls on the
+        # pageable numpy arrays, inputs staged inside the call.
+        bgw.ff_sigma(f)
+        t0 = time.perf_counter()
+        nh = 3
+        for _ in range(nh):
+            bgw.ff_sigma(f)
+        ff_host_s = (time.perf_counter() - t0) / nh
+        # The call reads ekq / dFreqGrid on the host and copies the slices the plan uses.
+        ff_h2d = (f.aqsmtemp.nbytes + f.aqsntemp.nbytes + f.vcoul.nbytes + f.I_epsR_array.nbytes
+                  + f.I_epsA_array.nbytes + f.inv_igp_index.nbytes + f.indinv.nbytes)
         # Option: iw-dependent wx (nfreqeval distinct outputs), FP64 and mixed.
         piw = {}
         for prec in ("fp64", "mixed"):
@@ -439,6 +450,10 @@ def run_ours(args, world, rank, local):
             piw[prec] = (statistics.mean(ks), statistics.mean(ds), out, pp)
         kf, df, of_, pf = piw["fp64"]
         km, dm, om, _ = piw["mixed"]
+        extra["ff"]["e2e_host_pageable"] = {
+            "value": ff_host_s, "unit": "s", "h2d_bytes_per_step_at_most": int(ff_h2d), "d2h_bytes_per_step": 16 * 21,
+            "note": "bgw_ff_sigma on pageable numpy buffers (wall time of the synchronous call): staging + kernels + "
+                    "outputs; only the frequency slices the plan reads are copied"}
         extra["ff_per_iw"] = {
             "option": "BGW_FLAG_FF_WX_PER_IW: wx = freqevalmin - ekq + iw*freqevalstep, 10 distinct outputs",
             "fp64": {"s_per_sigma": df / 1e3, "contraction_ms": kf,

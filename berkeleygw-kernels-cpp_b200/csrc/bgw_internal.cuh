@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <functional>
 #include <cstddef>
 #include <mutex>
 
@@ -86,6 +87,7 @@ struct Workspace {
   int device = -1;
   void *pinned = nullptr;  // page-locked host staging (grow-only)
   size_t pinned_cap = 0;
+  void *stage_slots = nullptr;  // two page-locked slots for stage_input
 };
 
 // Returns the workspace of `device` (created on first use).
@@ -123,8 +125,21 @@ void set_last_profile(const bgw_profile &p);
 // Validates options, selects the device, fetches the workspace.
 int begin_call(const bgw_options *user, CallEnv *env);
 // Copies `bytes` from a host or device input into a device pointer usable
-// by kernels (host memory: staged into slot `s`).
+// by kernels (host memory: staged into slot `s`; large pageable inputs go
+// through two page-locked slots filled by several host threads, so the host
+// copy of one piece overlaps the DMA of the previous one).
 int stage_input(CallEnv *env, int s, const void *src, size_t bytes, const void **dev_out);
+
+// Runs fn(i0, i1) over [0, n) in `parts` contiguous ranges, one host thread
+// each (the calling thread takes the first).
+void parallel_ranges(int64_t n, int parts, const std::function<void(int64_t, int64_t)> &fn);
+// Host threads for `work_items` items of which each thread should get at
+// least `per_thread` (at most 16 and the hardware concurrency).
+int host_threads(int64_t work_items, int64_t per_thread);
+// True when `p` is host memory that CUDA has not page-locked.
+bool is_pageable(const void *p);
+// memcpy of `bytes` by several host threads (1 MiB pieces).
+void parallel_memcpy(void *dst, const void *src, size_t bytes);
 // Synchronous completion: waits for the stream, reads the device status.
 int finish_call(CallEnv *env);
 

@@ -38,30 +38,6 @@ constexpr int kThreads = 256;
 constexpr int kElems = 4;                 // ig elements per thread
 constexpr int kChunk = kThreads * kElems;  // ig per item
 
-// Runs fn(i0, i1) over [0, n) split into `parts` contiguous ranges, one host
-// thread each (the calling thread takes the first).
-void parallel_ranges(int64_t n, int parts, const std::function<void(int64_t, int64_t)> &fn) {
-  parts = (int)std::max<int64_t>(1, std::min<int64_t>(parts, n));
-  std::vector<std::thread> pool;
-  for (int t = 1; t < parts; ++t) pool.emplace_back(fn, n * t / parts, n * (t + 1) / parts);
-  fn(0, n / parts);
-  for (auto &th : pool) th.join();
-}
-
-int host_threads(int64_t work_items, int64_t per_thread) {
-  return (int)std::max<int64_t>(
-      1, std::min<int64_t>({16, (int64_t)std::thread::hardware_concurrency(), work_items / per_thread}));
-}
-
-// True when `p` is host memory that CUDA has not page-locked.
-bool is_pageable(const void *p) {
-  cudaPointerAttributes at;
-  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
-    (void)cudaGetLastError();
-    return true;
-  }
-  return at.type == cudaMemoryTypeUnregistered;
-}
 
 // ---------------------------------------------------------------- prep --
 // st[p][n1] = sch_store1(n1, p); wx4[n1] = (wx[n1][0..2], 0); S[p] (if

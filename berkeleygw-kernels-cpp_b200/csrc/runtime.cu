@@ -1,9 +1,13 @@
 // runtime.cu -- options, per-device workspace cache, host<->device staging
 // and status handling shared by every libbgwsigma entry point.
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+
+#include <thread>
+#include <vector>
 
 #include "bgw_internal.cuh"
 
@@ -150,6 +154,41 @@ int begin_call(const bgw_options *user, CallEnv *env) {
   return BGW_OK;
 }
 
+void parallel_ranges(int64_t n, int parts, const std::function<void(int64_t, int64_t)> &fn) {
+  parts = (int)std::max<int64_t>(1, std::min<int64_t>(parts, n));
+  std::vector<std::thread> pool;
+  for (int t = 1; t < parts; ++t) pool.emplace_back(fn, n * t / parts, n * (t + 1) / parts);
+  fn(0, n / parts);
+  for (auto &th : pool) th.join();
+}
+
+int host_threads(int64_t work_items, int64_t per_thread) {
+  return (int)std::max<int64_t>(
+      1, std::min<int64_t>({16, (int64_t)std::thread::hardware_concurrency(), work_items / per_thread}));
+}
+
+bool is_pageable(const void *p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return true;
+  }
+  return at.type == cudaMemoryTypeUnregistered;
+}
+
+void parallel_memcpy(void *dst, const void *src, size_t bytes) {
+  const int64_t pieces = (int64_t)((bytes + (1 << 20) - 1) >> 20);
+  parallel_ranges(pieces, host_threads(pieces, 4), [&](int64_t b0, int64_t b1) {
+    const size_t lo = (size_t)b0 << 20, hi = std::min(bytes, (size_t)b1 << 20);
+    if (hi > lo) std::memcpy(static_cast<char *>(dst) + lo, static_cast<const char *>(src) + lo, hi - lo);
+  });
+}
+
+namespace {
+constexpr size_t kStageSlot = size_t(32) << 20;        // bytes per page-locked slot
+constexpr size_t kStageMin = size_t(8) << 20;          // smaller inputs: one plain copy
+}  // namespace
+
 int stage_input(CallEnv *env, int s, const void *src, size_t bytes, const void **dev_out) {
   if (!env->host) {
     if ((reinterpret_cast<uintptr_t>(src) & 15u) != 0) return BGW_ERR_INVALID_ARG;
@@ -157,9 +196,35 @@ int stage_input(CallEnv *env, int s, const void *src, size_t bytes, const void *
     return BGW_OK;
   }
   void *d = nullptr;
-  BGW_TRY(ws_reserve(env->ws, s, bytes, &d));
-  if (bytes) BGW_CUDA_TRY(cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, env->stream));
+  Workspace *ws = env->ws;
+  BGW_TRY(ws_reserve(ws, s, bytes, &d));
   *dev_out = d;
+  if (!bytes) return BGW_OK;
+  if (bytes < kStageMin || !is_pageable(src)) {
+    BGW_CUDA_TRY(cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, env->stream));
+    return BGW_OK;
+  }
+  // Pageable: pieces of kStageSlot bytes, alternating between two slots; a
+  // slot is refilled only after the DMA that read it has completed.
+  cudaStream_t cs = nullptr;
+  BGW_TRY(ws_copy_stream(ws, &cs));  // creates the slot events
+  if (!ws->stage_slots) {
+    cudaError_t e = cudaHostAlloc(&ws->stage_slots, 2 * kStageSlot, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+      (void)cudaGetLastError();
+      ws->stage_slots = nullptr;
+      return BGW_ERR_ALLOC;
+    }
+  }
+  for (size_t off = 0, k = 0; off < bytes; off += kStageSlot, ++k) {
+    const size_t n = std::min(kStageSlot, bytes - off);
+    const int slot = (int)(k & 1);
+    BGW_CUDA_TRY(cudaEventSynchronize(ws->stage_free[slot]));
+    char *buf = static_cast<char *>(ws->stage_slots) + (size_t)slot * kStageSlot;
+    parallel_memcpy(buf, static_cast<const char *>(src) + off, n);
+    BGW_CUDA_TRY(cudaMemcpyAsync(static_cast<char *>(d) + off, buf, n, cudaMemcpyHostToDevice, env->stream));
+    BGW_CUDA_TRY(cudaEventRecord(ws->stage_free[slot], env->stream));
+  }
   return BGW_OK;
 }
 
@@ -250,6 +315,8 @@ int bgw_release_workspace(int32_t device) {
     if (ws->pinned) BGW_CUDA_TRY(cudaFreeHost(ws->pinned));
     ws->pinned = nullptr;
     ws->pinned_cap = 0;
+    if (ws->stage_slots) BGW_CUDA_TRY(cudaFreeHost(ws->stage_slots));
+    ws->stage_slots = nullptr;
   }
   return BGW_OK;
 }
