@@ -13,7 +13,8 @@
 // The quotients are recomputed (nothing of size bands x G' x G is stored).
 // This is the factored form: valid for the reference's band-independent wx.
 //
-// One CTA streams whole G' rows (round robin): it writes both gradient rows,
+// One CTA streams whole G' rows (round robin, staged in chunks by bulk
+// copies): it writes both gradient rows,
 // reduces T(p, .) over the row with a fixed-order block sum and adds the
 // sch_store1 term at (p, igp) itself, so no second pass over the row is
 // needed.  dSigma/domega is reduced per CTA, then in a fixed order.
@@ -28,7 +29,6 @@ namespace bgw {
 namespace {
 
 constexpr int kAdjThreads = 256;
-constexpr int kAdjElems = 2;
 
 // C(p), S(p) = C(p) wtilde[p][igp] and igp(p) (-1 if out of range).  One
 // warp per column, fixed-order band sum.
@@ -66,98 +66,132 @@ __global__ void __launch_bounds__(256)
 __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 
+constexpr int kAdjChunk = 1024;  // G elements of a row per staged step
+
+struct AdjSmem {
+  double2 wt[2][kAdjChunk];
+  double2 ie[2][kAdjChunk];
+  unsigned long long bar[2];
+  double red[(kAdjThreads / 32) * 6];
+};
+
 // grad_wt / grad_ie may be null (not requested).  partials: 6 doubles per
-// CTA (dSigma_iw/domega, re/im).
+// CTA (dSigma_iw/domega, re/im).  The CTA's rows are walked in chunks of
+// kAdjChunk elements; thread 0 stages chunk j + 1 of wtilde / I_eps into
+// shared memory with 1-D bulk copies (TMA engine, mbarrier completion,
+// double-buffered) while the block computes chunk j, so HBM reads are in
+// flight without costing registers.  Every wait is bounded.
 __global__ void __launch_bounds__(kAdjThreads, 2)
     gpp_adjoint_kernel(int P, int G, const double2 *__restrict__ wtilde, const double2 *__restrict__ ieps,
                        const double2 *__restrict__ Cp, const double2 *__restrict__ Sp, const int *__restrict__ igp,
                        const double *__restrict__ wx3, const double2 *__restrict__ gcot,
-                       double2 *__restrict__ grad_wt, double2 *__restrict__ grad_ie, double *__restrict__ partials) {
-  __shared__ double red[(kAdjThreads / 32) * 6];
+                       double2 *__restrict__ grad_wt, double2 *__restrict__ grad_ie, double *__restrict__ partials,
+                       int *status) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  AdjSmem &sm = *reinterpret_cast<AdjSmem *>(smem_raw);
   const int tid = threadIdx.x;
   const double x[3] = {wx3[0], wx3[1], wx3[2]};
   // conj(G_iw): the cotangents enter as sum_iw conj(G_iw) dSigma_iw/dz.
   const double2 cg[3] = {cconj(gcot[0]), cconj(gcot[1]), cconj(gcot[2])};
   double dw_r[3] = {0.0, 0.0, 0.0}, dw_i[3] = {0.0, 0.0, 0.0};  // sum S I q^2 (sign applied at the end)
-  for (int p = blockIdx.x; p < P; p += gridDim.x) {
+
+  const int nch = (G + kAdjChunk - 1) / kAdjChunk;
+  const long long my_rows = (long long)blockIdx.x < P ? (P - 1 - (long long)blockIdx.x) / gridDim.x + 1 : 0;
+  const long long nsteps = my_rows * nch;
+  if (tid == 0) {
+    mbar_init(reinterpret_cast<uint64_t *>(&sm.bar[0]), 1);
+    mbar_init(reinterpret_cast<uint64_t *>(&sm.bar[1]), 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  auto issue = [&](long long j) {
+    const long long p = blockIdx.x + (j / nch) * (long long)gridDim.x;
+    const int g0 = (int)(j % nch) * kAdjChunk;
+    const int nvalid = min(kAdjChunk, G - g0);
+    const int buf = (int)(j & 1);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(&sm.bar[buf]);
+    mbar_expect_tx(bar, 2u * (uint32_t)nvalid * 16u);
+    bulk_g2s(sm.wt[buf], wtilde + p * G + g0, (uint32_t)nvalid * 16u, bar);
+    bulk_g2s(sm.ie[buf], ieps + p * G + g0, (uint32_t)nvalid * 16u, bar);
+  };
+  bool ok = true;
+  if (tid == 0 && nsteps > 0) issue(0);
+  double t_r[3] = {0.0, 0.0, 0.0}, t_i[3] = {0.0, 0.0, 0.0};  // T(p, iw) (this thread)
+  double u_r[3] = {0.0, 0.0, 0.0}, u_i[3] = {0.0, 0.0, 0.0};  // sum_ig I q^2 (this thread)
+  for (long long j = 0; j < nsteps; ++j) {
+    if (tid == 0 && j + 1 < nsteps) issue(j + 1);
+    const int buf = (int)(j & 1);
+    if (!mbar_wait_bounded(reinterpret_cast<uint64_t *>(&sm.bar[buf]), (uint32_t)((j >> 1) & 1), kWaitCycles)) {
+      raise_status(status, BGW_ERR_TIMEOUT, blockIdx.x);
+      ok = false;
+    }
+    if (__syncthreads_or(!ok)) break;  // every thread agrees before leaving
+    const long long p = blockIdx.x + (j / nch) * (long long)gridDim.x;
+    const int c = (int)(j % nch);
+    const int g0 = c * kAdjChunk;
+    const int nvalid = min(kAdjChunk, G - g0);
     const double2 S = Sp[p];
-    double t_r[3] = {0.0, 0.0, 0.0}, t_i[3] = {0.0, 0.0, 0.0};   // T(p, iw)
-    double u_r[3] = {0.0, 0.0, 0.0}, u_i[3] = {0.0, 0.0, 0.0};   // sum_ig I q^2 (this thread)
-    // Loads of chunk g0 + step are issued before chunk g0 is computed
-    // (register double buffering), so HBM traffic overlaps the FP64 work.
-    constexpr int kStep = kAdjThreads * kAdjElems;
-    double2 w[kAdjElems], v[kAdjElems], wn[kAdjElems], vn[kAdjElems];
-    auto load = [&](int g0, double2 (&ww)[kAdjElems], double2 (&vv)[kAdjElems]) {
+#pragma unroll 1
+    for (int k = 0; k < kAdjChunk / kAdjThreads; ++k) {
+      const int idx = k * kAdjThreads + tid;
+      if (idx >= nvalid) break;
+      const double2 w = sm.wt[buf][idx], v = sm.ie[buf][idx];
+      double2 hI = make_double2(0.0, 0.0), hW = make_double2(0.0, 0.0);
 #pragma unroll
-      for (int k = 0; k < kAdjElems; ++k) {
-        const int ig = g0 + k * kAdjThreads + tid;
-        if (ig < G) {
-          ww[k] = __ldcs(wtilde + (size_t)p * G + ig);
-          vv[k] = __ldcs(ieps + (size_t)p * G + ig);
-        } else {
-          ww[k] = make_double2(0.0, 1.0);
-          vv[k] = make_double2(0.0, 0.0);
+      for (int iw = 0; iw < 3; ++iw) {
+        const double dr = x[iw] - w.x;
+        const double r = rcp_refined(fma(dr, dr, w.y * w.y));
+        const double2 q = make_double2(dr * r, w.y * r);  // 1 / (x - w)
+        const double2 iq = cmul(v, q);                     // I q
+        const double2 iq2 = cmul(iq, q);                   // I q^2
+        t_r[iw] += iq.x;
+        t_i[iw] += iq.y;
+        u_r[iw] += iq2.x;
+        u_i[iw] += iq2.y;
+        hI = cadd(hI, cmul(cg[iw], q));
+        hW = cadd(hW, cmul(cg[iw], iq2));
+      }
+      // grad = conj(sum_iw conj(G_iw) dSigma_iw/dz)
+      const size_t at = (size_t)p * G + g0 + idx;
+      if (grad_ie) __stcs(grad_ie + at, cconj(cmul(S, hI)));
+      if (grad_wt) __stcs(grad_wt + at, cconj(cmul(S, hW)));
+    }
+    __syncthreads();  // buffer `buf` is free for step j + 2
+    if (c == nch - 1) {
+      // Row done: S u into dSigma/domega, then T(p, .) over the whole row and
+      // the sch_store1 term at (p, igp): dSigma_iw/dwtilde[p][igp] += C(p) T(p, iw).
+#pragma unroll
+      for (int iw = 0; iw < 3; ++iw) {
+        const double2 su = cmul(S, make_double2(u_r[iw], u_i[iw]));
+        dw_r[iw] += su.x;
+        dw_i[iw] += su.y;
+      }
+      double tv[6] = {t_r[0], t_i[0], t_r[1], t_i[1], t_r[2], t_i[2]};
+      block_sum<6, kAdjThreads>(tv, sm.red);
+      if (tid == 0 && grad_wt) {
+        const int g = igp[p];
+        if (g >= 0) {
+          double2 h = make_double2(0.0, 0.0);
+#pragma unroll
+          for (int iw = 0; iw < 3; ++iw) h = cadd(h, cmul(cg[iw], make_double2(tv[2 * iw], tv[2 * iw + 1])));
+          const double2 add = cconj(cmul(Cp[p], h));
+          const double2 cur = grad_wt[(size_t)p * G + g];
+          grad_wt[(size_t)p * G + g] = cadd(cur, add);
         }
       }
-    };
-    load(0, w, v);
-    for (int g0 = 0; g0 < G; g0 += kStep) {
-      if (g0 + kStep < G) load(g0 + kStep, wn, vn);
+      __syncthreads();
 #pragma unroll
-      for (int k = 0; k < kAdjElems; ++k) {
-        const int ig = g0 + k * kAdjThreads + tid;
-        double2 hI = make_double2(0.0, 0.0), hW = make_double2(0.0, 0.0);
-#pragma unroll
-        for (int iw = 0; iw < 3; ++iw) {
-          const double dr = x[iw] - w[k].x;
-          const double r = rcp_refined(fma(dr, dr, w[k].y * w[k].y));
-          const double2 q = make_double2(dr * r, w[k].y * r);         // 1 / (x - w)
-          const double2 iq = cmul(v[k], q);                            // I q
-          const double2 iq2 = cmul(iq, q);                             // I q^2
-          t_r[iw] += iq.x;
-          t_i[iw] += iq.y;
-          u_r[iw] += iq2.x;
-          u_i[iw] += iq2.y;
-          hI = cadd(hI, cmul(cg[iw], q));
-          hW = cadd(hW, cmul(cg[iw], iq2));
-        }
-        if (ig < G) {
-          // grad = conj(sum_iw conj(G_iw) dSigma_iw/dz)
-          if (grad_ie) __stcs(grad_ie + (size_t)p * G + ig, cconj(cmul(S, hI)));
-          if (grad_wt) __stcs(grad_wt + (size_t)p * G + ig, cconj(cmul(S, hW)));
-        }
-      }
-#pragma unroll
-      for (int k = 0; k < kAdjElems; ++k) {
-        w[k] = wn[k];
-        v[k] = vn[k];
-      }
+      for (int iw = 0; iw < 3; ++iw) t_r[iw] = t_i[iw] = u_r[iw] = u_i[iw] = 0.0;
     }
-#pragma unroll
-    for (int iw = 0; iw < 3; ++iw) {
-      const double2 su = cmul(S, make_double2(u_r[iw], u_i[iw]));
-      dw_r[iw] += su.x;
-      dw_i[iw] += su.y;
-    }
-    // T(p, .) over the whole row, then the sch_store1 term at (p, igp):
-    // dSigma_iw/dwtilde[p][igp] += C(p) T(p, iw).
-    double tv[6] = {t_r[0], t_i[0], t_r[1], t_i[1], t_r[2], t_i[2]};
-    block_sum<6, kAdjThreads>(tv, red);
-    if (tid == 0 && grad_wt) {
-      const int g = igp[p];
-      if (g >= 0) {
-        double2 h = make_double2(0.0, 0.0);
-#pragma unroll
-        for (int iw = 0; iw < 3; ++iw) h = cadd(h, cmul(cg[iw], make_double2(tv[2 * iw], tv[2 * iw + 1])));
-        const double2 add = cconj(cmul(Cp[p], h));
-        double2 cur = grad_wt[(size_t)p * G + g];
-        grad_wt[(size_t)p * G + g] = cadd(cur, add);
-      }
-    }
-    __syncthreads();
+  }
+  if (!ok && tid == 0) {
+    // Let copies still in flight land before the CTA's shared memory is
+    // released (bounded as well).
+    (void)mbar_wait_bounded(reinterpret_cast<uint64_t *>(&sm.bar[0]), 0, kWaitCycles);
+    (void)mbar_wait_bounded(reinterpret_cast<uint64_t *>(&sm.bar[1]), 0, kWaitCycles);
   }
   double vv[6] = {-dw_r[0], -dw_i[0], -dw_r[1], -dw_i[1], -dw_r[2], -dw_i[2]};
-  block_sum<6, kAdjThreads>(vv, red);
+  block_sum<6, kAdjThreads>(vv, sm.red);
   if (tid == 0) {
 #pragma unroll
     for (int k = 0; k < 6; ++k) partials[(size_t)blockIdx.x * 6 + k] = vv[k];
@@ -188,7 +222,9 @@ int gpp_adjoint_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const in
   count_launch();
   BGW_CUDA_TRY(cudaGetLastError());
   int per_sm = 0;
-  BGW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gpp_adjoint_kernel, kAdjThreads, 0));
+  const size_t smem = sizeof(AdjSmem);
+  BGW_CUDA_TRY(cudaFuncSetAttribute(gpp_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  BGW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gpp_adjoint_kernel, kAdjThreads, smem));
   int grid = (int)std::min<long long>(std::max<int64_t>(P, 1), (long long)ws->sm_count * std::max(per_sm, 1));
   BGW_TRY(ws_reserve(ws, SLOT_PARTIALS, sizeof(double) * 6 * (size_t)grid, &partials));
   if (!domega) {
@@ -196,8 +232,8 @@ int gpp_adjoint_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const in
     domega = static_cast<double *>(scratch_out);
   }
   BGW_TRY(prof_mark(env, 1));
-  gpp_adjoint_kernel<<<grid, kAdjThreads, 0, stream>>>((int)P, (int)G, wt, ie, Cp, Sp, igp, wx, gcot, grad_wt,
-                                                       grad_ie, (double *)partials);
+  gpp_adjoint_kernel<<<grid, kAdjThreads, smem, stream>>>((int)P, (int)G, wt, ie, Cp, Sp, igp, wx, gcot, grad_wt,
+                                                          grad_ie, (double *)partials, env->d_status);
   count_launch();
   BGW_CUDA_TRY(cudaGetLastError());
   BGW_TRY(prof_mark(env, 2));
