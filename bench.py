@@ -375,6 +375,20 @@ def run_ours(args, world, rank, local):
                 "dachtemp_domega": rel_err(adj[2].cpu().numpy(), rd)}
             extra["gpp_mixed"]["rel_err_vs_oracle"] = rel_err(mres.cpu().numpy(), Oracle().gpp(g, factored=True))
         del adj
+        # Screened exchange of the occupied bands (bgw_gpp_sigma's asxtemp:
+        # the occupied-band sum at +wx and -wx), device-resident, factored.
+        for _ in range(2):
+            bgw.gpp_sigma(d, stream=sh, algorithm="factored", want_ach=False, flags=bgw.FLAG_PROFILE)
+        sdev = []
+        for _ in range(max(3, args.steps // 2)):
+            _, sx = bgw.gpp_sigma(d, stream=sh, algorithm="factored", want_ach=False, flags=bgw.FLAG_PROFILE)
+            sdev.append(bgw.last_profile()["device_ms"])
+        extra["gpp_sx"] = {"output": "asxtemp", "nvband": g.nvband, "s_per_call": statistics.mean(sdev) / 1e3,
+                           "note": "not in the reference (no flagOCC branch): parity unpinned, checked against "
+                                   "the oracle's product form"}
+        if rank == 0 and not args.no_cpu:
+            from oracle.oracle import Oracle
+            extra["gpp_sx"]["rel_err_vs_oracle"] = rel_err(sx.cpu().numpy(), Oracle().gpp_sx(g, factored=True))
     del d
     torch.cuda.empty_cache()
 

@@ -108,6 +108,7 @@ def load(build_if_needed: bool = True) -> ctypes.CDLL:
     lib.bgw_last_profile.argtypes = [ctypes.POINTER(Profile)]
     opt = ctypes.POINTER(Options)
     lib.bgw_noflagOCC_solver.argtypes = [_I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, opt]
+    lib.bgw_gpp_sigma.argtypes = [_I64, _I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, opt]
     lib.bgw_noflagOCC_solver_noalloc.argtypes = [_I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P,
                                                  ctypes.c_int32, _P]
     lib.bgw_noflagOCC_solver_backward.argtypes = [_I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P,
@@ -219,6 +220,33 @@ def noflagOCC_solver(inp: GppInputs, *, precision="fp64", algorithm="auto", stre
                                   _ptr(out), ctypes.byref(o))
     _check("bgw_noflagOCC_solver", st)
     return out
+
+
+def gpp_sigma(inp: GppInputs, nvband=None, *, want_ach=True, want_asx=True, precision="fp64", algorithm="auto",
+              stream=None, flags=0, device_status=None):
+    """(achtemp[3], asxtemp[3]) complex128: the Coulomb-hole sum over all
+    bands and the GPP screened exchange of the occupied bands n1 < nvband
+    (default: inp.nvband).  A result not asked for is None."""
+    lib = load()
+    mem = _where(inp)
+    nv = inp.nvband if nvband is None else int(nvband)
+
+    def buf():
+        if mem == "host":
+            return np.zeros(3, dtype=np.complex128)
+        import torch
+        return torch.zeros(3, dtype=torch.complex128, device=inp.wtilde_array.device)
+
+    ach = buf() if want_ach else None
+    asx = buf() if want_asx else None
+    o = make_options(mem, precision, algorithm, inp.wx_band_stride, stream=_stream_handle(inp, stream),
+                     flags=flags, device_status=device_status)
+    st = lib.bgw_gpp_sigma(inp.number_bands, nv, inp.ngpown, inp.ncouls, _ptr(inp.inv_igp_index),
+                           _ptr(inp.indinv), len(inp.indinv), _ptr(inp.wx_array), _ptr(inp.wtilde_array),
+                           _ptr(inp.aqsmtemp), _ptr(inp.aqsntemp), _ptr(inp.I_eps_array), _ptr(inp.vcoul),
+                           _nz(ach), _nz(asx), ctypes.byref(o))
+    _check("bgw_gpp_sigma", st)
+    return ach, asx
 
 
 def noflagOCC_solver_backward(inp: GppInputs, grad_achtemp, *, want_wtilde=True, want_I_eps=True,

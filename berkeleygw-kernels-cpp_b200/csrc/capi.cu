@@ -20,6 +20,10 @@ int gpp_run_host(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *
                  int64_t indinv_len, const double *wx, size_t wx_n, int64_t wx_stride, const double *wt,
                  const double *am, const double *an, const double *ie, const double *vc, double *achtemp_dev);
 
+int gpp_sx_enqueue(CallEnv *env, int64_t nvband, int64_t P, int64_t G, const int32_t *inv, const int32_t *indinv,
+                   int64_t indinv_len, const double *wx, size_t wx_n, int64_t wx_stride, const double2 *wt,
+                   const double2 *am, const double2 *an, const double2 *ie, const double *vc, double *asx_dev);
+
 int gpp_adjoint_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *inv, const int32_t *indinv,
                         int64_t indinv_len, const double *wx, const double2 *wt, const double2 *am,
                         const double2 *an, const double2 *ie, const double *vc, const double2 *gcot,
@@ -116,6 +120,57 @@ extern "C" int bgw_noflagOCC_solver(int64_t number_bands, int64_t ngpown, int64_
   }
   if (env->host) BGW_CUDA_TRY(cudaMemcpyAsync(achtemp, out, 6 * sizeof(double), cudaMemcpyDeviceToHost, env->stream));
   env->prof.flops = 63.0 * (double)nb * (double)P * (double)G;
+  return finish_call(env);
+}
+
+extern "C" int bgw_gpp_sigma(int64_t number_bands, int64_t nvband, int64_t ngpown, int64_t ncouls,
+                             const int32_t *inv_igp_index, const int32_t *indinv, int64_t indinv_len,
+                             const double *wx_array, const double *wtilde_array, const double *aqsmtemp,
+                             const double *aqsntemp, const double *I_eps_array, const double *vcoul,
+                             double *achtemp, double *asxtemp, const bgw_options *opt) {
+  const int64_t nb = number_bands, P = ngpown, G = ncouls;
+  if (nb < 0 || P < 0 || G <= 0 || G > INT32_MAX || nb > INT32_MAX || P > INT32_MAX) return BGW_ERR_INVALID_ARG;
+  if (nvband < 0 || nvband > nb) return BGW_ERR_INVALID_ARG;
+  if (!dims_ok(nb, G) || !dims_ok(P, G) || indinv_len <= 0 || indinv_len > INT32_MAX) return BGW_ERR_INVALID_ARG;
+  if ((!achtemp && !asxtemp) || !vcoul || !indinv) return BGW_ERR_INVALID_ARG;
+  if (P > 0 && (!inv_igp_index || !wtilde_array || !I_eps_array)) return BGW_ERR_INVALID_ARG;
+  if (nb > 0 && P > 0 && (!aqsmtemp || !aqsntemp)) return BGW_ERR_INVALID_ARG;
+  Call c(opt);
+  if (c.st != BGW_OK) return c.st;
+  CallEnv *env = &c.env;
+  const int64_t stride = env->opt.wx_band_stride;
+  if (!wx_array && (nb > 0 || stride == 0)) return BGW_ERR_INVALID_ARG;
+  if (stride != 0 && stride < 3) return BGW_ERR_INVALID_ARG;
+  const size_t wx_n = !wx_array ? 0 : stride == 0 ? 3 : (size_t)(nb > 0 ? (nb - 1) * stride + 3 : 3);
+  // Both sums read the same inputs: stage them once (host memory: copied,
+  // large pageable arrays through the page-locked slots).
+  const void *inv = nullptr, *ind = nullptr, *wx = nullptr, *wt = nullptr, *am = nullptr, *an = nullptr,
+             *ie = nullptr, *vc = nullptr;
+  const size_t pg = (size_t)P * (size_t)G * 16, ng = (size_t)nb * (size_t)G * 16;
+  BGW_TRY(stage_input(env, SLOT_IN0, inv_igp_index, sizeof(int32_t) * (size_t)P, &inv));
+  BGW_TRY(stage_input(env, SLOT_IN1, indinv, sizeof(int32_t) * (size_t)indinv_len, &ind));
+  BGW_TRY(stage_input(env, SLOT_IN2, wx_array, sizeof(double) * wx_n, &wx));
+  BGW_TRY(stage_input(env, SLOT_IN3, wtilde_array, pg, &wt));
+  BGW_TRY(stage_input(env, SLOT_IN4, aqsmtemp, ng, &am));
+  BGW_TRY(stage_input(env, SLOT_IN5, aqsntemp, ng, &an));
+  BGW_TRY(stage_input(env, SLOT_IN6, I_eps_array, pg, &ie));
+  BGW_TRY(stage_input(env, SLOT_IN7, vcoul, sizeof(double) * (size_t)G, &vc));
+  double *out = nullptr;  // achtemp | asxtemp (6 doubles each)
+  BGW_TRY(out_buffer(env, nullptr, 12 * sizeof(double), &out));
+  double *o_ach = env->host ? out : achtemp, *o_asx = env->host ? out + 6 : asxtemp;
+  if (achtemp)
+    BGW_TRY(gpp_enqueue(env, nb, P, G, (const int32_t *)inv, (const int32_t *)ind, indinv_len, (const double *)wx,
+                        stride, (const double2 *)wt, (const double2 *)am, (const double2 *)an, (const double2 *)ie,
+                        (const double *)vc, o_ach));
+  if (asxtemp)
+    BGW_TRY(gpp_sx_enqueue(env, nvband, P, G, (const int32_t *)inv, (const int32_t *)ind, indinv_len,
+                           (const double *)wx, wx_n, stride, (const double2 *)wt, (const double2 *)am,
+                           (const double2 *)an, (const double2 *)ie, (const double *)vc, o_asx));
+  if (env->host) {
+    if (achtemp) BGW_CUDA_TRY(cudaMemcpyAsync(achtemp, o_ach, 6 * sizeof(double), cudaMemcpyDeviceToHost, env->stream));
+    if (asxtemp) BGW_CUDA_TRY(cudaMemcpyAsync(asxtemp, o_asx, 6 * sizeof(double), cudaMemcpyDeviceToHost, env->stream));
+  }
+  env->prof.flops = 63.0 * (double)P * (double)G * ((achtemp ? (double)nb : 0.0) + (asxtemp ? 2.0 * nvband : 0.0));
   return finish_call(env);
 }
 

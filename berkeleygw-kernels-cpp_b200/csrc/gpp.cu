@@ -559,6 +559,49 @@ int gpp_run_host(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *
                             issue, (long long)P);
 }
 
+// ------------------------------------------------- screened exchange (SX) --
+//
+// bgw_gpp_sigma's asxtemp (the GPP model's screened exchange over the
+// occupied bands; not in the reference, which has no flagOCC branch).  With
+// Omega^2 / wtilde = I_eps wtilde[p][igp] (the reference's Coulomb-hole
+// weight) the SX term is -2 sch_store1 I_eps wtilde / (wx^2 - wtilde^2), and
+// by partial fractions wtilde / (wx^2 - wtilde^2) = (1/(wx - wtilde) -
+// 1/(wx + wtilde)) / 2, so
+//   asxtemp(wx) = -( Sigma_occ(wx) + Sigma_occ(-wx) ),
+// Sigma_occ being the Coulomb-hole sum of the plain kernels restricted to the
+// occupied bands.  The two evaluations reuse gpp_enqueue; these kernels negate
+// wx and combine the results.
+namespace {
+__global__ void gpp_negate_kernel(const double *__restrict__ in, double *__restrict__ out, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = -in[i];
+}
+__global__ void gpp_sx_combine_kernel(const double *__restrict__ a, const double *__restrict__ b,
+                                      double *__restrict__ out) {
+  if (threadIdx.x < 6) out[threadIdx.x] = -(a[threadIdx.x] + b[threadIdx.x]);
+}
+}  // namespace
+
+int gpp_sx_enqueue(CallEnv *env, int64_t nvband, int64_t P, int64_t G, const int32_t *inv, const int32_t *indinv,
+                   int64_t indinv_len, const double *wx, size_t wx_n, int64_t wx_stride, const double2 *wt,
+                   const double2 *am, const double2 *an, const double2 *ie, const double *vc, double *asx_dev) {
+  void *tmp = nullptr, *wxn = nullptr;
+  BGW_TRY(ws_reserve(env->ws, SLOT_IN10, sizeof(double) * 12, &tmp));
+  BGW_TRY(ws_reserve(env->ws, SLOT_IN11, sizeof(double) * std::max<size_t>(wx_n, 1), &wxn));
+  double *t_pos = static_cast<double *>(tmp), *t_neg = t_pos + 6;
+  const int g = (int)std::min<size_t>((wx_n + 255) / 256, 1024);
+  gpp_negate_kernel<<<std::max(g, 1), 256, 0, env->stream>>>(wx, static_cast<double *>(wxn), (long long)wx_n);
+  count_launch();
+  BGW_CUDA_TRY(cudaGetLastError());
+  BGW_TRY(gpp_enqueue(env, nvband, P, G, inv, indinv, indinv_len, wx, wx_stride, wt, am, an, ie, vc, t_pos));
+  BGW_TRY(gpp_enqueue(env, nvband, P, G, inv, indinv, indinv_len, static_cast<const double *>(wxn), wx_stride, wt,
+                      am, an, ie, vc, t_neg));
+  gpp_sx_combine_kernel<<<1, 32, 0, env->stream>>>(t_pos, t_neg, asx_dev);
+  count_launch();
+  BGW_CUDA_TRY(cudaGetLastError());
+  return BGW_OK;
+}
+
 // ------------------------------------------------------ no-allocation path --
 //
 // bgw_noflagOCC_solver_noalloc (include/bgw_sigma.h) serves callers that

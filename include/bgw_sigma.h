@@ -186,6 +186,30 @@ int bgw_gpp_batch_info(const bgw_gpp_batch *batch, int32_t *elems_per_thread,
                        int32_t *grid, int64_t *total_items);
 int bgw_gpp_batch_destroy(bgw_gpp_batch *batch);
 
+/* ------------------------------------------ GPP, Coulomb hole + exchange --
+ * No counterpart in the reference, whose GPP solver (GPP/gpp.cpp:307-402)
+ * has no flagOCC branch and no asxtemp output; the screened-exchange part
+ * is specified from the GPP model and its parity is therefore unpinned.
+ *   achtemp (may be NULL): the Coulomb-hole sum of bgw_noflagOCC_solver over
+ *            all number_bands bands (bitwise equal to a device-memory
+ *            bgw_noflagOCC_solver call; host inputs are staged whole here);
+ *   asxtemp (may be NULL): screened exchange of the occupied bands n1 <
+ *            nvband, eps^-1 - 1 = Omega^2 / (w^2 - wtilde^2) with Omega^2 /
+ *            wtilde = I_eps[p][ig] wtilde[p][igp]:
+ *     asxtemp[iw] = - sum_{n1<nvband, p, ig} conj(aqsm[n1][igp]) aqsn[n1][igp]
+ *                   vcoul[igp] wtilde[p][igp] I_eps[p][ig] wtilde[p][ig]
+ *                   / (wx^2 - wtilde[p][ig]^2)
+ *            (bare exchange excluded), evaluated as minus the Coulomb-hole sum
+ *            of the occupied bands at +wx plus the same at -wx (partial
+ *            fractions).  3 complex each.
+ * Inputs as bgw_noflagOCC_solver (memory, precision, algorithm and wx_band_stride
+ * options apply to both sums); 0 <= nvband <= number_bands. */
+int bgw_gpp_sigma(int64_t number_bands, int64_t nvband, int64_t ngpown, int64_t ncouls,
+                  const int32_t *inv_igp_index, const int32_t *indinv, int64_t indinv_len,
+                  const double *wx_array, const double *wtilde_array, const double *aqsmtemp,
+                  const double *aqsntemp, const double *I_eps_array, const double *vcoul,
+                  double *achtemp, double *asxtemp, const bgw_options *opt);
+
 /* --------------------------------------------------- GPP, no allocation --
  * No counterpart in the reference.  A variant of bgw_noflagOCC_solver for
  * callers that cannot allocate GPU memory: code whose device memory is all

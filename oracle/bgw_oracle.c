@@ -125,6 +125,83 @@ int orc_gpp_direct(long nb, long P, long G, const int *inv_igp_index,
   return 0;
 }
 
+/* Screened exchange (SX, the GPP `flagOCC` branch) -- NOT in the reference,
+ * so its parity is unpinned: specified here from the GPP model
+ *   eps^-1_GG'(w) = delta_GG' + Omega^2 / (w^2 - wtilde^2),
+ * with the Coulomb-hole weight the reference uses, Omega^2 / wtilde =
+ * I_eps[p][ig] wtilde[p][igp] (sch_store1 already carries 0.5 conj(aqsm)
+ * aqsn vcoul wtilde[p][igp], gpp.cpp:369-371), for the occupied bands only:
+ *   asxtemp[iw] = - sum_{n1 < nvband} sum_p conj(aqsm[n1][igp]) aqsn[n1][igp]
+ *                 vcoul[igp] wtilde[p][igp]
+ *                 sum_ig I_eps[p][ig] wtilde[p][ig] / (wx^2 - wtilde[p][ig]^2)
+ * (the delta_GG' bare-exchange part is excluded).  Product form, long double
+ * complex division per term; wx[n1 * stride + iw] as in orc_gpp_direct.
+ * factored != 0 (stride 0 only): X(p) = sum_n1 of the band factor first,
+ * O(P G) -- the full-size form. */
+static void sx_term(double wx, const double *wt, const double *ie, ld *qr, ld *qi) {
+  const ld wr = wt[0], wi = wt[1];
+  const ld nr = (ld)ie[0] * wr - (ld)ie[1] * wi, ni = (ld)ie[0] * wi + (ld)ie[1] * wr;  /* I wtilde */
+  const ld dr = (ld)wx * (ld)wx - (wr * wr - wi * wi), di = -2.0L * wr * wi;          /* wx^2 - wtilde^2 */
+  const ld den = dr * dr + di * di;
+  *qr = (nr * dr + ni * di) / den;
+  *qi = (ni * dr - nr * di) / den;
+}
+
+int orc_gpp_sx(long nb, long nvband, long P, long G, const int *inv_igp_index, const int *indinv,
+               long indinv_len, const double *wx, long wx_band_stride, const double *wtilde,
+               const double *aqsm, const double *aqsn, const double *I_eps, const double *vcoul,
+               double *asxtemp, int factored) {
+  if (nb < 0 || nvband < 0 || nvband > nb || P < 0 || G <= 0 || wx_band_stride < 0) return -1;
+  if (factored && wx_band_stride != 0) return -1;
+  long *igp = (long *)malloc(sizeof(long) * (size_t)(P > 0 ? P : 1));
+  ld *part = (ld *)calloc((size_t)(P > 0 ? P : 1) * 6, sizeof(ld));
+  if (!igp || !part) { free(igp); free(part); return -1; }
+  if (resolve_igp(P, G, inv_igp_index, indinv, indinv_len, igp)) {
+    free(igp); free(part); return -1;
+  }
+#pragma omp parallel for schedule(dynamic, 1)
+  for (long p = 0; p < P; ++p) {
+    const long g = igp[p];
+    ld acc[6] = {0, 0, 0, 0, 0, 0};
+    if (factored) {
+      ld xr = 0, xi = 0;  /* X(p) = sum over occupied bands of -2 sch_store1 */
+      for (long n1 = 0; n1 < nvband; ++n1) {
+        ld sr, si;
+        gpp_store1(aqsm + 2 * (n1 * G + g), aqsn + 2 * (n1 * G + g), vcoul[g], wtilde + 2 * (p * G + g), &sr, &si);
+        xr -= 2.0L * sr;
+        xi -= 2.0L * si;
+      }
+      for (long ig = 0; ig < G; ++ig)
+        for (int iw = 0; iw < 3; ++iw) {
+          ld qr, qi;
+          sx_term(wx[iw], wtilde + 2 * (p * G + ig), I_eps + 2 * (p * G + ig), &qr, &qi);
+          acc[2 * iw] += qr * xr - qi * xi;
+          acc[2 * iw + 1] += qr * xi + qi * xr;
+        }
+    } else {
+      for (long n1 = 0; n1 < nvband; ++n1) {
+        ld sr, si;
+        gpp_store1(aqsm + 2 * (n1 * G + g), aqsn + 2 * (n1 * G + g), vcoul[g], wtilde + 2 * (p * G + g), &sr, &si);
+        const ld xr = -2.0L * sr, xi = -2.0L * si;
+        for (long ig = 0; ig < G; ++ig)
+          for (int iw = 0; iw < 3; ++iw) {
+            ld qr, qi;
+            sx_term(wx[n1 * wx_band_stride + iw], wtilde + 2 * (p * G + ig), I_eps + 2 * (p * G + ig), &qr, &qi);
+            acc[2 * iw] += qr * xr - qi * xi;
+            acc[2 * iw + 1] += qr * xi + qi * xr;
+          }
+      }
+    }
+    for (int k = 0; k < 6; ++k) part[6 * p + k] = acc[k];
+  }
+  ld tot[6] = {0, 0, 0, 0, 0, 0};
+  for (long p = 0; p < P; ++p)
+    for (int k = 0; k < 6; ++k) tot[k] += part[6 * p + k];
+  for (int k = 0; k < 6; ++k) asxtemp[k] = (double)tot[k];
+  free(igp); free(part);
+  return 0;
+}
+
 /* Factored evaluation of the same sum for a band-independent wx (the
  * reference's case): nothing inside the ig/iw loop of gpp.cpp:373-390 depends
  * on n1 except sch_store1, so

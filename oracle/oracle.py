@@ -51,6 +51,7 @@ class Oracle:
         lib = ctypes.CDLL(str(path))
         lib.orc_gpp_direct.argtypes = [_L, _L, _L, _P, _P, _L, _P, _L, _P, _P, _P, _P, _P, _P]
         lib.orc_gpp_factored.argtypes = [_L, _L, _L, _P, _P, _L, _P, _P, _P, _P, _P, _P, _P]
+        lib.orc_gpp_sx.argtypes = [_L, _L, _L, _L, _P, _P, _L, _P, _L, _P, _P, _P, _P, _P, _P, ctypes.c_int]
         lib.orc_compute_fact.argtypes = [_D, ctypes.c_int, _P, ctypes.c_int, ctypes.c_int,
                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(_D), ctypes.POINTER(_D)]
         lib.orc_compute_fact.restype = None
@@ -74,6 +75,19 @@ class Oracle:
             st = self.lib.orc_gpp_direct(g.number_bands, g.ngpown, g.ncouls, _p(g.inv_igp_index), _p(g.indinv),
                                          len(g.indinv), _p(g.wx_array), g.wx_band_stride, _p(g.wtilde_array),
                                          _p(g.aqsmtemp), _p(g.aqsntemp), _p(g.I_eps_array), _p(g.vcoul), _p(out))
+        if st != 0:
+            raise ValueError("oracle rejected the GPP inputs")
+        return out
+
+    def gpp_sx(self, g, nvband: int | None = None, factored: bool = False) -> np.ndarray:
+        """Screened exchange of the occupied bands (asxtemp), specified from
+        the GPP model (not in the reference: parity unpinned)."""
+        nv = g.nvband if nvband is None else nvband
+        out = np.zeros(3, dtype=np.complex128)
+        st = self.lib.orc_gpp_sx(g.number_bands, nv, g.ngpown, g.ncouls, _p(g.inv_igp_index), _p(g.indinv),
+                                 len(g.indinv), _p(g.wx_array), g.wx_band_stride if not factored else 0,
+                                 _p(g.wtilde_array), _p(g.aqsmtemp), _p(g.aqsntemp), _p(g.I_eps_array), _p(g.vcoul),
+                                 _p(out), int(factored))
         if st != 0:
             raise ValueError("oracle rejected the GPP inputs")
         return out

@@ -119,3 +119,39 @@ def test_ff_per_iw_oracle_pinned_at_iw1(golden, oracle, name):
     asx, cor = oracle.asx(f, per_iw=True), oracle.cor(f, per_iw=True)
     assert rel_err(asx[1], l2c(ref["asx"])[1]) < 1e-14
     assert rel_err(cor[1], l2c(ref["cor"])[1]) < 1e-14
+
+
+# ------------------------------------------------ GPP screened exchange --
+# Specified from the GPP model (the reference has no flagOCC branch): parity
+# unpinned; the oracle's product form is checked against the partial-fraction
+# identity over the reference-pinned Coulomb-hole sum and a closed form.
+
+def _occupied(g, nv, negate):
+    import dataclasses
+    stride = g.wx_band_stride
+    wx = g.wx_array[: (nv - 1) * stride + 3] if stride and nv else g.wx_array
+    return dataclasses.replace(g, number_bands=nv, aqsmtemp=g.aqsmtemp[:nv], aqsntemp=g.aqsntemp[:nv],
+                               wx_array=np.ascontiguousarray(-wx if negate else wx))
+
+
+@pytest.mark.parametrize("per_band", [False, True])
+@pytest.mark.parametrize("nv", [1, 3, 7])
+def test_gpp_sx_partial_fractions(oracle, nv, per_band):
+    g = I.gpp_seeded(9, nv, 400, 8, seed=40 + nv, wx_per_band=per_band)
+    sx = oracle.gpp_sx(g)
+    pf = -(oracle.gpp(_occupied(g, nv, False)) + oracle.gpp(_occupied(g, nv, True)))
+    assert rel_err(sx, pf) < 1e-14
+    if not per_band:
+        assert rel_err(oracle.gpp_sx(g, factored=True), sx) < 1e-13
+
+
+def test_gpp_sx_uniform_closed_form(oracle):
+    # gpp_uniform: s I_eps = 0.125i, wtilde = 0.5 + 0.5i, so each occupied
+    # (band, p, ig) term is -0.125i (1/(wx - wt) - 1/(wx + wt)).
+    nb, nv, G, npg = 8, 3, 400, 20
+    g = I.gpp_uniform(nb, nv, G, npg)
+    wt = 0.5 + 0.5j
+    n = nv * (G // npg) * G
+    kat = np.array([-n * 0.125j * (1 / (w - wt) - 1 / (w + wt)) for w in (3.0, 4.0, 5.0)])
+    assert rel_err(oracle.gpp_sx(g), kat) < 1e-13
+    assert np.all(oracle.gpp_sx(g, nvband=0) == 0)
