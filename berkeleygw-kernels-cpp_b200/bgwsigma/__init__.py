@@ -54,7 +54,8 @@ class BgwError(RuntimeError):
 class Options(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_int32), ("memory", ctypes.c_int32), ("precision", ctypes.c_int32),
                 ("gpp_algorithm", ctypes.c_int32), ("wx_band_stride", ctypes.c_int64), ("device", ctypes.c_int32),
-                ("flags", ctypes.c_int32), ("stream", ctypes.c_void_p), ("device_status", ctypes.c_void_p)]
+                ("flags", ctypes.c_int32), ("stream", ctypes.c_void_p), ("device_status", ctypes.c_void_p),
+                ("pole_guard", ctypes.c_double)]
 
 
 class Profile(ctypes.Structure):
@@ -180,7 +181,7 @@ def _where(inp) -> str:
 
 
 def make_options(memory="host", precision="fp64", algorithm="auto", wx_band_stride=0, device=-1, stream=None,
-                 flags=0, device_status=None) -> Options:
+                 flags=0, device_status=None, pole_guard=0.0) -> Options:
     o = Options()
     load().bgw_options_init(ctypes.byref(o))
     o.memory = MEMORY[memory]
@@ -191,6 +192,7 @@ def make_options(memory="host", precision="fp64", algorithm="auto", wx_band_stri
     o.flags = int(flags)
     o.stream = stream
     o.device_status = device_status
+    o.pole_guard = float(pole_guard)
     return o
 
 
@@ -201,9 +203,10 @@ def _stream_handle(inp, stream):
 
 
 def noflagOCC_solver(inp: GppInputs, *, precision="fp64", algorithm="auto", stream=None, out=None,
-                     flags=0, device_status=None) -> np.ndarray:
+                     flags=0, device_status=None, pole_guard=0.0) -> np.ndarray:
     """achtemp[3] (complex128).  `out`: optional preallocated output (host
-    numpy complex128[3] or a CUDA tensor for device-resident inputs)."""
+    numpy complex128[3] or a CUDA tensor for device-resident inputs).
+    `pole_guard` > 0: terms with |wx - wtilde| below it contribute zero."""
     lib = load()
     mem = _where(inp)
     if out is None:
@@ -213,7 +216,7 @@ def noflagOCC_solver(inp: GppInputs, *, precision="fp64", algorithm="auto", stre
             import torch
             out = torch.zeros(3, dtype=torch.complex128, device=inp.wtilde_array.device)
     o = make_options(mem, precision, algorithm, inp.wx_band_stride, stream=_stream_handle(inp, stream),
-                     flags=flags, device_status=device_status)
+                     flags=flags, device_status=device_status, pole_guard=pole_guard)
     st = lib.bgw_noflagOCC_solver(inp.number_bands, inp.ngpown, inp.ncouls, _ptr(inp.inv_igp_index),
                                   _ptr(inp.indinv), len(inp.indinv), _ptr(inp.wx_array), _ptr(inp.wtilde_array),
                                   _ptr(inp.aqsmtemp), _ptr(inp.aqsntemp), _ptr(inp.I_eps_array), _ptr(inp.vcoul),
@@ -223,7 +226,7 @@ def noflagOCC_solver(inp: GppInputs, *, precision="fp64", algorithm="auto", stre
 
 
 def gpp_sigma(inp: GppInputs, nvband=None, *, want_ach=True, want_asx=True, precision="fp64", algorithm="auto",
-              stream=None, flags=0, device_status=None):
+              stream=None, flags=0, device_status=None, pole_guard=0.0):
     """(achtemp[3], asxtemp[3]) complex128: the Coulomb-hole sum over all
     bands and the GPP screened exchange of the occupied bands n1 < nvband
     (default: inp.nvband).  A result not asked for is None."""
@@ -240,7 +243,7 @@ def gpp_sigma(inp: GppInputs, nvband=None, *, want_ach=True, want_asx=True, prec
     ach = buf() if want_ach else None
     asx = buf() if want_asx else None
     o = make_options(mem, precision, algorithm, inp.wx_band_stride, stream=_stream_handle(inp, stream),
-                     flags=flags, device_status=device_status)
+                     flags=flags, device_status=device_status, pole_guard=pole_guard)
     st = lib.bgw_gpp_sigma(inp.number_bands, nv, inp.ngpown, inp.ncouls, _ptr(inp.inv_igp_index),
                            _ptr(inp.indinv), len(inp.indinv), _ptr(inp.wx_array), _ptr(inp.wtilde_array),
                            _ptr(inp.aqsmtemp), _ptr(inp.aqsntemp), _ptr(inp.I_eps_array), _ptr(inp.vcoul),
@@ -250,7 +253,7 @@ def gpp_sigma(inp: GppInputs, nvband=None, *, want_ach=True, want_asx=True, prec
 
 
 def noflagOCC_solver_backward(inp: GppInputs, grad_achtemp, *, want_wtilde=True, want_I_eps=True,
-                              want_domega=True, stream=None, flags=0):
+                              want_domega=True, stream=None, flags=0, pole_guard=0.0):
     """Adjoint of noflagOCC_solver.  grad_achtemp: 3 complex cotangents
     (dL/dRe + i dL/dIm of each achtemp entry).  Returns (grad_wtilde,
     grad_I_eps, dachtemp_domega) -- complex arrays [ngpown][ncouls],
@@ -270,7 +273,8 @@ def noflagOCC_solver_backward(inp: GppInputs, grad_achtemp, *, want_wtilde=True,
         gw = torch.zeros((P, G), dtype=torch.complex128, device=dev) if want_wtilde else None
         gi = torch.zeros((P, G), dtype=torch.complex128, device=dev) if want_I_eps else None
         dw = torch.zeros(3, dtype=torch.complex128, device=dev) if want_domega else None
-    o = make_options(mem, "fp64", "auto", inp.wx_band_stride, stream=_stream_handle(inp, stream), flags=flags)
+    o = make_options(mem, "fp64", "auto", inp.wx_band_stride, stream=_stream_handle(inp, stream), flags=flags,
+                     pole_guard=pole_guard)
     st = lib.bgw_noflagOCC_solver_backward(inp.number_bands, P, G, _ptr(inp.inv_igp_index), _ptr(inp.indinv),
                                            len(inp.indinv), _ptr(inp.wx_array), _ptr(inp.wtilde_array),
                                            _ptr(inp.aqsmtemp), _ptr(inp.aqsntemp), _ptr(inp.I_eps_array),
@@ -283,7 +287,7 @@ class GppBatch:
     """Many device-resident GPP instances in one persistent launch (a CUDA
     graph replayed by execute()).  `instances`: GppInputs with CUDA tensors."""
 
-    def __init__(self, instances, *, precision="fp64", algorithm="auto", stream=None):
+    def __init__(self, instances, *, precision="fp64", algorithm="auto", stream=None, pole_guard=0.0):
         import torch
         lib = load()
         self.instances = list(instances)
@@ -299,7 +303,7 @@ class GppBatch:
                                  self.out[k].data_ptr())
         self._arr = arr
         o = make_options("device", precision, algorithm, stream=_stream_handle(None, stream),
-                         device=dev.index if dev.index is not None else -1)
+                         device=dev.index if dev.index is not None else -1, pole_guard=pole_guard)
         h = _P()
         _check("bgw_gpp_batch_create", lib.bgw_gpp_batch_create(arr, len(self.instances), ctypes.byref(o),
                                                                 ctypes.byref(h)))

@@ -192,6 +192,7 @@ extern "C" int bgw_noflagOCC_solver_backward(int64_t number_bands, int64_t ngpow
   if (c.st != BGW_OK) return c.st;
   CallEnv *env = &c.env;
   if (env->opt.wx_band_stride != 0) return BGW_ERR_UNSUPPORTED;  // factored adjoint only
+  if (env->opt.pole_guard > 0.0) return BGW_ERR_UNSUPPORTED;      // no near-pole cut-off
   const void *inv = nullptr, *ind = nullptr, *wx = nullptr, *wt = nullptr, *am = nullptr, *an = nullptr,
              *ie = nullptr, *vc = nullptr, *gc = nullptr;
   const size_t pg = (size_t)P * (size_t)G * 16, ng = (size_t)nb * (size_t)G * 16;

@@ -114,6 +114,7 @@ struct BandSmem {
   double4 wx[2][BCH];
   unsigned long long bar[2];
   double red[(kThreads / 32) * 6];
+  double xr_lo[kThreads / 32], xr_hi[kThreads / 32];  // MIXED: chunk frequency range
 };
 
 // Every band reads its own frequencies from the staged wx4 rows (for the
@@ -122,11 +123,16 @@ struct BandSmem {
 // MIXED: quotients in FP32 (rcp.approx.ftz.f32), the per-band products with
 // sch_store1 and the accumulation over bands in FP64 with TwoSum
 // compensation.
-template <int BCH, bool MIXED>
+// GUARD (FP64): near-pole cut-off, terms with |wdiff|^2 < guard2 contribute
+// zero.  MIXED: elements near the chunk's frequencies take an FP64 path
+// (near_elems / near_sweep), which also applies the cut-off (guard_d =
+// sqrt(guard2)); GUARD is not used.
+template <int BCH, bool MIXED, bool GUARD>
 __global__ void __launch_bounds__(kThreads, MIXED ? 1 : 2)
     gpp_bandloop_kernel(int nb, int G, long long items, int nchunks_g, const double2 *__restrict__ wtilde,
                         const double2 *__restrict__ ieps, const double2 *__restrict__ st,
-                        const double4 *__restrict__ wx4, double *__restrict__ partials, int *status) {
+                        const double4 *__restrict__ wx4, double *__restrict__ partials, int *status,
+                        double guard2, double guard_d) {
   constexpr int kE = BandCfg<MIXED>::kE;
   constexpr int kCH = BandCfg<MIXED>::kCH;
   using T = typename std::conditional<MIXED, float, double>::type;
@@ -190,7 +196,16 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 1 : 2)
 
     Elem<T> e[kE];
     load_elems<T, kE>(e, sm.wt[buf], sm.ie[buf], nvalid, kThreads, tid);
-    band_sweep<MIXED, kE>(e, sm.wx[buf], sm.st[buf], nbv, acc_r, acc_i, lo_r, lo_i);
+    uint32_t near = 0;
+    if constexpr (MIXED) {
+      const double2 xr = chunk_wx_range<kThreads>(sm.wx[buf], nbv, sm.xr_lo, sm.xr_hi);
+      near = near_elems<kE>(e, sm.wt[buf], nvalid, kThreads, tid, xr, guard_d);
+    }
+    band_sweep<MIXED, kE, GUARD && !MIXED>(e, sm.wx[buf], sm.st[buf], nbv, acc_r, acc_i, lo_r, lo_i, guard2);
+    if constexpr (MIXED) {
+      if (near) near_sweep(near, sm.wt[buf], sm.ie[buf], kThreads, tid, sm.wx[buf], sm.st[buf], nbv, guard2, acc_r,
+                           acc_i, lo_r, lo_i);
+    }
     __syncthreads();  // buffer `buf` is free for step j + 2
   }
   if (!ok && tid == 0) {
@@ -213,10 +228,12 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 1 : 2)
 // Band-independent wx: achtemp[iw] = sum_p S(p) * sum_ig q(p, ig, iw).
 // HBM-bound stream over wtilde / I_eps with 128-bit loads; one item =
 // (p, chunk of kChunk ig); per-thread sums are folded per CTA.
+// GUARD: near-pole cut-off as in the band loop.
+template <bool GUARD>
 __global__ void __launch_bounds__(kThreads)
     gpp_factored_kernel(int G, long long items, int nchunks_g, const double2 *__restrict__ wtilde,
                         const double2 *__restrict__ ieps, const double2 *__restrict__ S,
-                        const double *__restrict__ wx3, double *__restrict__ partials) {
+                        const double *__restrict__ wx3, double *__restrict__ partials, double guard2) {
   __shared__ double red[(kThreads / 32) * 6];
   const int tid = threadIdx.x;
   const double x[3] = {wx3[0], wx3[1], wx3[2]};
@@ -243,7 +260,9 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
       for (int iw = 0; iw < 3; ++iw) {
         const double dr = x[iw] - w[k].x;
-        const double r = rcp_refined(fma(dr, dr, wi2));
+        const double den = fma(dr, dr, wi2);
+        double r = rcp_refined(den);
+        if constexpr (GUARD) r = den < guard2 ? 0.0 : r;
         tr[iw] = fma(fma(dr, v[k].x, a), r, tr[iw]);
         ti[iw] = fma(fma(dr, v[k].y, b), r, ti[iw]);
       }
@@ -265,11 +284,11 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-template <int BCH, bool MIXED>
+template <int BCH, bool MIXED, bool GUARD = false>
 int bandloop_per_sm(int *per_sm) {
   using Smem = BandSmem<BCH, MIXED>;
   const size_t smem = sizeof(Smem);
-  auto kfn = gpp_bandloop_kernel<BCH, MIXED>;
+  auto kfn = gpp_bandloop_kernel<BCH, MIXED, GUARD>;
   BGW_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   BGW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kfn, kThreads, smem));
   return *per_sm >= 1 ? BGW_OK : BGW_ERR_UNSUPPORTED;
@@ -277,10 +296,10 @@ int bandloop_per_sm(int *per_sm) {
 
 // Launches the band loop over rows [0, P) of the given (already offset)
 // arrays; writes `grid` partials (6 doubles each) starting at `partials`.
-template <int BCH, bool MIXED>
+template <int BCH, bool MIXED, bool GUARD>
 int launch_bandloop(cudaStream_t stream, int max_grid, int nb, int G, const double2 *wt, const double2 *ie,
                     const double2 *st, const double4 *wx4, int64_t P, double *partials, int *grid_out,
-                    int *status) {
+                    int *status, double guard2, double guard_d) {
   using Smem = BandSmem<BCH, MIXED>;
   const size_t smem = sizeof(Smem);
   const int nchunks_g = (int)((G + BandCfg<MIXED>::kCH - 1) / BandCfg<MIXED>::kCH);
@@ -288,8 +307,9 @@ int launch_bandloop(cudaStream_t stream, int max_grid, int nb, int G, const doub
   long long grid = std::min<long long>(items, (long long)max_grid);
   if (grid < 1) grid = 1;
   *grid_out = (int)grid;
-  gpp_bandloop_kernel<BCH, MIXED><<<(int)grid, kThreads, smem, stream>>>(nb, G, items, nchunks_g, wt, ie, st, wx4,
-                                                                          partials, status);
+  gpp_bandloop_kernel<BCH, MIXED, GUARD><<<(int)grid, kThreads, smem, stream>>>(nb, G, items, nchunks_g, wt, ie, st,
+                                                                                 wx4, partials, status, guard2,
+                                                                                 guard_d);
   count_launch();
   BGW_CUDA_TRY(cudaGetLastError());
   return BGW_OK;
@@ -326,6 +346,8 @@ int gpp_enqueue_chunks(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int
   if (factored && env->opt.precision == BGW_PRECISION_MIXED) return BGW_ERR_UNSUPPORTED;
   if (factored && wx_stride != 0) return BGW_ERR_UNSUPPORTED;  // needs a band-independent wx
   const bool mixed = env->opt.precision == BGW_PRECISION_MIXED;
+  const bool guard = env->opt.pole_guard > 0.0;
+  const double guard2 = env->opt.pole_guard * env->opt.pole_guard;
   auto prep_grid_for = [&](int64_t rows) {
     return (int)std::max<long long>(1, std::min<long long>((rows + 7) / 8, (long long)ws->sm_count * 16));
   };
@@ -336,8 +358,10 @@ int gpp_enqueue_chunks(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int
     per_launch = ws->sm_count * 8;
   } else {
     int per_sm = 0;
-    if (mixed) BGW_TRY((bandloop_per_sm<256, true>(&per_sm)));
-    else BGW_TRY((bandloop_per_sm<256, false>(&per_sm)));
+    // Also sets the launched instantiation's shared-memory limit.
+    if (mixed) BGW_TRY((bandloop_per_sm<256, true, false>(&per_sm)));
+    else if (guard) BGW_TRY((bandloop_per_sm<256, false, true>(&per_sm)));
+    else BGW_TRY((bandloop_per_sm<256, false, false>(&per_sm)));
     per_launch = ws->sm_count * per_sm;
   }
   void *partials_v = nullptr, *tab = nullptr, *wx4 = nullptr;
@@ -375,7 +399,12 @@ int gpp_enqueue_chunks(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int
       const long long items = (long long)rows * nchunks_g;
       const int grid = (int)std::min<long long>(std::max<long long>(items, 1), (long long)per_launch);
       if (c == 0) BGW_TRY(prof_mark(env, 1));
-      gpp_factored_kernel<<<grid, kThreads, 0, stream>>>((int)G, items, nchunks_g, wt_c, ie_c, S_c, wx, part_c);
+      if (guard)
+        gpp_factored_kernel<true><<<grid, kThreads, 0, stream>>>((int)G, items, nchunks_g, wt_c, ie_c, S_c, wx,
+                                                                 part_c, guard2);
+      else
+        gpp_factored_kernel<false><<<grid, kThreads, 0, stream>>>((int)G, items, nchunks_g, wt_c, ie_c, S_c, wx,
+                                                                  part_c, 0.0);
       count_launch();
       BGW_CUDA_TRY(cudaGetLastError());
       total += grid;
@@ -388,12 +417,17 @@ int gpp_enqueue_chunks(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int
       BGW_CUDA_TRY(cudaGetLastError());
       if (c == 0) BGW_TRY(prof_mark(env, 1));
       int grid = 0;
+      const double4 *w4 = (const double4 *)wx4;
+      const double gd = env->opt.pole_guard;
       if (mixed) {
-        BGW_TRY((launch_bandloop<256, true>(stream, per_launch, (int)nb, (int)G, wt_c, ie_c, st_c,
-                                            (const double4 *)wx4, rows, part_c, &grid, env->d_status)));
+        BGW_TRY((launch_bandloop<256, true, false>(stream, per_launch, (int)nb, (int)G, wt_c, ie_c, st_c, w4, rows,
+                                                   part_c, &grid, env->d_status, guard2, gd)));
+      } else if (guard) {
+        BGW_TRY((launch_bandloop<256, false, true>(stream, per_launch, (int)nb, (int)G, wt_c, ie_c, st_c, w4, rows,
+                                                   part_c, &grid, env->d_status, guard2, gd)));
       } else {
-        BGW_TRY((launch_bandloop<256, false>(stream, per_launch, (int)nb, (int)G, wt_c, ie_c, st_c,
-                                             (const double4 *)wx4, rows, part_c, &grid, env->d_status)));
+        BGW_TRY((launch_bandloop<256, false, false>(stream, per_launch, (int)nb, (int)G, wt_c, ie_c, st_c, w4, rows,
+                                                    part_c, &grid, env->d_status, 0.0, 0.0)));
       }
       total += grid;
     }
@@ -700,10 +734,10 @@ extern "C" int bgw_noflagOCC_solver_noalloc(int64_t number_bands, int64_t ngpown
   BGW_CUDA_TRY(cudaGetLastError());
   int grid = (int)std::min<long long>(std::max<long long>(items, 1), (long long)sms * 8);
   grid = std::min(grid, kNoAllocMaxGrid);
-  gpp_factored_kernel<<<grid, kThreads, 0, s>>>((int)G, items, nchunks_g,
+  gpp_factored_kernel<false><<<grid, kThreads, 0, s>>>((int)G, items, nchunks_g,
                                                 reinterpret_cast<const double2 *>(wtilde_array),
                                                 reinterpret_cast<const double2 *>(I_eps_array), S, wx_array,
-                                                partials);
+                                                partials, 0.0);
   count_launch();
   BGW_CUDA_TRY(cudaGetLastError());
   reduce_partials_kernel<6><<<1, 256, 0, s>>>(partials, grid, achtemp);

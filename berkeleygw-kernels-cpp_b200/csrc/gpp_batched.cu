@@ -120,6 +120,7 @@ struct BatchSmem {
   double4 wx[2][BCH];
   unsigned long long bar[2];
   double red[(kBThreads / 32) * 6];
+  double xr_lo[kBThreads / 32], xr_hi[kBThreads / 32];  // MIXED: chunk frequency range
 };
 
 // Flushes the running sums of instance slot `seg` of this CTA.
@@ -213,7 +214,17 @@ __global__ void __launch_bounds__(kBThreads, (MIXED && KE == 8) ? 1 : 2)
     const int nbv = max(0, min(BCH, I.nb - cur.c * BCH));
     Elem<T> e[KE];
     load_elems<T, KE>(e, sm.wt[buf], sm.ie[buf], nvalid, kBThreads, tid);
+    // MIXED: elements near the chunk's frequencies are summed in FP64.
+    uint32_t near = 0;
+    if constexpr (MIXED) {
+      const double2 xr = chunk_wx_range<kBThreads>(sm.wx[buf], nbv, sm.xr_lo, sm.xr_hi);
+      near = near_elems<KE>(e, sm.wt[buf], nvalid, kBThreads, tid, xr, 0.0);
+    }
     band_sweep<MIXED, KE>(e, sm.wx[buf], sm.st[buf], nbv, acc_r, acc_i, lo_r, lo_i);
+    if constexpr (MIXED) {
+      if (near) near_sweep(near, sm.wt[buf], sm.ie[buf], kBThreads, tid, sm.wx[buf], sm.st[buf], nbv, 0.0, acc_r,
+                           acc_i, lo_r, lo_i);
+    }
     __syncthreads();  // buffer `buf` is free for step s + 2
     if (!more || nx.i != cur.i) flush(acc_r, acc_i, lo_r, lo_i, sm.red, partials, max_seg, cur.i - inst_lo);
     if (!more) break;
@@ -504,6 +515,7 @@ extern "C" int bgw_gpp_batch_create(const bgw_gpp_instance *instances, int64_t n
   BGW_TRY(begin_call(opt, &env));
   if (env.host) return BGW_ERR_INVALID_ARG;  // device-resident instances only
   if (env.opt.flags & (BGW_FLAG_ASYNC | BGW_FLAG_PROFILE)) return BGW_ERR_INVALID_ARG;
+  if (env.opt.pole_guard > 0.0) return BGW_ERR_UNSUPPORTED;  // near-pole cut-off: single calls only
   const bool mixed = env.opt.precision == BGW_PRECISION_MIXED;
   // Factored only when every wx is band-independent (and FP64).
   bool all_shared = true;
@@ -743,8 +755,10 @@ extern "C" int bgw_gpp_batch_execute(bgw_gpp_batch *B, const bgw_options *opt) {
   bgw_options o;
   bgw_options_init(&o);
   if (opt) {
-    if (opt->struct_size < (int32_t)sizeof(bgw_options)) return BGW_ERR_INVALID_ARG;
-    o = *opt;
+    if (opt->struct_size < (int32_t)(offsetof(bgw_options, device_status) + sizeof(int32_t *)))
+      return BGW_ERR_INVALID_ARG;
+    std::memcpy(&o, opt, std::min<size_t>((size_t)opt->struct_size, sizeof(o)));
+    o.struct_size = (int32_t)sizeof(o);
   }
   if ((o.flags & BGW_FLAG_ASYNC) && !o.device_status) return BGW_ERR_INVALID_ARG;
   BGW_CUDA_TRY(cudaSetDevice(B->device));

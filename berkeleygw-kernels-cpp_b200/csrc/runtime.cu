@@ -1,6 +1,7 @@
 // runtime.cu -- options, per-device workspace cache, host<->device staging
 // and status handling shared by every libbgwsigma entry point.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -124,7 +125,10 @@ int begin_call(const bgw_options *user, CallEnv *env) {
   if (user) {
     if (user->struct_size < (int32_t)offsetof(bgw_options, device_status) + (int32_t)sizeof(int32_t *))
       return BGW_ERR_INVALID_ARG;
-    std::memcpy(&env->opt, user, sizeof(bgw_options));
+    // A caller built against a shorter bgw_options keeps the defaults of
+    // the fields it does not have.
+    std::memcpy(&env->opt, user, std::min<size_t>((size_t)user->struct_size, sizeof(bgw_options)));
+    env->opt.struct_size = (int32_t)sizeof(bgw_options);
   }
   const bgw_options &o = env->opt;
   if (o.memory != BGW_MEMORY_HOST && o.memory != BGW_MEMORY_DEVICE) return BGW_ERR_INVALID_ARG;
@@ -132,6 +136,7 @@ int begin_call(const bgw_options *user, CallEnv *env) {
   if (o.gpp_algorithm != BGW_GPP_BANDLOOP && o.gpp_algorithm != BGW_GPP_FACTORED && o.gpp_algorithm != BGW_GPP_AUTO)
     return BGW_ERR_INVALID_ARG;
   if (o.wx_band_stride < 0) return BGW_ERR_INVALID_ARG;
+  if (!(o.pole_guard >= 0.0) || !std::isfinite(o.pole_guard)) return BGW_ERR_INVALID_ARG;
   if ((o.flags & BGW_FLAG_ASYNC) && (o.memory != BGW_MEMORY_DEVICE || o.device_status == nullptr))
     return BGW_ERR_INVALID_ARG;
   if ((o.flags & BGW_FLAG_PROFILE) && (o.flags & BGW_FLAG_ASYNC)) return BGW_ERR_INVALID_ARG;
@@ -269,6 +274,7 @@ void bgw_options_init(bgw_options *opt) {
   opt->flags = 0;
   opt->stream = nullptr;
   opt->device_status = nullptr;
+  opt->pole_guard = 0.0;
 }
 
 const char *bgw_status_string(int status) {

@@ -89,7 +89,20 @@ typedef struct bgw_options {
   int32_t flags;           /* BGW_FLAG_*                                    */
   void *stream;            /* cudaStream_t; NULL = legacy default stream    */
   int32_t *device_status;  /* device int written with BGW_FLAG_ASYNC        */
+  double pole_guard;       /* GPP near-pole guard delta >= 0; 0 = off       */
 } bgw_options;
+/* pole_guard (GPP sums only; not in the reference, which has no guard and
+ * only clamps wx >= 1e-6, GPP/gpp.cpp:273-274): with delta > 0 every
+ * (band, G', G, frequency) term whose |wdiff|^2 = |wx - wtilde|^2 is below
+ * delta^2 contributes zero -- the term's pole is excluded from the sum
+ * (principal-value cut-off) instead of growing like 1/|wdiff|.  The test is
+ * made on the |wdiff|^2 the kernel computes (FP64, or FP32 with
+ * BGW_PRECISION_MIXED).  In bgw_gpp_sigma's asxtemp the cut applies to each
+ * of the two partial fractions 1/(wx - wtilde) and 1/(-wx - wtilde).
+ * Supported by bgw_noflagOCC_solver and bgw_gpp_sigma; the adjoint and the
+ * batched calls return BGW_ERR_UNSUPPORTED for delta > 0; the FF calls
+ * ignore it.  Callers compiled against an older, shorter bgw_options (a
+ * smaller struct_size) get delta = 0. */
 
 /* Fills *opt with the defaults (host memory, FP64, AUTO, stride 0,
  * current device, default stream, synchronous). */

@@ -66,12 +66,24 @@ static void gpp_store1(const double *am, const double *an, double vc,
   *si = r * ci + i * cr;
 }
 
+/* Near-pole guard (not in the reference, which has none; specified from
+ * first principles): with delta > 0 a pole term 1/(w - wtilde) whose
+ * |w - wtilde|^2 is below delta^2 is left out of the sum.  0 (the default)
+ * keeps every term, as the reference does.  Set by orc_set_pole_guard; read
+ * by gpp_quot and sx_term. */
+static ld g_pole_guard2 = 0.0L;
+
+void orc_set_pole_guard(double delta) { g_pole_guard2 = (ld)delta * (ld)delta; }
+
+static int guarded(ld dr, ld di) { return g_pole_guard2 > 0.0L && dr * dr + di * di < g_pole_guard2; }
+
 /* One (my_igp, ig, iw) quotient of gpp.cpp:374-380 without sch_store1:
  *   conj(wdiff) / |wdiff|^2 * I_eps,  wdiff = wx - wtilde. */
 static void gpp_quot(double wx, const double *wt, const double *ie, ld *qr,
                      ld *qi) {
   ld dr = (ld)wx - (ld)wt[0];
   ld di = -(ld)wt[1];
+  if (guarded(dr, di)) { *qr = 0.0L; *qi = 0.0L; return; }
   ld rcp = 1.0L / (dr * dr + di * di);
   ld cr = dr * rcp, ci = -di * rcp;      /* conj(wdiff) * rcp */
   ld er = ie[0], ei = ie[1];
@@ -140,6 +152,22 @@ int orc_gpp_direct(long nb, long P, long G, const int *inv_igp_index,
  * O(P G) -- the full-size form. */
 static void sx_term(double wx, const double *wt, const double *ie, ld *qr, ld *qi) {
   const ld wr = wt[0], wi = wt[1];
+  /* With the guard on, a pole of the product form within delta of wx
+   * (wtilde = wx) or of -wx (wtilde = -wx) drops that pole's partial
+   * fraction: I wtilde / (wx^2 - wtilde^2) = (I/2) (1/(wx - wtilde) -
+   * 1/(wx + wtilde)). */
+  const int gm = guarded((ld)wx - wr, -wi), gp = guarded((ld)wx + wr, wi);
+  if (gm || gp) {
+    *qr = 0.0L; *qi = 0.0L;
+    if (gm && gp) return;
+    const ld sgn = gm ? -0.5L : 0.5L;                       /* keep -1/(wx+wt) or +1/(wx-wt) */
+    const ld dr = gm ? (ld)wx + wr : (ld)wx - wr, di = gm ? wi : -wi;
+    const ld den = dr * dr + di * di;
+    const ld cr = sgn * dr / den, ci = -sgn * di / den;     /* sgn / (dr + i di) */
+    *qr = cr * (ld)ie[0] - ci * (ld)ie[1];
+    *qi = cr * (ld)ie[1] + ci * (ld)ie[0];
+    return;
+  }
   const ld nr = (ld)ie[0] * wr - (ld)ie[1] * wi, ni = (ld)ie[0] * wi + (ld)ie[1] * wr;  /* I wtilde */
   const ld dr = (ld)wx * (ld)wx - (wr * wr - wi * wi), di = -2.0L * wr * wi;          /* wx^2 - wtilde^2 */
   const ld den = dr * dr + di * di;

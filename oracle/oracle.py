@@ -52,6 +52,8 @@ class Oracle:
         lib.orc_gpp_direct.argtypes = [_L, _L, _L, _P, _P, _L, _P, _L, _P, _P, _P, _P, _P, _P]
         lib.orc_gpp_factored.argtypes = [_L, _L, _L, _P, _P, _L, _P, _P, _P, _P, _P, _P, _P]
         lib.orc_gpp_sx.argtypes = [_L, _L, _L, _L, _P, _P, _L, _P, _L, _P, _P, _P, _P, _P, _P, ctypes.c_int]
+        lib.orc_set_pole_guard.argtypes = [_D]
+        lib.orc_set_pole_guard.restype = None
         lib.orc_compute_fact.argtypes = [_D, ctypes.c_int, _P, ctypes.c_int, ctypes.c_int,
                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(_D), ctypes.POINTER(_D)]
         lib.orc_compute_fact.restype = None
@@ -64,7 +66,17 @@ class Oracle:
         lib.orc_ff_cor_iw.argtypes = lib.orc_ff_cor.argtypes
         self.lib = lib
 
-    def gpp(self, g, factored: bool = False) -> np.ndarray:
+    def _guarded(self, pole_guard, fn):
+        """Runs fn() with the oracle's near-pole guard set to pole_guard."""
+        self.lib.orc_set_pole_guard(float(pole_guard))
+        try:
+            return fn()
+        finally:
+            self.lib.orc_set_pole_guard(0.0)
+
+    def gpp(self, g, factored: bool = False, pole_guard: float = 0.0) -> np.ndarray:
+        if pole_guard:
+            return self._guarded(pole_guard, lambda: self.gpp(g, factored))
         out = np.zeros(3, dtype=np.complex128)
         if factored:
             assert g.wx_band_stride == 0
@@ -79,9 +91,11 @@ class Oracle:
             raise ValueError("oracle rejected the GPP inputs")
         return out
 
-    def gpp_sx(self, g, nvband: int | None = None, factored: bool = False) -> np.ndarray:
+    def gpp_sx(self, g, nvband: int | None = None, factored: bool = False, pole_guard: float = 0.0) -> np.ndarray:
         """Screened exchange of the occupied bands (asxtemp), specified from
         the GPP model (not in the reference: parity unpinned)."""
+        if pole_guard:
+            return self._guarded(pole_guard, lambda: self.gpp_sx(g, nvband, factored))
         nv = g.nvband if nvband is None else nvband
         out = np.zeros(3, dtype=np.complex128)
         st = self.lib.orc_gpp_sx(g.number_bands, nv, g.ngpown, g.ncouls, _p(g.inv_igp_index), _p(g.indinv),

@@ -155,3 +155,57 @@ def test_gpp_sx_uniform_closed_form(oracle):
     kat = np.array([-n * 0.125j * (1 / (w - wt) - 1 / (w + wt)) for w in (3.0, 4.0, 5.0)])
     assert rel_err(oracle.gpp_sx(g), kat) < 1e-13
     assert np.all(oracle.gpp_sx(g, nvband=0) == 0)
+
+
+# ------------------------------------------------------ near-pole guard --
+# Not in the reference (it has no guard): terms with |wx - wtilde| < delta
+# are left out.  Checked against an independent numpy evaluation and, for
+# the exchange, against the partial-fraction identity with the guard on.
+
+def near_pole_case(seed=3, nb=6, nv=2, G=300, npg=6):
+    """Seeded inputs with wx inside wtilde's range and planted poles: some
+    wtilde within 1e-7 of wx[1] and of -wx[0] (the exchange's -wx sum)."""
+    g = I.gpp_seeded(nb, nv, G, npg, seed=seed)
+    g.wx_array = np.array([1.0, 1.25, 1.5])
+    wt = g.wtilde_array.copy()
+    rng = np.random.default_rng(seed)
+    P = wt.shape[0]
+    for k in range(6):
+        p, ig = int(rng.integers(P)), int(rng.integers(G))
+        wt[p, ig] = (g.wx_array[1] if k % 2 == 0 else -g.wx_array[0]) + 1e-7 * (1 + 1j)
+    g.wtilde_array = wt
+    return g
+
+
+def numpy_gpp(g, delta):
+    igp = g.indinv[g.inv_igp_index]
+    P = g.ngpown
+    s = (np.conj(g.aqsmtemp[:, igp]) * g.aqsntemp[:, igp] * 0.5 * g.vcoul[igp]
+         * g.wtilde_array[np.arange(P), igp]).sum(axis=0)                  # S(p)
+    out = np.zeros(3, np.complex128)
+    for iw, x in enumerate(g.wx_array):
+        d = x - g.wtilde_array
+        q = np.where(np.abs(d) ** 2 < delta ** 2, 0.0, g.I_eps_array / np.where(d == 0, 1, d))
+        out[iw] = (s[:, None] * q).sum()
+    return out
+
+
+@pytest.mark.parametrize("delta", [1e-4, 3e-2, 0.2])
+def test_gpp_pole_guard_vs_numpy(oracle, delta):
+    g = near_pole_case()
+    got = oracle.gpp(g, pole_guard=delta)
+    assert rel_err(got, numpy_gpp(g, delta)) < 1e-12
+    assert rel_err(oracle.gpp(g, factored=True, pole_guard=delta), got) < 1e-13
+    # Unguarded, the planted poles dominate.
+    assert np.abs(oracle.gpp(g)).max() > 50 * np.abs(got).max()
+    # The guard is reset after the call.
+    assert np.array_equal(oracle.gpp(g), oracle.gpp(g, pole_guard=0.0))
+
+
+@pytest.mark.parametrize("delta", [1e-4, 3e-2])
+def test_gpp_sx_pole_guard_partial_fractions(oracle, delta):
+    g = near_pole_case(seed=5, nv=3)
+    sx = oracle.gpp_sx(g, pole_guard=delta)
+    pf = -(oracle.gpp(_occupied(g, 3, False), pole_guard=delta) + oracle.gpp(_occupied(g, 3, True), pole_guard=delta))
+    assert rel_err(sx, pf) < 1e-13
+    assert rel_err(oracle.gpp_sx(g, factored=True, pole_guard=delta), sx) < 1e-13
