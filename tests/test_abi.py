@@ -126,3 +126,30 @@ def test_dropin_drivers_link():
         # main calls the kernels through undefined (shim) symbols, and the
         # weakened reference definitions are overridden.
         assert "noflagOCC_solver" in out or "achsDtemp_Kernel" in out
+
+
+def test_pole_guard_option_validation(bgw):
+    """pole_guard is validated before any device work; a caller with the
+    shorter, older bgw_options (struct_size without the field) never has the
+    trailing bytes read."""
+    import torch
+    g = I.gpp_seeded(2, 1, 40, 20)
+    assert _gpp_call(bgw, g, pole_guard=float("nan")) == -1
+    assert _gpp_call(bgw, g, pole_guard=-1.0) == -1
+    lib = bgw.load()
+    o = bgw.make_options("host", pole_guard=float("nan"))
+    o.struct_size = bgw.Options.pole_guard.offset          # the older layout
+    out = np.zeros(3, dtype=np.complex128)
+    p = bgw._ptr
+    st = lib.bgw_noflagOCC_solver(g.number_bands, g.ngpown, g.ncouls, p(g.inv_igp_index), p(g.indinv),
+                                  len(g.indinv), p(g.wx_array), p(g.wtilde_array), p(g.aqsmtemp),
+                                  p(g.aqsntemp), p(g.I_eps_array), p(g.vcoul), p(out), ctypes.byref(o))
+    assert st == (0 if torch.cuda.is_available() else -5)
+
+
+def test_gpp_sigma_nvband_validation(bgw):
+    g = I.gpp_seeded(4, 2, 40, 20)
+    for nv in (-1, 5):
+        with pytest.raises(bgw.BgwError) as e:
+            bgw.gpp_sigma(g, nvband=nv)
+        assert e.value.status == -1
