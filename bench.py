@@ -386,9 +386,13 @@ def run_ours(args, world, rank, local):
         extra["gpp_sx"] = {"output": "asxtemp", "nvband": g.nvband, "s_per_call": statistics.mean(sdev) / 1e3,
                            "note": "not in the reference (no flagOCC branch): parity unpinned, checked against "
                                    "the oracle's product form"}
+        # The same output from the mixed band loop (FP32 quotients).
+        _, sxm = bgw.gpp_sigma(d, stream=sh, algorithm="bandloop", precision="mixed", want_ach=False)
         if rank == 0 and not args.no_cpu:
             from oracle.oracle import Oracle
-            extra["gpp_sx"]["rel_err_vs_oracle"] = rel_err(sx.cpu().numpy(), Oracle().gpp_sx(g, factored=True))
+            sx_ref = Oracle().gpp_sx(g, factored=True)
+            extra["gpp_sx"]["rel_err_vs_oracle"] = rel_err(sx.cpu().numpy(), sx_ref)
+            extra["gpp_sx"]["rel_err_mixed_vs_oracle"] = rel_err(sxm.cpu().numpy(), sx_ref)
     del d
     torch.cuda.empty_cache()
 

@@ -99,11 +99,14 @@ __global__ void gpp_wx_kernel(int nb, const double *__restrict__ wx, long long s
 //   dr  = x - wr,  |wdiff|^2 = dr^2 + wi^2,
 //   conj(wdiff) * I_eps = (dr*Ir + a) + i (dr*Ii + b).
 // Elements per thread: FP64 4, mixed 8 (the FP32 quotients are cheap, so a
-// longer run per band amortises the FP64 band combination).
+// longer run per band amortises the band combination).  Threads per CTA:
+// FP64 256 (2 CTAs per SM); mixed 384 (one CTA per SM: 12 warps, as many as
+// its registers allow, to hide the MUFU latency; 223 KB of staging).
 template <bool MIXED>
 struct BandCfg {
   static constexpr int kE = MIXED ? 8 : 4;
-  static constexpr int kCH = kThreads * kE;
+  static constexpr int kNT = MIXED ? 384 : kThreads;
+  static constexpr int kCH = kNT * kE;
 };
 
 template <int BCH, bool MIXED>
@@ -113,29 +116,31 @@ struct BandSmem {
   double2 st[2][BCH];
   double4 wx[2][BCH];
   unsigned long long bar[2];
-  double red[(kThreads / 32) * 6];
-  double xr_lo[kThreads / 32], xr_hi[kThreads / 32];  // MIXED: chunk frequency range
+  double red[(BandCfg<MIXED>::kNT / 32) * 6];
+  double xr_lo[BandCfg<MIXED>::kNT / 32], xr_hi[BandCfg<MIXED>::kNT / 32];  // MIXED: chunk frequency range
+  float4 xf[MIXED ? BCH : 1];                                                 // MIXED: FP32 frequency rows
+  float2 sf[MIXED ? BCH : 1];                                                 // MIXED: FP32 sch_store1
 };
 
 // Every band reads its own frequencies from the staged wx4 rows (for the
 // reference's band-independent wx the rows repeat one triple), so each
 // (band, G', G, frequency) quotient is evaluated, as in gpp.cpp:343-390.
-// MIXED: quotients in FP32 (rcp.approx.ftz.f32), the per-band products with
-// sch_store1 and the accumulation over bands in FP64 with TwoSum
-// compensation.
+// MIXED: quotients in FP32 (rcp.approx.ftz.f32), their products with
+// sch_store1 summed in FP32 over groups of 8 bands, the group sums
+// accumulated in FP64 with TwoSum compensation (band_sweep_mixed).
 // GUARD (FP64): near-pole cut-off, terms with |wdiff|^2 < guard2 contribute
 // zero.  MIXED: elements near the chunk's frequencies take an FP64 path
 // (near_elems / near_sweep), which also applies the cut-off (guard_d =
 // sqrt(guard2)); GUARD is not used.
 template <int BCH, bool MIXED, bool GUARD>
-__global__ void __launch_bounds__(kThreads, MIXED ? 1 : 2)
+__global__ void __launch_bounds__(BandCfg<MIXED>::kNT, MIXED ? 1 : 2)
     gpp_bandloop_kernel(int nb, int G, long long items, int nchunks_g, const double2 *__restrict__ wtilde,
                         const double2 *__restrict__ ieps, const double2 *__restrict__ st,
                         const double4 *__restrict__ wx4, double *__restrict__ partials, int *status,
                         double guard2, double guard_d) {
   constexpr int kE = BandCfg<MIXED>::kE;
   constexpr int kCH = BandCfg<MIXED>::kCH;
-  using T = typename std::conditional<MIXED, float, double>::type;
+  constexpr int kThreads = BandCfg<MIXED>::kNT;  // shadows the file-wide 256
   extern __shared__ __align__(128) unsigned char smem_raw[];
   using Smem = BandSmem<BCH, MIXED>;
   Smem &sm = *reinterpret_cast<Smem *>(smem_raw);
@@ -194,17 +199,18 @@ __global__ void __launch_bounds__(kThreads, MIXED ? 1 : 2)
     const int b0 = c * BCH;
     const int nbv = min(BCH, nb - b0);
 
-    Elem<T> e[kE];
-    load_elems<T, kE>(e, sm.wt[buf], sm.ie[buf], nvalid, kThreads, tid);
-    uint32_t near = 0;
     if constexpr (MIXED) {
-      const double2 xr = chunk_wx_range<kThreads>(sm.wx[buf], nbv, sm.xr_lo, sm.xr_hi);
-      near = near_elems<kE>(e, sm.wt[buf], nvalid, kThreads, tid, xr, guard_d);
-    }
-    band_sweep<MIXED, kE, GUARD && !MIXED>(e, sm.wx[buf], sm.st[buf], nbv, acc_r, acc_i, lo_r, lo_i, guard2);
-    if constexpr (MIXED) {
+      Elem<float> e[kE];
+      load_elems<float, kE>(e, sm.wt[buf], sm.ie[buf], nvalid, kThreads, tid);
+      const double2 xr = stage_mixed_rows<kThreads>(sm.wx[buf], sm.st[buf], nbv, sm.xf, sm.sf, sm.xr_lo, sm.xr_hi);
+      const uint32_t near = near_elems<kE>(e, sm.wt[buf], nvalid, kThreads, tid, xr, guard_d);
+      band_sweep_mixed<kE>(e, sm.xf, sm.sf, nbv, acc_r, acc_i, lo_r, lo_i);
       if (near) near_sweep(near, sm.wt[buf], sm.ie[buf], kThreads, tid, sm.wx[buf], sm.st[buf], nbv, guard2, acc_r,
                            acc_i, lo_r, lo_i);
+    } else {
+      Elem<double> e[kE];
+      load_elems<double, kE>(e, sm.wt[buf], sm.ie[buf], nvalid, kThreads, tid);
+      band_sweep<kE, GUARD>(e, sm.wx[buf], sm.st[buf], nbv, acc_r, acc_i, guard2);
     }
     __syncthreads();  // buffer `buf` is free for step j + 2
   }
@@ -290,7 +296,7 @@ int bandloop_per_sm(int *per_sm) {
   const size_t smem = sizeof(Smem);
   auto kfn = gpp_bandloop_kernel<BCH, MIXED, GUARD>;
   BGW_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  BGW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kfn, kThreads, smem));
+  BGW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kfn, BandCfg<MIXED>::kNT, smem));
   return *per_sm >= 1 ? BGW_OK : BGW_ERR_UNSUPPORTED;
 }
 
@@ -307,7 +313,7 @@ int launch_bandloop(cudaStream_t stream, int max_grid, int nb, int G, const doub
   long long grid = std::min<long long>(items, (long long)max_grid);
   if (grid < 1) grid = 1;
   *grid_out = (int)grid;
-  gpp_bandloop_kernel<BCH, MIXED, GUARD><<<(int)grid, kThreads, smem, stream>>>(nb, G, items, nchunks_g, wt, ie, st,
+  gpp_bandloop_kernel<BCH, MIXED, GUARD><<<(int)grid, BandCfg<MIXED>::kNT, smem, stream>>>(nb, G, items, nchunks_g, wt, ie, st,
                                                                                  wx4, partials, status, guard2,
                                                                                  guard_d);
   count_launch();

@@ -112,7 +112,7 @@ __global__ void batch_wx_kernel(const BatchInst *__restrict__ inst, int n) {
   }
 }
 
-template <int BCH, int KE>
+template <int BCH, int KE, bool MIXED>
 struct BatchSmem {
   double2 wt[2][kBThreads * KE];
   double2 ie[2][kBThreads * KE];
@@ -121,6 +121,8 @@ struct BatchSmem {
   unsigned long long bar[2];
   double red[(kBThreads / 32) * 6];
   double xr_lo[kBThreads / 32], xr_hi[kBThreads / 32];  // MIXED: chunk frequency range
+  float4 xf[MIXED ? BCH : 1];                            // MIXED: FP32 frequency rows
+  float2 sf[MIXED ? BCH : 1];                            // MIXED: FP32 sch_store1
 };
 
 // Flushes the running sums of instance slot `seg` of this CTA.
@@ -143,10 +145,9 @@ template <int BCH, int KE, bool MIXED>
 __global__ void __launch_bounds__(kBThreads, (MIXED && KE == 8) ? 1 : 2)
     batch_bandloop_kernel(const BatchInst *__restrict__ inst, int n, const long long *__restrict__ range,
                           int max_seg, double *__restrict__ partials, int *status) {
-  using T = typename std::conditional<MIXED, float, double>::type;
   constexpr int kCH = kBThreads * KE;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  auto &sm = *reinterpret_cast<BatchSmem<BCH, KE> *>(smem_raw);
+  auto &sm = *reinterpret_cast<BatchSmem<BCH, KE, MIXED> *>(smem_raw);
   const int tid = threadIdx.x;
   const long long j0 = range[blockIdx.x], j1 = range[blockIdx.x + 1];
   if (j0 >= j1) return;  // uniform per CTA: no barrier is skipped by some threads only
@@ -212,18 +213,19 @@ __global__ void __launch_bounds__(kBThreads, (MIXED && KE == 8) ? 1 : 2)
     const int g0 = (int)(local % I.nchunk) * kCH;
     const int nvalid = min(kCH, I.G - g0);
     const int nbv = max(0, min(BCH, I.nb - cur.c * BCH));
-    Elem<T> e[KE];
-    load_elems<T, KE>(e, sm.wt[buf], sm.ie[buf], nvalid, kBThreads, tid);
     // MIXED: elements near the chunk's frequencies are summed in FP64.
-    uint32_t near = 0;
     if constexpr (MIXED) {
-      const double2 xr = chunk_wx_range<kBThreads>(sm.wx[buf], nbv, sm.xr_lo, sm.xr_hi);
-      near = near_elems<KE>(e, sm.wt[buf], nvalid, kBThreads, tid, xr, 0.0);
-    }
-    band_sweep<MIXED, KE>(e, sm.wx[buf], sm.st[buf], nbv, acc_r, acc_i, lo_r, lo_i);
-    if constexpr (MIXED) {
+      Elem<float> e[KE];
+      load_elems<float, KE>(e, sm.wt[buf], sm.ie[buf], nvalid, kBThreads, tid);
+      const double2 xr = stage_mixed_rows<kBThreads>(sm.wx[buf], sm.st[buf], nbv, sm.xf, sm.sf, sm.xr_lo, sm.xr_hi);
+      const uint32_t near = near_elems<KE>(e, sm.wt[buf], nvalid, kBThreads, tid, xr, 0.0);
+      band_sweep_mixed<KE>(e, sm.xf, sm.sf, nbv, acc_r, acc_i, lo_r, lo_i);
       if (near) near_sweep(near, sm.wt[buf], sm.ie[buf], kBThreads, tid, sm.wx[buf], sm.st[buf], nbv, 0.0, acc_r,
                            acc_i, lo_r, lo_i);
+    } else {
+      Elem<double> e[KE];
+      load_elems<double, KE>(e, sm.wt[buf], sm.ie[buf], nvalid, kBThreads, tid);
+      band_sweep<KE>(e, sm.wx[buf], sm.st[buf], nbv, acc_r, acc_i);
     }
     __syncthreads();  // buffer `buf` is free for step s + 2
     if (!more || nx.i != cur.i) flush(acc_r, acc_i, lo_r, lo_i, sm.red, partials, max_seg, cur.i - inst_lo);
@@ -346,7 +348,7 @@ struct Variant {
 template <int KE, bool MIXED>
 int band_variant(Variant *v) {
   v->ke = KE;
-  v->smem = sizeof(BatchSmem<256, KE>);
+  v->smem = sizeof(BatchSmem<256, KE, MIXED>);
   auto kfn = batch_bandloop_kernel<256, KE, MIXED>;
   BGW_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v->smem));
   BGW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v->per_sm, kfn, kBThreads, v->smem));

@@ -91,56 +91,42 @@ __device__ __forceinline__ void load_elems(Elem<T> (&e)[kE], const double2 *__re
   }
 }
 
-// The band sweep of the GPP band loop (gpp.cpp:360-390): for each of nbv
-// bands, the kE x 3 quotients q = conj(wdiff) I_eps / |wdiff|^2 of this
-// thread's elements are summed and multiplied by sch_store1 (st[b]), and the
-// product is accumulated per frequency.  FP64: reciprocal by rcp_refined.
-// MIXED: quotients and their per-band partial in FP32, the product and the
-// accumulation in FP64 with TwoSum tails (lo_r / lo_i).
+// The band sweep of the FP64 GPP band loop (gpp.cpp:360-390): for each of
+// nbv bands, the kE x 3 quotients q = conj(wdiff) I_eps / |wdiff|^2 of this
+// thread's elements are summed (reciprocal by rcp_refined) and multiplied by
+// sch_store1 (st[b]), and the product is accumulated per frequency.  (The
+// mixed form is band_sweep_mixed below.)
 // GUARD: a term with |wdiff|^2 < guard2 contributes zero (near-pole cut-off;
 // the select discards the reciprocal, so a zero |wdiff| yields no NaN).
-template <bool MIXED, int kE, bool GUARD = false>
-__device__ __forceinline__ void band_sweep(const Elem<typename std::conditional<MIXED, float, double>::type> (&e)[kE],
-                                           const double4 *__restrict__ wx, const double2 *__restrict__ st, int nbv,
-                                           double (&acc_r)[3], double (&acc_i)[3], double (&lo_r)[3],
-                                           double (&lo_i)[3], double guard2 = 0.0) {
-  using T = typename std::conditional<MIXED, float, double>::type;
+template <int kE, bool GUARD = false>
+__device__ __forceinline__ void band_sweep(const Elem<double> (&e)[kE], const double4 *__restrict__ wx,
+                                           const double2 *__restrict__ st, int nbv, double (&acc_r)[3],
+                                           double (&acc_i)[3], double guard2 = 0.0) {
   for (int bb = 0; bb < nbv; ++bb) {
     const double4 w4 = wx[bb];
-    const T x[3] = {(T)w4.x, (T)w4.y, (T)w4.z};
+    const double x[3] = {w4.x, w4.y, w4.z};
     const double2 s = st[bb];
-    T tr[3] = {(T)0, (T)0, (T)0}, ti[3] = {(T)0, (T)0, (T)0};
+    double tr[3] = {0.0, 0.0, 0.0}, ti[3] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int k = 0; k < kE; ++k) {
 #pragma unroll
       for (int iw = 0; iw < 3; ++iw) {
-        const T dr = x[iw] - e[k].wr;
-        const T den = fma(dr, dr, e[k].wi2);
-        T r;
-        if constexpr (MIXED) {
-          r = rcp_approx_f32(den);
-        } else {
-          r = rcp_refined(den);
-        }
-        if constexpr (GUARD) r = den < (T)guard2 ? (T)0 : r;
-        const T nr = fma(dr, e[k].Ir, e[k].a);
-        const T ni = fma(dr, e[k].Ii, e[k].b);
+        const double dr = x[iw] - e[k].wr;
+        const double den = fma(dr, dr, e[k].wi2);
+        double r = rcp_refined(den);
+        if constexpr (GUARD) r = den < guard2 ? 0.0 : r;
+        const double nr = fma(dr, e[k].Ir, e[k].a);
+        const double ni = fma(dr, e[k].Ii, e[k].b);
         tr[iw] = fma(nr, r, tr[iw]);
         ti[iw] = fma(ni, r, ti[iw]);
       }
     }
 #pragma unroll
     for (int iw = 0; iw < 3; ++iw) {
-      const double trd = (double)tr[iw], tid_ = (double)ti[iw];
-      if constexpr (MIXED) {
-        two_sum_acc(acc_r[iw], lo_r[iw], fma(trd, s.x, -tid_ * s.y));
-        two_sum_acc(acc_i[iw], lo_i[iw], fma(trd, s.y, tid_ * s.x));
-      } else {
-        acc_r[iw] = fma(trd, s.x, acc_r[iw]);
-        acc_r[iw] = fma(-tid_, s.y, acc_r[iw]);
-        acc_i[iw] = fma(trd, s.y, acc_i[iw]);
-        acc_i[iw] = fma(tid_, s.x, acc_i[iw]);
-      }
+      acc_r[iw] = fma(tr[iw], s.x, acc_r[iw]);
+      acc_r[iw] = fma(-ti[iw], s.y, acc_r[iw]);
+      acc_i[iw] = fma(tr[iw], s.y, acc_i[iw]);
+      acc_i[iw] = fma(ti[iw], s.x, acc_i[iw]);
     }
   }
 }
@@ -158,14 +144,19 @@ __device__ __forceinline__ void band_sweep(const Elem<typename std::conditional<
 // elements are zeroed in the FP32 copy and summed in FP64, guard included.
 constexpr double kNearFrac = 0.25;
 
-// [lo, hi] of the frequencies of the chunk's nbv bands, broadcast to every
-// thread (all threads must call; two warp-level folds and one barrier).
+// Per step of the mixed band loop: FP32 copies of the chunk's nbv frequency
+// rows (xf) and sch_store1 values (sf), and [lo, hi] of its frequencies,
+// broadcast to every thread (all threads must call; two warp-level folds and
+// one barrier, which also publishes xf / sf).
 template <int kThreads>
-__device__ __forceinline__ double2 chunk_wx_range(const double4 *__restrict__ wx, int nbv, double *s_lo,
-                                                  double *s_hi) {
+__device__ __forceinline__ double2 stage_mixed_rows(const double4 *__restrict__ wx, const double2 *__restrict__ st,
+                                                    int nbv, float4 *xf, float2 *sf, double *s_lo, double *s_hi) {
   double lo = INFINITY, hi = -INFINITY;
   for (int b = threadIdx.x; b < nbv; b += kThreads) {
     const double4 w = wx[b];
+    const double2 v = st[b];
+    xf[b] = make_float4((float)w.x, (float)w.y, (float)w.z, 0.f);
+    sf[b] = make_float2((float)v.x, (float)v.y);
     lo = fmin(lo, fmin(w.x, fmin(w.y, w.z)));
     hi = fmax(hi, fmax(w.x, fmax(w.y, w.z)));
   }
@@ -185,6 +176,51 @@ __device__ __forceinline__ double2 chunk_wx_range(const double4 *__restrict__ wx
     hi = fmax(hi, s_hi[w]);
   }
   return make_double2(lo, hi);
+}
+
+// The band sweep of the mixed band loop: the quotients of band_sweep in
+// FP32 (rcp.approx.ftz.f32), their products with sch_store1 summed in FP32
+// over groups of kGroup bands, each group sum added to the FP64 accumulators
+// with TwoSum (one conversion and two TwoSums per kGroup bands and
+// frequency: the XU and FP64 pipes stay free for the reciprocals, which
+// bound this loop).
+template <int kE>
+__device__ __forceinline__ void band_sweep_mixed(const Elem<float> (&e)[kE], const float4 *__restrict__ xf,
+                                                 const float2 *__restrict__ sf, int nbv, double (&acc_r)[3],
+                                                 double (&acc_i)[3], double (&lo_r)[3], double (&lo_i)[3]) {
+  constexpr int kGroup = 8;
+  for (int b0 = 0; b0 < nbv; b0 += kGroup) {
+    const int b1 = min(b0 + kGroup, nbv);
+    float gr[3] = {0.f, 0.f, 0.f}, gi[3] = {0.f, 0.f, 0.f};
+    for (int bb = b0; bb < b1; ++bb) {
+      const float4 w4 = xf[bb];
+      const float x[3] = {w4.x, w4.y, w4.z};
+      const float2 s = sf[bb];
+      float tr[3] = {0.f, 0.f, 0.f}, ti[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+      for (int k = 0; k < kE; ++k) {
+#pragma unroll
+        for (int iw = 0; iw < 3; ++iw) {
+          const float dr = x[iw] - e[k].wr;
+          const float r = rcp_approx_f32(fmaf(dr, dr, e[k].wi2));
+          tr[iw] = fmaf(fmaf(dr, e[k].Ir, e[k].a), r, tr[iw]);
+          ti[iw] = fmaf(fmaf(dr, e[k].Ii, e[k].b), r, ti[iw]);
+        }
+      }
+#pragma unroll
+      for (int iw = 0; iw < 3; ++iw) {
+        gr[iw] = fmaf(tr[iw], s.x, gr[iw]);
+        gr[iw] = fmaf(-ti[iw], s.y, gr[iw]);
+        gi[iw] = fmaf(tr[iw], s.y, gi[iw]);
+        gi[iw] = fmaf(ti[iw], s.x, gi[iw]);
+      }
+    }
+#pragma unroll
+    for (int iw = 0; iw < 3; ++iw) {
+      two_sum_acc(acc_r[iw], lo_r[iw], (double)gr[iw]);
+      two_sum_acc(acc_i[iw], lo_i[iw], (double)gi[iw]);
+    }
+  }
 }
 
 // Marks this thread's near elements (bit k for element k) and zeroes their
