@@ -383,7 +383,16 @@ def run_ours(args, world, rank, local):
         for _ in range(max(3, args.steps // 2)):
             _, sx = bgw.gpp_sigma(d, stream=sh, algorithm="factored", want_ach=False, flags=bgw.FLAG_PROFILE)
             sdev.append(bgw.last_profile()["device_ms"])
+        bdev = []
+        for _ in range(max(3, args.steps // 2)):
+            bgw.gpp_sigma(d, stream=sh, algorithm="factored", flags=bgw.FLAG_PROFILE)
+            p = bgw.last_profile()
+            bdev.append((p["device_ms"], p["main_kernel_ms"]))
         extra["gpp_sx"] = {"output": "asxtemp", "nvband": g.nvband, "s_per_call": statistics.mean(sdev) / 1e3,
+                           "achtemp_and_asxtemp_s_per_call": statistics.mean(b[0] for b in bdev) / 1e3,
+                           "kernel": p["main_kernel"], "kernel_ms": statistics.mean(b[1] for b in bdev),
+                           "hbm_frac": p["main_bytes"] / (statistics.mean(b[1] for b in bdev) * 1e-3) / 1e9
+                           / _hbm_peak(),
                            "note": "not in the reference (no flagOCC branch): parity unpinned, checked against "
                                    "the oracle's product form"}
         # The same output from the mixed band loop (FP32 quotients).

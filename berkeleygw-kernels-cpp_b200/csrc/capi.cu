@@ -23,6 +23,10 @@ int gpp_run_host(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *
 int gpp_sx_enqueue(CallEnv *env, int64_t nvband, int64_t P, int64_t G, const int32_t *inv, const int32_t *indinv,
                    int64_t indinv_len, const double *wx, size_t wx_n, int64_t wx_stride, const double2 *wt,
                    const double2 *am, const double2 *an, const double2 *ie, const double *vc, double *asx_dev);
+int gpp_sigma_factored_enqueue(CallEnv *env, int64_t nb, int64_t nv, int64_t P, int64_t G, const int32_t *inv,
+                               const int32_t *indinv, int64_t indinv_len, const double *wx, const double2 *wt,
+                               const double2 *am, const double2 *an, const double2 *ie, const double *vc,
+                               double *ach_dev, double *asx_dev);
 
 int gpp_adjoint_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *inv, const int32_t *indinv,
                         int64_t indinv_len, const double *wx, const double2 *wt, const double2 *am,
@@ -158,14 +162,26 @@ extern "C" int bgw_gpp_sigma(int64_t number_bands, int64_t nvband, int64_t ngpow
   double *out = nullptr;  // achtemp | asxtemp (6 doubles each)
   BGW_TRY(out_buffer(env, nullptr, 12 * sizeof(double), &out));
   double *o_ach = env->host ? out : achtemp, *o_asx = env->host ? out + 6 : asxtemp;
-  if (achtemp)
-    BGW_TRY(gpp_enqueue(env, nb, P, G, (const int32_t *)inv, (const int32_t *)ind, indinv_len, (const double *)wx,
-                        stride, (const double2 *)wt, (const double2 *)am, (const double2 *)an, (const double2 *)ie,
-                        (const double *)vc, o_ach));
-  if (asxtemp)
-    BGW_TRY(gpp_sx_enqueue(env, nvband, P, G, (const int32_t *)inv, (const int32_t *)ind, indinv_len,
-                           (const double *)wx, wx_n, stride, (const double2 *)wt, (const double2 *)am,
-                           (const double2 *)an, (const double2 *)ie, (const double *)vc, o_asx));
+  const bool factored = env->opt.gpp_algorithm == BGW_GPP_FACTORED ||
+                        (env->opt.gpp_algorithm == BGW_GPP_AUTO && stride == 0 &&
+                         env->opt.precision == BGW_PRECISION_FP64);
+  if (factored && (stride != 0 || env->opt.precision != BGW_PRECISION_FP64)) return BGW_ERR_UNSUPPORTED;
+  if (factored && asxtemp && P > 0) {
+    // Both outputs in one pass over wtilde / I_eps.
+    BGW_TRY(gpp_sigma_factored_enqueue(env, nb, nvband, P, G, (const int32_t *)inv, (const int32_t *)ind,
+                                       indinv_len, (const double *)wx, (const double2 *)wt, (const double2 *)am,
+                                       (const double2 *)an, (const double2 *)ie, (const double *)vc,
+                                       achtemp ? o_ach : nullptr, o_asx));
+  } else {
+    if (achtemp)
+      BGW_TRY(gpp_enqueue(env, nb, P, G, (const int32_t *)inv, (const int32_t *)ind, indinv_len,
+                          (const double *)wx, stride, (const double2 *)wt, (const double2 *)am, (const double2 *)an,
+                          (const double2 *)ie, (const double *)vc, o_ach));
+    if (asxtemp)
+      BGW_TRY(gpp_sx_enqueue(env, nvband, P, G, (const int32_t *)inv, (const int32_t *)ind, indinv_len,
+                             (const double *)wx, wx_n, stride, (const double2 *)wt, (const double2 *)am,
+                             (const double2 *)an, (const double2 *)ie, (const double *)vc, o_asx));
+  }
   if (env->host) {
     if (achtemp) BGW_CUDA_TRY(cudaMemcpyAsync(achtemp, o_ach, 6 * sizeof(double), cudaMemcpyDeviceToHost, env->stream));
     if (asxtemp) BGW_CUDA_TRY(cudaMemcpyAsync(asxtemp, o_asx, 6 * sizeof(double), cudaMemcpyDeviceToHost, env->stream));

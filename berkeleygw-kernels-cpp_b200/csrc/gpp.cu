@@ -47,17 +47,20 @@ constexpr int kChunk = kThreads * kElems;  // ig per item
 // One warp per column p: st row (if st != nullptr) and S[p] (if S != nullptr).
 // gstride > 0: am / an / vc were gathered on the host to the columns
 // igp(p) (am[n1 * gstride + p], vc[p]); wtilde is always read at igp(p).
+// S_occ (optional): the same sum over the first nv bands only (the occupied
+// bands of the screened exchange); S is unaffected by it.
 __global__ void __launch_bounds__(256) gpp_prep_kernel(int nb, int P, int G, const int *__restrict__ inv,
                                                        const int *__restrict__ indinv, long long indinv_len,
                                                        const double2 *__restrict__ wt, const double2 *__restrict__ am,
                                                        const double2 *__restrict__ an, const double *__restrict__ vc,
                                                        double2 *__restrict__ st, double2 *__restrict__ S,
-                                                       int *status, long long gstride) {
+                                                       int *status, long long gstride, int nv = 0,
+                                                       double2 *__restrict__ S_occ = nullptr) {
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
   for (int p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; p < P; p += warps) {
     int g = resolve_igp(p, inv, indinv, indinv_len, G, status);
-    double sr = 0.0, si = 0.0;
+    double sr = 0.0, si = 0.0, or_ = 0.0, oi = 0.0;
     for (int n1 = lane; n1 < nb; n1 += 32) {
       double2 s = make_double2(0.0, 0.0);
       if (g >= 0 && gstride > 0) {
@@ -76,11 +79,20 @@ __global__ void __launch_bounds__(256) gpp_prep_kernel(int nb, int P, int G, con
       if (st) st[(size_t)p * nb + n1] = s;
       sr += s.x;
       si += s.y;
+      if (n1 < nv) {
+        or_ += s.x;
+        oi += s.y;
+      }
     }
     if (S) {
       sr = warp_sum(sr);
       si = warp_sum(si);
       if (lane == 0) S[p] = make_double2(sr, si);
+    }
+    if (S_occ) {
+      or_ = warp_sum(or_);
+      oi = warp_sum(oi);
+      if (lane == 0) S_occ[p] = make_double2(or_, oi);
     }
   }
 }
@@ -235,19 +247,26 @@ __global__ void __launch_bounds__(BandCfg<MIXED>::kNT, MIXED ? 1 : 2)
 // HBM-bound stream over wtilde / I_eps with 128-bit loads; one item =
 // (p, chunk of kChunk ig); per-thread sums are folded per CTA.
 // GUARD: near-pole cut-off as in the band loop.
-template <bool GUARD>
-__global__ void __launch_bounds__(kThreads)
+// SX: also the screened exchange of the occupied bands in the same pass over
+// wtilde / I_eps: the sums at -wx are formed beside those at +wx, and
+// asxtemp = -sum_p S_occ(p) (T(p, wx) + T(p, -wx)) (partial fractions of
+// wtilde / (wx^2 - wtilde^2)); partials then hold 12 doubles per CTA,
+// achtemp's 6 (bitwise the same as without SX) and asxtemp's 6.
+template <bool GUARD, bool SX = false>
+__global__ void __launch_bounds__(kThreads, SX ? 2 : 4)
     gpp_factored_kernel(int G, long long items, int nchunks_g, const double2 *__restrict__ wtilde,
                         const double2 *__restrict__ ieps, const double2 *__restrict__ S,
-                        const double *__restrict__ wx3, double *__restrict__ partials, double guard2) {
-  __shared__ double red[(kThreads / 32) * 6];
+                        const double *__restrict__ wx3, double *__restrict__ partials, double guard2,
+                        const double2 *__restrict__ S_occ = nullptr) {
+  constexpr int W = SX ? 12 : 6;
+  __shared__ double red[(kThreads / 32) * W];
   const int tid = threadIdx.x;
   const double x[3] = {wx3[0], wx3[1], wx3[2]};
   double acc_r[3] = {0.0, 0.0, 0.0}, acc_i[3] = {0.0, 0.0, 0.0};
-  for (long long item = blockIdx.x; item < items; item += gridDim.x) {
+  double ax_r[3] = {0.0, 0.0, 0.0}, ax_i[3] = {0.0, 0.0, 0.0};  // SX
+  auto load = [&](long long item, double2 (&w)[kElems], double2 (&v)[kElems]) {
     const long long p = item / nchunks_g;
     const int g0 = (int)(item % nchunks_g) * kChunk;
-    double2 w[kElems], v[kElems];
 #pragma unroll
     for (int k = 0; k < kElems; ++k) {
       const int ig = g0 + k * kThreads + tid;
@@ -259,7 +278,29 @@ __global__ void __launch_bounds__(kThreads)
         v[k] = make_double2(0.0, 0.0);
       }
     }
+  };
+  // SX (twice the arithmetic per element): the next item's elements are
+  // loaded before the current item is evaluated, so its loads are in flight
+  // during the math.
+  double2 wn[kElems], vn[kElems];
+  if constexpr (SX) {
+    if ((long long)blockIdx.x < items) load(blockIdx.x, wn, vn);
+  }
+  for (long long item = blockIdx.x; item < items; item += gridDim.x) {
+    const long long p = item / nchunks_g;
+    double2 w[kElems], v[kElems];
+    if constexpr (SX) {
+#pragma unroll
+      for (int k = 0; k < kElems; ++k) {
+        w[k] = wn[k];
+        v[k] = vn[k];
+      }
+      if (item + gridDim.x < items) load(item + gridDim.x, wn, vn);
+    } else {
+      load(item, w, v);
+    }
     double tr[3] = {0.0, 0.0, 0.0}, ti[3] = {0.0, 0.0, 0.0};
+    double ur[3] = {0.0, 0.0, 0.0}, ui[3] = {0.0, 0.0, 0.0};  // SX: at -wx
 #pragma unroll
     for (int k = 0; k < kElems; ++k) {
       const double wi2 = w[k].y * w[k].y, a = -w[k].y * v[k].y, b = w[k].y * v[k].x;
@@ -271,6 +312,14 @@ __global__ void __launch_bounds__(kThreads)
         if constexpr (GUARD) r = den < guard2 ? 0.0 : r;
         tr[iw] = fma(fma(dr, v[k].x, a), r, tr[iw]);
         ti[iw] = fma(fma(dr, v[k].y, b), r, ti[iw]);
+        if constexpr (SX) {
+          const double dn = -x[iw] - w[k].x;
+          const double dn2 = fma(dn, dn, wi2);
+          double rn = rcp_refined(dn2);
+          if constexpr (GUARD) rn = dn2 < guard2 ? 0.0 : rn;
+          ur[iw] = fma(fma(dn, v[k].x, a), rn, ur[iw]);
+          ui[iw] = fma(fma(dn, v[k].y, b), rn, ui[iw]);
+        }
       }
     }
     const double2 s = S[p];
@@ -281,12 +330,32 @@ __global__ void __launch_bounds__(kThreads)
       acc_i[iw] = fma(tr[iw], s.y, acc_i[iw]);
       acc_i[iw] = fma(ti[iw], s.x, acc_i[iw]);
     }
+    if constexpr (SX) {
+      const double2 so = S_occ[p];
+#pragma unroll
+      for (int iw = 0; iw < 3; ++iw) {
+        const double qr = tr[iw] + ur[iw], qi = ti[iw] + ui[iw];
+        ax_r[iw] = fma(-qr, so.x, ax_r[iw]);
+        ax_r[iw] = fma(qi, so.y, ax_r[iw]);
+        ax_i[iw] = fma(-qr, so.y, ax_i[iw]);
+        ax_i[iw] = fma(-qi, so.x, ax_i[iw]);
+      }
+    }
   }
-  double vv[6] = {acc_r[0], acc_i[0], acc_r[1], acc_i[1], acc_r[2], acc_i[2]};
-  block_sum<6, kThreads>(vv, red);
+  double vv[W];
+#pragma unroll
+  for (int iw = 0; iw < 3; ++iw) {
+    vv[2 * iw] = acc_r[iw];
+    vv[2 * iw + 1] = acc_i[iw];
+    if constexpr (SX) {
+      vv[6 + 2 * iw] = ax_r[iw];
+      vv[6 + 2 * iw + 1] = ax_i[iw];
+    }
+  }
+  block_sum<W, kThreads>(vv, red);
   if (tid == 0) {
 #pragma unroll
-    for (int k = 0; k < 6; ++k) partials[(size_t)blockIdx.x * 6 + k] = vv[k];
+    for (int k = 0; k < W; ++k) partials[(size_t)blockIdx.x * W + k] = vv[k];
   }
 }
 
@@ -621,6 +690,65 @@ __global__ void gpp_sx_combine_kernel(const double *__restrict__ a, const double
   if (threadIdx.x < 6) out[threadIdx.x] = -(a[threadIdx.x] + b[threadIdx.x]);
 }
 }  // namespace
+
+namespace {
+__global__ void gpp_split12_kernel(const double *__restrict__ in, double *__restrict__ ach, double *__restrict__ asx) {
+  const int k = threadIdx.x;
+  if (k < 6 && ach) ach[k] = in[k];
+  if (k < 6 && asx) asx[k] = in[6 + k];
+}
+}  // namespace
+
+// Factored form (band-independent wx, FP64) of bgw_gpp_sigma: one prep pass
+// forms S(p) over all bands and S_occ(p) over the first nv, one pass over
+// wtilde / I_eps forms both outputs (gpp_factored_kernel<., true>).
+// achtemp is bitwise that of gpp_enqueue's factored path.
+int gpp_sigma_factored_enqueue(CallEnv *env, int64_t nb, int64_t nv, int64_t P, int64_t G, const int32_t *inv,
+                               const int32_t *indinv, int64_t indinv_len, const double *wx, const double2 *wt,
+                               const double2 *am, const double2 *an, const double2 *ie, const double *vc,
+                               double *ach_dev, double *asx_dev) {
+  Workspace *ws = env->ws;
+  cudaStream_t stream = env->stream;
+  const bool guard = env->opt.pole_guard > 0.0;
+  const double guard2 = env->opt.pole_guard * env->opt.pole_guard;
+  const int per_launch = ws->sm_count * 8;
+  void *partials_v = nullptr, *tab = nullptr, *out12 = nullptr;
+  BGW_TRY(ws_reserve(ws, SLOT_PARTIALS, sizeof(double) * 12 * (size_t)per_launch, &partials_v));
+  BGW_TRY(ws_reserve(ws, SLOT_TABLE0, sizeof(double2) * 2 * (size_t)std::max<int64_t>(P, 1), &tab));
+  BGW_TRY(ws_reserve(ws, SLOT_IN10, sizeof(double) * 12, &out12));
+  double2 *S = static_cast<double2 *>(tab), *S_occ = S + std::max<int64_t>(P, 1);
+  const int prep_grid = (int)std::max<long long>(1, std::min<long long>((P + 7) / 8, (long long)ws->sm_count * 16));
+  gpp_prep_kernel<<<prep_grid, 256, 0, stream>>>((int)nb, (int)P, (int)G, inv, indinv, indinv_len, wt, am, an, vc,
+                                                 nullptr, S, env->d_status, 0LL, (int)nv, S_occ);
+  count_launch();
+  BGW_CUDA_TRY(cudaGetLastError());
+  const int nchunks_g = (int)((G + kChunk - 1) / kChunk);
+  const long long items = (long long)P * nchunks_g;
+  // The grid of gpp_enqueue's factored launch: the same CTA partition, so
+  // achtemp's partial sums (and the result) are bitwise the same.
+  const int grid = (int)std::min<long long>(std::max<long long>(items, 1), (long long)per_launch);
+  double *partials = static_cast<double *>(partials_v);
+  BGW_TRY(prof_mark(env, 1));
+  if (guard)
+    gpp_factored_kernel<true, true><<<grid, kThreads, 0, stream>>>((int)G, items, nchunks_g, wt, ie, S, wx,
+                                                                   partials, guard2, S_occ);
+  else
+    gpp_factored_kernel<false, true><<<grid, kThreads, 0, stream>>>((int)G, items, nchunks_g, wt, ie, S, wx,
+                                                                    partials, 0.0, S_occ);
+  count_launch();
+  BGW_CUDA_TRY(cudaGetLastError());
+  BGW_TRY(prof_mark(env, 2));
+  env->prof.main_bytes = 32.0 * (double)P * (double)G + 32.0 * (double)P;
+  std::snprintf(env->prof.main_kernel, sizeof(env->prof.main_kernel), "gpp_factored_kernel<sx>");
+  env->prof.main_launches = 1;
+  reduce_partials_kernel<12><<<1, 256, 0, stream>>>(partials, grid, static_cast<double *>(out12));
+  count_launch();
+  BGW_CUDA_TRY(cudaGetLastError());
+  gpp_split12_kernel<<<1, 32, 0, stream>>>(static_cast<const double *>(out12), ach_dev, asx_dev);
+  count_launch();
+  BGW_CUDA_TRY(cudaGetLastError());
+  return BGW_OK;
+}
 
 int gpp_sx_enqueue(CallEnv *env, int64_t nvband, int64_t P, int64_t G, const int32_t *inv, const int32_t *indinv,
                    int64_t indinv_len, const double *wx, size_t wx_n, int64_t wx_stride, const double2 *wt,
