@@ -367,6 +367,25 @@ def run_ours(args, world, rank, local):
             "roofline": {"bound": "hbm", "achieved": p["main_bytes"] / (ak * 1e-3) / 1e9, "unit": "GB/s",
                          "peak": _hbm_peak(), "frac": p["main_bytes"] / (ak * 1e-3) / 1e9 / _hbm_peak(),
                          "algorithmic_bytes_per_launch": p["main_bytes"]}}
+        # Band-loop adjoint: band-dependent wx (wx[n1] = wx + U[-0.25, 0.25]),
+        # every band walked per element.
+        import dataclasses
+        shift = torch.rand(g.number_bands, dtype=torch.float64, device=d.wx_array.device,
+                           generator=torch.Generator(device=d.wx_array.device).manual_seed(5)) * 0.5 - 0.25
+        db = dataclasses.replace(d, wx_array=(torch.as_tensor(g.wx_array, device=d.wx_array.device)[None, :]
+                                              + shift[:, None]).contiguous(), wx_band_stride=3)
+        bgw.noflagOCC_solver_backward(db, gcot, stream=sh, flags=bgw.FLAG_PROFILE)
+        bms = []
+        for _ in range(2):
+            bgw.noflagOCC_solver_backward(db, gcot, stream=sh, flags=bgw.FLAG_PROFILE)
+            bms.append(bgw.last_profile()["main_kernel_ms"])
+        extra["gpp_adjoint"]["bandloop"] = {
+            "kernel": bgw.last_profile()["main_kernel"], "kernel_ms": statistics.mean(bms),
+            "wx": "band-dependent (stride 3)",
+            "fp64_ops_per_term": 18,
+            "fp64_pipe_frac": 18 * 3 * g.number_bands * g.ngpown * g.ncouls / (statistics.mean(bms) * 1e-3)
+            / (dfma_peak * 1e12 / 2)}
+        del db
         if rank == 0 and not args.no_cpu:
             from oracle.oracle import Oracle
             rw, ri, rd = Oracle().gpp_backward(g, gcot)

@@ -253,7 +253,7 @@ def gpp_sigma(inp: GppInputs, nvband=None, *, want_ach=True, want_asx=True, prec
 
 
 def noflagOCC_solver_backward(inp: GppInputs, grad_achtemp, *, want_wtilde=True, want_I_eps=True,
-                              want_domega=True, stream=None, flags=0, pole_guard=0.0):
+                              want_domega=True, stream=None, flags=0, pole_guard=0.0, algorithm="auto"):
     """Adjoint of noflagOCC_solver.  grad_achtemp: 3 complex cotangents
     (dL/dRe + i dL/dIm of each achtemp entry).  Returns (grad_wtilde,
     grad_I_eps, dachtemp_domega) -- complex arrays [ngpown][ncouls],
@@ -273,7 +273,7 @@ def noflagOCC_solver_backward(inp: GppInputs, grad_achtemp, *, want_wtilde=True,
         gw = torch.zeros((P, G), dtype=torch.complex128, device=dev) if want_wtilde else None
         gi = torch.zeros((P, G), dtype=torch.complex128, device=dev) if want_I_eps else None
         dw = torch.zeros(3, dtype=torch.complex128, device=dev) if want_domega else None
-    o = make_options(mem, "fp64", "auto", inp.wx_band_stride, stream=_stream_handle(inp, stream), flags=flags,
+    o = make_options(mem, "fp64", algorithm, inp.wx_band_stride, stream=_stream_handle(inp, stream), flags=flags,
                      pole_guard=pole_guard)
     st = lib.bgw_noflagOCC_solver_backward(inp.number_bands, P, G, _ptr(inp.inv_igp_index), _ptr(inp.indinv),
                                            len(inp.indinv), _ptr(inp.wx_array), _ptr(inp.wtilde_array),

@@ -28,6 +28,12 @@ int gpp_sigma_factored_enqueue(CallEnv *env, int64_t nb, int64_t nv, int64_t P, 
                                const double2 *am, const double2 *an, const double2 *ie, const double *vc,
                                double *ach_dev, double *asx_dev);
 
+int gpp_adjoint_bandloop_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *inv,
+                                 const int32_t *indinv, int64_t indinv_len, const double *wx, int64_t wx_stride,
+                                 const double2 *wt, const double2 *am, const double2 *an, const double2 *ie,
+                                 const double *vc, const double2 *gcot, double2 *grad_wt, double2 *grad_ie,
+                                 double *domega);
+
 int gpp_adjoint_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *inv, const int32_t *indinv,
                         int64_t indinv_len, const double *wx, const double2 *wt, const double2 *am,
                         const double2 *an, const double2 *ie, const double *vc, const double2 *gcot,
@@ -207,14 +213,18 @@ extern "C" int bgw_noflagOCC_solver_backward(int64_t number_bands, int64_t ngpow
   Call c(opt);
   if (c.st != BGW_OK) return c.st;
   CallEnv *env = &c.env;
-  if (env->opt.wx_band_stride != 0) return BGW_ERR_UNSUPPORTED;  // factored adjoint only
-  if (env->opt.pole_guard > 0.0) return BGW_ERR_UNSUPPORTED;      // no near-pole cut-off
+  if (env->opt.pole_guard > 0.0) return BGW_ERR_UNSUPPORTED;  // no near-pole cut-off
+  const int64_t stride = env->opt.wx_band_stride;
+  if (stride != 0 && stride < 3) return BGW_ERR_INVALID_ARG;
+  // The factored adjoint needs a band-independent wx; the band loop takes any.
+  const bool bandloop = stride != 0 || env->opt.gpp_algorithm == BGW_GPP_BANDLOOP;
+  const size_t wx_n = stride == 0 ? 3 : (size_t)(nb > 0 ? (nb - 1) * stride + 3 : 3);
   const void *inv = nullptr, *ind = nullptr, *wx = nullptr, *wt = nullptr, *am = nullptr, *an = nullptr,
              *ie = nullptr, *vc = nullptr, *gc = nullptr;
   const size_t pg = (size_t)P * (size_t)G * 16, ng = (size_t)nb * (size_t)G * 16;
   BGW_TRY(stage_input(env, SLOT_IN0, inv_igp_index, sizeof(int32_t) * (size_t)P, &inv));
   BGW_TRY(stage_input(env, SLOT_IN1, indinv, sizeof(int32_t) * (size_t)indinv_len, &ind));
-  BGW_TRY(stage_input(env, SLOT_IN2, wx_array, sizeof(double) * 3, &wx));
+  BGW_TRY(stage_input(env, SLOT_IN2, wx_array, sizeof(double) * wx_n, &wx));
   BGW_TRY(stage_input(env, SLOT_IN3, wtilde_array, pg, &wt));
   BGW_TRY(stage_input(env, SLOT_IN4, aqsmtemp, ng, &am));
   BGW_TRY(stage_input(env, SLOT_IN5, aqsntemp, ng, &an));
@@ -239,19 +249,26 @@ extern "C" int bgw_noflagOCC_solver_backward(int64_t number_bands, int64_t ngpow
   } else if (((uintptr_t)grad_wtilde | (uintptr_t)grad_I_eps) & 15u) {
     return BGW_ERR_INVALID_ARG;
   }
-  BGW_TRY(gpp_adjoint_enqueue(env, nb, P, G, (const int32_t *)inv, (const int32_t *)ind, indinv_len,
-                              (const double *)wx, (const double2 *)wt, (const double2 *)am, (const double2 *)an,
-                              (const double2 *)ie, (const double *)vc, (const double2 *)gc, (double2 *)d_gw,
-                              (double2 *)d_gi, d_dw));
+  if (bandloop)
+    BGW_TRY(gpp_adjoint_bandloop_enqueue(env, nb, P, G, (const int32_t *)inv, (const int32_t *)ind, indinv_len,
+                                         (const double *)wx, stride, (const double2 *)wt, (const double2 *)am,
+                                         (const double2 *)an, (const double2 *)ie, (const double *)vc,
+                                         (const double2 *)gc, (double2 *)d_gw, (double2 *)d_gi, d_dw));
+  else
+    BGW_TRY(gpp_adjoint_enqueue(env, nb, P, G, (const int32_t *)inv, (const int32_t *)ind, indinv_len,
+                                (const double *)wx, (const double2 *)wt, (const double2 *)am, (const double2 *)an,
+                                (const double2 *)ie, (const double *)vc, (const double2 *)gc, (double2 *)d_gw,
+                                (double2 *)d_gi, d_dw));
   if (env->host) {
     if (grad_wtilde) BGW_CUDA_TRY(cudaMemcpyAsync(grad_wtilde, d_gw, pg, cudaMemcpyDeviceToHost, env->stream));
     if (grad_I_eps) BGW_CUDA_TRY(cudaMemcpyAsync(grad_I_eps, d_gi, pg, cudaMemcpyDeviceToHost, env->stream));
     if (dachtemp_domega)
       BGW_CUDA_TRY(cudaMemcpyAsync(dachtemp_domega, d_dw, sizeof(double) * 6, cudaMemcpyDeviceToHost, env->stream));
   }
-  // Algorithmic flops: per (G', G, frequency) element the quotient (as the
-  // forward) plus 4 complex products; 21 + 24 = 45.
-  env->prof.flops = 45.0 * 3.0 * (double)P * (double)G;
+  // Algorithmic flops: per (G', G, frequency) element (factored) or per
+  // (band, G', G, frequency) term (band loop) the quotient (as the forward)
+  // plus 4 complex products; 21 + 24 = 45.
+  env->prof.flops = 45.0 * 3.0 * (double)P * (double)G * (bandloop ? (double)nb : 1.0);
   return finish_call(env);
 }
 

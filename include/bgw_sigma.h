@@ -142,9 +142,14 @@ int bgw_noflagOCC_solver(int64_t number_bands, int64_t ngpown, int64_t ncouls,
  *   grad_wtilde [ngpown][ncouls] complex (includes wtilde[p][igp] inside
  *                                         sch_store1), may be NULL
  *   grad_I_eps  [ngpown][ncouls] complex, may be NULL
- *   dachtemp_domega [3] complex: d achtemp[iw] / d wx[iw], may be NULL
+ *   dachtemp_domega [3] complex: d achtemp[iw] / d omega for a common
+ *                   shift omega of wx[.][iw] (every band's), may be NULL
  * Quotients are recomputed, nothing of size bands x G' x G is stored.
- * Requires the band-independent wx (wx_band_stride 0).  Same arguments as
+ * Band-independent wx (wx_band_stride 0) with gpp_algorithm AUTO or
+ * FACTORED: the factored form, HBM-bound.  A band-dependent wx
+ * (wx_band_stride >= 3, wx_array [number_bands][stride]) or BANDLOOP: the
+ * band-loop form, which walks every band per element (FP64-pipe bound).
+ * FP64 only; pole_guard > 0 returns BGW_ERR_UNSUPPORTED.  Same arguments as
  * the forward otherwise. */
 int bgw_noflagOCC_solver_backward(int64_t number_bands, int64_t ngpown,
                                   int64_t ncouls, const int32_t *inv_igp_index,

@@ -95,12 +95,11 @@ static void gpp_quot(double wx, const double *wt, const double *ie, ld *qr,
  * wx is read as wx[n1 * wx_band_stride + iw]; stride 0 is the reference
  * (wx_array has no band index, gpp.cpp:239).  achtemp receives 3 complex
  * values (6 doubles).  Cost O(nb * P * G * 3): small sizes only. */
-int orc_gpp_direct(long nb, long P, long G, const int *inv_igp_index,
-                   const int *indinv, long indinv_len, const double *wx,
-                   long wx_band_stride, const double *wtilde,
-                   const double *aqsm, const double *aqsn,
-                   const double *I_eps, const double *vcoul,
-                   double *achtemp) {
+static int gpp_direct_ld(long nb, long P, long G, const int *inv_igp_index,
+                         const int *indinv, long indinv_len, const double *wx,
+                         long wx_band_stride, const double *wtilde,
+                         const double *aqsm, const double *aqsn,
+                         const double *I_eps, const double *vcoul, ld *out) {
   if (nb < 0 || P < 0 || G <= 0 || wx_band_stride < 0) return -1;
   long *igp = (long *)malloc(sizeof(long) * (size_t)(P > 0 ? P : 1));
   ld *part = (ld *)calloc((size_t)(nb > 0 ? nb : 1) * 6, sizeof(ld));
@@ -132,9 +131,34 @@ int orc_gpp_direct(long nb, long P, long G, const int *inv_igp_index,
   ld tot[6] = {0, 0, 0, 0, 0, 0};
   for (long n1 = 0; n1 < nb; ++n1)
     for (int k = 0; k < 6; ++k) tot[k] += part[6 * n1 + k];
-  for (int k = 0; k < 6; ++k) achtemp[k] = (double)tot[k];
+  for (int k = 0; k < 6; ++k) out[k] = tot[k];
   free(igp); free(part);
   return 0;
+}
+
+int orc_gpp_direct(long nb, long P, long G, const int *inv_igp_index,
+                   const int *indinv, long indinv_len, const double *wx,
+                   long wx_band_stride, const double *wtilde,
+                   const double *aqsm, const double *aqsn,
+                   const double *I_eps, const double *vcoul,
+                   double *achtemp) {
+  ld out[6];
+  const int st = gpp_direct_ld(nb, P, G, inv_igp_index, indinv, indinv_len, wx, wx_band_stride, wtilde, aqsm,
+                               aqsn, I_eps, vcoul, out);
+  if (st) return st;
+  for (int k = 0; k < 6; ++k) achtemp[k] = (double)out[k];
+  return 0;
+}
+
+/* The same sum with long-double outputs (finite differences of the band-
+ * dependent form). */
+int orc_gpp_direct_ld(long nb, long P, long G, const int *inv_igp_index,
+                      const int *indinv, long indinv_len, const double *wx,
+                      long wx_band_stride, const double *wtilde,
+                      const double *aqsm, const double *aqsn,
+                      const double *I_eps, const double *vcoul, ld *out) {
+  return gpp_direct_ld(nb, P, G, inv_igp_index, indinv, indinv_len, wx, wx_band_stride, wtilde, aqsm, aqsn,
+                       I_eps, vcoul, out);
 }
 
 /* Screened exchange (SX, the GPP `flagOCC` branch) -- NOT in the reference,
@@ -668,6 +692,107 @@ int orc_gpp_backward(long nb, long P, long G, const int *inv_igp_index,
   }
   free(igp); free(part);
   return 0;
+}
+
+/* Band-loop form of the same gradient for a band-dependent wx
+ * (wx[n1 * wx_band_stride + iw]; stride 0 is the reference's shared triple):
+ * nothing is factored over bands.  With s(n1, p) = C(n1, p) wtilde[p][igp],
+ * C(n1, p) = conj(aqsm[n1][igp]) aqsn[n1][igp] 0.5 vcoul[igp] and
+ * q = 1 / (wx[n1][iw] - wtilde[p][ig]):
+ *   dSigma_iw/dI_eps[p][ig]  = A_iw = sum_n1 s q
+ *   dSigma_iw/dwtilde[p][ig] = I_eps B_iw,  B_iw = sum_n1 s q^2
+ *                              (+ D_iw(p) = sum_ig I_eps sum_n1 C q at ig = igp)
+ *   dSigma_iw/domega         = - sum_{p, ig} I_eps B_iw
+ * and the gradients follow as in orc_gpp_backward.  Cost O(nb P G 3):
+ * small sizes only. */
+int orc_gpp_backward_direct(long nb, long P, long G, const int *inv_igp_index,
+                            const int *indinv, long indinv_len, const double *wx,
+                            long wx_band_stride, const double *wtilde,
+                            const double *aqsm, const double *aqsn,
+                            const double *I_eps, const double *vcoul,
+                            const double *gcot, double *grad_wt, double *grad_ie,
+                            double *domega) {
+  if (nb < 0 || P < 0 || G <= 0 || wx_band_stride < 0) return -1;
+  long *igp = (long *)malloc(sizeof(long) * (size_t)(P > 0 ? P : 1));
+  ld *part = (ld *)calloc((size_t)(P > 0 ? P : 1) * 6, sizeof(ld));
+  if (!igp || !part) { free(igp); free(part); return -1; }
+  if (resolve_igp(P, G, inv_igp_index, indinv, indinv_len, igp)) {
+    free(igp); free(part); return -1;
+  }
+  ld cgr[3], cgi[3];
+  for (int iw = 0; iw < 3; ++iw) { cgr[iw] = gcot[2 * iw]; cgi[iw] = -(ld)gcot[2 * iw + 1]; }
+  int bad = 0;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (long p = 0; p < P; ++p) {
+    const long g = igp[p];
+    ld *C = (ld *)malloc(sizeof(ld) * 2 * (size_t)(nb > 0 ? nb : 1));
+    if (!C) { bad = 1; continue; }
+    for (long n1 = 0; n1 < nb; ++n1) {
+      ld ar = aqsm[2 * (n1 * G + g)], ai = -(ld)aqsm[2 * (n1 * G + g) + 1];
+      ld br = aqsn[2 * (n1 * G + g)], bi = aqsn[2 * (n1 * G + g) + 1];
+      ld v = 0.5L * (ld)vcoul[g];
+      C[2 * n1] = (ar * br - ai * bi) * v;
+      C[2 * n1 + 1] = (ar * bi + ai * br) * v;
+    }
+    const ld wgr = wtilde[2 * (p * G + g)], wgi = wtilde[2 * (p * G + g) + 1];
+    ld Dr[3] = {0, 0, 0}, Di[3] = {0, 0, 0}, Wr[3] = {0, 0, 0}, Wi[3] = {0, 0, 0};
+    ld diag_r = 0, diag_i = 0;  /* conj-free value of the (p, igp) entry */
+    for (long ig = 0; ig < G; ++ig) {
+      const ld wr = wtilde[2 * (p * G + ig)], wi = wtilde[2 * (p * G + ig) + 1];
+      const ld er = I_eps[2 * (p * G + ig)], ei = I_eps[2 * (p * G + ig) + 1];
+      ld hIr = 0, hIi = 0, hWr = 0, hWi = 0;
+      for (int iw = 0; iw < 3; ++iw) {
+        ld Apr = 0, Api = 0, Bpr = 0, Bpi = 0;  /* sum_n1 C q, sum_n1 C q^2 */
+        for (long n1 = 0; n1 < nb; ++n1) {
+          const ld dr = (ld)wx[n1 * wx_band_stride + iw] - wr, di = -wi;
+          const ld den = dr * dr + di * di;
+          const ld qr = dr / den, qi = -di / den;
+          const ld q2r = qr * qr - qi * qi, q2i = 2.0L * qr * qi;
+          const ld cr = C[2 * n1], ci = C[2 * n1 + 1];
+          Apr += cr * qr - ci * qi;  Api += cr * qi + ci * qr;
+          Bpr += cr * q2r - ci * q2i; Bpi += cr * q2i + ci * q2r;
+        }
+        /* A = wtilde[p][igp] A', I B = I wtilde[p][igp] B' */
+        const ld Ar = wgr * Apr - wgi * Api, Ai = wgr * Api + wgi * Apr;
+        const ld Br = wgr * Bpr - wgi * Bpi, Bi = wgr * Bpi + wgi * Bpr;
+        const ld ibr = er * Br - ei * Bi, ibi = er * Bi + ei * Br;
+        Dr[iw] += er * Apr - ei * Api;  Di[iw] += er * Api + ei * Apr;
+        Wr[iw] += ibr; Wi[iw] += ibi;
+        hIr += cgr[iw] * Ar - cgi[iw] * Ai;   hIi += cgr[iw] * Ai + cgi[iw] * Ar;
+        hWr += cgr[iw] * ibr - cgi[iw] * ibi; hWi += cgr[iw] * ibi + cgi[iw] * ibr;
+      }
+      if (grad_ie) {
+        grad_ie[2 * (p * G + ig)] = (double)hIr;
+        grad_ie[2 * (p * G + ig) + 1] = (double)(-hIi);
+      }
+      if (grad_wt) {
+        grad_wt[2 * (p * G + ig)] = (double)hWr;
+        grad_wt[2 * (p * G + ig) + 1] = (double)(-hWi);
+      }
+      if (ig == g) { diag_r = hWr; diag_i = hWi; }
+    }
+    if (grad_wt) {
+      for (int iw = 0; iw < 3; ++iw) {
+        diag_r += cgr[iw] * Dr[iw] - cgi[iw] * Di[iw];
+        diag_i += cgr[iw] * Di[iw] + cgi[iw] * Dr[iw];
+      }
+      grad_wt[2 * (p * G + g)] = (double)diag_r;
+      grad_wt[2 * (p * G + g) + 1] = (double)(-diag_i);
+    }
+    for (int iw = 0; iw < 3; ++iw) {
+      part[6 * p + 2 * iw] = -Wr[iw];
+      part[6 * p + 2 * iw + 1] = -Wi[iw];
+    }
+    free(C);
+  }
+  if (!bad && domega) {
+    ld tot[6] = {0, 0, 0, 0, 0, 0};
+    for (long p = 0; p < P; ++p)
+      for (int k = 0; k < 6; ++k) tot[k] += part[6 * p + k];
+    for (int k = 0; k < 6; ++k) domega[k] = (double)tot[k];
+  }
+  free(igp); free(part);
+  return bad ? -1 : 0;
 }
 
 /* orc_gpp_factored with long-double outputs (6 values), for finite

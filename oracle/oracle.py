@@ -58,7 +58,9 @@ class Oracle:
                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(_D), ctypes.POINTER(_D)]
         lib.orc_compute_fact.restype = None
         lib.orc_gpp_backward.argtypes = [_L, _L, _L, _P, _P, _L, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]
+        lib.orc_gpp_backward_direct.argtypes = [_L, _L, _L, _P, _P, _L, _P, _L, _P, _P, _P, _P, _P, _P, _P, _P, _P]
         lib.orc_gpp_factored_ld.argtypes = [_L, _L, _L, _P, _P, _L, _P, _P, _P, _P, _P, _P, _P]
+        lib.orc_gpp_direct_ld.argtypes = [_L, _L, _L, _P, _P, _L, _P, _L, _P, _P, _P, _P, _P, _P]
         lib.orc_ff_achs.argtypes = [_L, _L, _L, _L, _P, _P, _L, _P, _P, _P, _P, _P]
         lib.orc_ff_asx.argtypes = [_L, _L, _L, _L, _L, _D, _D, _D, _P, _P, _P, _P, _L, _P, _P, _P, _P, _P, _P]
         lib.orc_ff_cor.argtypes = [_L, _L, _L, _L, _L, _L, _D, _D, _P, _P, _P, _P, _L, _P, _P, _P, _P, _P, _P]
@@ -106,6 +108,18 @@ class Oracle:
             raise ValueError("oracle rejected the GPP inputs")
         return out
 
+    def gpp_direct_ld(self, g) -> np.ndarray:
+        """Band-loop GPP sum (any wx_band_stride) with long-double outputs:
+        6 np.longdouble (re, im per iw)."""
+        out = np.zeros(6, dtype=np.longdouble)
+        st = self.lib.orc_gpp_direct_ld(g.number_bands, g.ngpown, g.ncouls, _p(g.inv_igp_index), _p(g.indinv),
+                                        len(g.indinv), _p(g.wx_array), g.wx_band_stride, _p(g.wtilde_array),
+                                        _p(g.aqsmtemp), _p(g.aqsntemp), _p(g.I_eps_array), _p(g.vcoul),
+                                        out.ctypes.data)
+        if st != 0:
+            raise ValueError("oracle rejected the GPP inputs")
+        return out
+
     def gpp_ld(self, g) -> np.ndarray:
         """Factored GPP sum with long-double outputs: 6 np.longdouble (re, im per iw)."""
         out = np.zeros(6, dtype=np.longdouble)
@@ -116,12 +130,22 @@ class Oracle:
             raise ValueError("oracle rejected the GPP inputs")
         return out
 
-    def gpp_backward(self, g, gcot):
-        """(grad_wtilde [P][G], grad_I_eps [P][G], dachtemp/domega [3]) complex128."""
+    def gpp_backward(self, g, gcot, direct: bool = False):
+        """(grad_wtilde [P][G], grad_I_eps [P][G], dachtemp/domega [3]) complex128.
+        direct (implied by a band-dependent wx): the band-loop form,
+        O(nb P G), small sizes only."""
         gc = np.ascontiguousarray(np.asarray(gcot, dtype=np.complex128).reshape(3))
         gw = np.zeros((g.ngpown, g.ncouls), np.complex128)
         gi = np.zeros((g.ngpown, g.ncouls), np.complex128)
         dw = np.zeros(3, np.complex128)
+        if direct or g.wx_band_stride:
+            st = self.lib.orc_gpp_backward_direct(g.number_bands, g.ngpown, g.ncouls, _p(g.inv_igp_index),
+                                                  _p(g.indinv), len(g.indinv), _p(g.wx_array), g.wx_band_stride,
+                                                  _p(g.wtilde_array), _p(g.aqsmtemp), _p(g.aqsntemp),
+                                                  _p(g.I_eps_array), _p(g.vcoul), _p(gc), _p(gw), _p(gi), _p(dw))
+            if st != 0:
+                raise ValueError("oracle rejected the GPP inputs")
+            return gw, gi, dw
         st = self.lib.orc_gpp_backward(g.number_bands, g.ngpown, g.ncouls, _p(g.inv_igp_index), _p(g.indinv),
                                        len(g.indinv), _p(g.wx_array), _p(g.wtilde_array), _p(g.aqsmtemp),
                                        _p(g.aqsntemp), _p(g.I_eps_array), _p(g.vcoul), _p(gc), _p(gw), _p(gi),

@@ -5,7 +5,9 @@ CPU: the long-double oracle gradient is pinned by central finite differences
 of I_eps_array (including every (p, igp) entry, where wtilde also enters
 sch_store1) and on the frequencies.
 GPU: the CUDA adjoint matches the oracle gradient to 1e-12 (normwise) at small
-and benchmark sizes, and central differences to 1e-6 on 64 seeded entries."""
+and benchmark sizes, and central differences to 1e-6 on 64 seeded entries.
+A band-dependent wx takes the band-loop adjoint, checked the same way against
+the oracle's band-loop gradient and long-double band-loop forward."""
 from __future__ import annotations
 
 import numpy as np
@@ -18,8 +20,14 @@ H = 1e-6
 FD_RTOL = 1e-6
 
 
+def _fwd(orc, g):
+    """Long-double forward: factored for a shared wx, the band loop for a
+    band-dependent one."""
+    return orc.gpp_direct_ld(g) if g.wx_band_stride else orc.gpp_ld(g)
+
+
 def _loss(orc, g, gcot) -> np.longdouble:
-    s = orc.gpp_ld(g)
+    s = _fwd(orc, g)
     gc = np.asarray(gcot, dtype=np.complex128)
     return np.longdouble(sum(np.longdouble(gc[i].real) * s[2 * i] + np.longdouble(gc[i].imag) * s[2 * i + 1]
                              for i in range(3)))
@@ -53,16 +61,20 @@ def _fd(orc, g, gcot, name, p, ig):
 
 
 def _fd_domega(orc, g, gcot):
-    """d achtemp[iw] / d wx[iw] (complex) by central differences."""
+    """d achtemp[iw] / d omega (complex) by central differences, omega
+    shifting wx[iw] (every band's, for a band-dependent wx)."""
     wx0 = g.wx_array.copy()
+    col = (lambda iw: (slice(None), iw)) if g.wx_band_stride else (lambda iw: iw)
+    if g.wx_band_stride:
+        assert g.wx_band_stride == 3 and wx0.ndim == 2
     res = []
     for iw in range(3):
-        g.wx_array[:] = wx0
-        g.wx_array[iw] = wx0[iw] + H
-        sp = orc.gpp_ld(g)
-        g.wx_array[iw] = wx0[iw] - H
-        sm = orc.gpp_ld(g)
-        g.wx_array[:] = wx0
+        g.wx_array[...] = wx0
+        g.wx_array[col(iw)] = wx0[col(iw)] + H
+        sp = _fwd(orc, g)
+        g.wx_array[col(iw)] = wx0[col(iw)] - H
+        sm = _fwd(orc, g)
+        g.wx_array[...] = wx0
         den = np.longdouble(2 * H)
         res.append(complex(float((sp[2 * iw] - sm[2 * iw]) / den), float((sp[2 * iw + 1] - sm[2 * iw + 1]) / den)))
     return np.array(res)
@@ -85,6 +97,23 @@ def test_oracle_gradient_matches_finite_differences(oracle):
     gcot = rng.standard_normal(3) + 1j * rng.standard_normal(3)
     grads = oracle.gpp_backward(g, gcot)
     _check_fd(oracle, g, gcot, grads, _entries(g, 64, rng))
+
+
+def test_oracle_band_loop_gradient_matches_finite_differences(oracle):
+    """Band-dependent wx: the oracle's band-loop gradient against central
+    differences of its long-double band-loop forward."""
+    rng = np.random.default_rng(8)
+    g = I.gpp_seeded(8, 2, 256, 8, seed=43, wx_per_band=True)   # ngpown 32
+    gcot = rng.standard_normal(3) + 1j * rng.standard_normal(3)
+    grads = oracle.gpp_backward(g, gcot)
+    _check_fd(oracle, g, gcot, grads, _entries(g, 32, rng))
+
+
+def test_oracle_band_loop_gradient_equals_factored_for_shared_wx(oracle):
+    g = I.gpp_seeded(12, 2, 600, 6, seed=44)
+    gcot = np.array([0.3 - 1.1j, 0.7 + 0.2j, -0.4 + 0.9j])
+    for a, b in zip(oracle.gpp_backward(g, gcot), oracle.gpp_backward(g, gcot, direct=True)):
+        assert rel_err(b, a) < 1e-15
 
 
 def test_oracle_gradient_linear_in_cotangent(oracle):
@@ -145,9 +174,59 @@ def test_gpu_adjoint_benchmark_size(bgw, oracle, cuda):
     assert rel_err(dw, rd) < 1e-12
 
 
+# ----------------------------------------------- band-loop adjoint (GPU) --
+
 @pytest.mark.gpu
-def test_gpu_adjoint_rejects_band_dependent_wx(bgw, cuda):
-    g = I.gpp_seeded(8, 2, 256, 8, seed=3, wx_per_band=True)
-    with pytest.raises(bgw.BgwError) as e:
-        bgw.noflagOCC_solver_backward(g, [1, 0, 0])
-    assert e.value.status == -7
+@pytest.mark.parametrize("dims", [(16, 512, 8), (300, 1000, 10), (5, 777, 3)])
+def test_gpu_band_loop_adjoint_matches_oracle(bgw, oracle, cuda, dims):
+    """Band-dependent wx (the band-loop adjoint); 300 bands span two staged
+    band chunks, ncouls not a multiple of the 512-element item."""
+    rng = np.random.default_rng(dims[0])
+    g = I.gpp_seeded(dims[0], 2, dims[1], dims[2], seed=dims[0] + 5, wx_per_band=True)
+    gcot = rng.standard_normal(3) + 1j * rng.standard_normal(3)
+    got = bgw.noflagOCC_solver_backward(g, gcot)
+    ref = oracle.gpp_backward(g, gcot)
+    for a, b in zip(got, ref):
+        assert rel_err(a, b) < 1e-12
+
+
+@pytest.mark.gpu
+def test_gpu_band_loop_adjoint_finite_differences(bgw, oracle, cuda):
+    rng = np.random.default_rng(21)
+    g = I.gpp_seeded(8, 2, 256, 8, seed=22, wx_per_band=True)
+    gcot = rng.standard_normal(3) + 1j * rng.standard_normal(3)
+    grads = bgw.noflagOCC_solver_backward(g, gcot)
+    _check_fd(oracle, g, gcot, grads, _entries(g, 32, rng))
+
+
+@pytest.mark.gpu
+def test_gpu_band_loop_adjoint_equals_factored_for_shared_wx(bgw, cuda):
+    g = bgw.to_device(I.gpp_seeded(48, 2, 4096, 16, seed=23), cuda)
+    gcot = np.array([0.3 - 1.1j, 0.7 + 0.2j, -0.4 + 0.9j])
+    a = bgw.noflagOCC_solver_backward(g, gcot)
+    b = bgw.noflagOCC_solver_backward(g, gcot, algorithm="bandloop")
+    for x, y in zip(a, b):
+        assert rel_err(y.cpu().numpy(), x.cpu().numpy()) < 1e-12
+
+
+@pytest.mark.gpu
+def test_gpu_band_loop_adjoint_host_device_and_reruns(bgw, cuda):
+    g = I.gpp_seeded(20, 2, 2048, 16, seed=24, wx_per_band=True)
+    gcot = np.array([1 + 2j, -0.5j, 0.25])
+    h = bgw.noflagOCC_solver_backward(g, gcot)
+    d = bgw.noflagOCC_solver_backward(bgw.to_device(g, cuda), gcot)
+    for a, b in zip(h, d):
+        assert np.array_equal(a, b.cpu().numpy())
+    for a, b in zip(h, bgw.noflagOCC_solver_backward(g, gcot)):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.gpu
+def test_gpu_band_loop_adjoint_no_bands(bgw, cuda):
+    g = I.gpp_seeded(4, 2, 512, 8, seed=25, wx_per_band=True)
+    g.number_bands = 0
+    g.aqsmtemp = g.aqsmtemp[:0]
+    g.aqsntemp = g.aqsntemp[:0]
+    g.wx_array = np.ascontiguousarray(g.wx_array[:1])
+    gw, gi, dw = bgw.noflagOCC_solver_backward(g, [1, 1j, 0])
+    assert not gw.any() and not gi.any() and not dw.any()
