@@ -654,9 +654,12 @@ def run_only(args, local):
         dims = dict(GPP_DIMS)
         if args.bands:
             dims["number_bands"] = args.bands
-        d = bgw.to_device(I.gpp_seeded(**dims, seed=1234), dev)
-        if args.only == "gpp_adjoint":
+        per_band = args.only == "gpp_adjoint_bandloop"
+        d = bgw.to_device(I.gpp_seeded(**dims, seed=1234, wx_per_band=per_band), dev)
+        if args.only in ("gpp_adjoint", "gpp_adjoint_bandloop"):
             call = lambda: bgw.noflagOCC_solver_backward(d, [1, 1j, -1], flags=bgw.FLAG_PROFILE)  # noqa: E731
+        elif args.only == "gpp_sigma":
+            call = lambda: bgw.gpp_sigma(d, algorithm="factored", flags=bgw.FLAG_PROFILE)  # noqa: E731
         else:
             alg = "bandloop" if args.only == "gpp_mixed" else args.only.split("_")[1]
             prec = "mixed" if args.only == "gpp_mixed" else "fp64"
@@ -705,7 +708,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and oracle check")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-instances extra")
-    ap.add_argument("--only", choices=["gpp_bandloop", "gpp_mixed", "gpp_factored", "gpp_adjoint", "ff", "ff_mixed",
+    ap.add_argument("--only", choices=["gpp_bandloop", "gpp_mixed", "gpp_factored", "gpp_adjoint",
+                                       "gpp_adjoint_bandloop", "gpp_sigma", "ff", "ff_mixed",
                                        "ff_mixed_all", "ff_per_iw", "ff_per_iw_mixed"],
                     default=None,
                     help="diagnostic: time one kernel path only (for profilers)")
