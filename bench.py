@@ -611,9 +611,11 @@ def bench_batched(bgw, I, dev, sh, stream, dfma_peak, rank):
         torch.cuda.synchronize(dev)
         return ev0.elapsed_time(ev1) / 1e3 / reps
 
-    for alg in ("bandloop", "factored"):
+    fp64_band_out = None
+    for key, alg, prec in (("bandloop", "bandloop", "fp64"), ("factored", "factored", "fp64"),
+                           ("bandloop_mixed", "bandloop", "mixed")):
         t0 = time.perf_counter()
-        b = bgw.GppBatch(insts, algorithm=alg, stream=sh)
+        b = bgw.GppBatch(insts, algorithm=alg, precision=prec, stream=sh)
         create_s = time.perf_counter() - t0
         t_batch = timed(lambda: b.execute(stream=sh), 3)
         batch_out = b.execute(stream=sh).cpu().numpy().copy()
@@ -621,20 +623,24 @@ def bench_batched(bgw, I, dev, sh, stream, dfma_peak, rank):
 
         def seq():
             for k, g in enumerate(insts):
-                r = bgw.noflagOCC_solver(g, algorithm=alg, stream=sh)
+                r = bgw.noflagOCC_solver(g, algorithm=alg, precision=prec, stream=sh)
                 seq_out[k] = r.cpu().numpy()
         t_seq = timed(seq, 1)
         err = max(rel_err(batch_out[k], seq_out[k]) for k in range(len(insts)))
         entry = {"batched_s": t_batch, "sequential_s": t_seq, "speedup_vs_sequential": t_seq / t_batch,
                  "instances_per_s": len(insts) / t_batch, "tuned": b.info(), "create_s": create_s,
                  "max_rel_diff_vs_sequential": err}
-        if alg == "bandloop":
+        if key == "bandloop":
+            fp64_band_out = batch_out
             entry["roofline"] = {"bound": "fp64", "achieved": flops / t_batch / 1e12, "unit": "TFLOP/s",
                                  "peak": dfma_peak, "frac": flops / t_batch / 1e12 / dfma_peak}
-        else:
+        elif key == "factored":
             entry["roofline"] = {"bound": "hbm", "achieved": stream_bytes / t_batch / 1e9, "unit": "GB/s",
                                  "peak": _hbm_peak(), "frac": stream_bytes / t_batch / 1e9 / _hbm_peak()}
-        res[alg] = entry
+        else:
+            entry["speedup_vs_fp64_batched"] = res["bandloop"]["batched_s"] / t_batch
+            entry["max_rel_err_vs_fp64"] = max(rel_err(batch_out[k], fp64_band_out[k]) for k in range(len(insts)))
+        res[key] = entry
         b.close()
     del insts
     return res
