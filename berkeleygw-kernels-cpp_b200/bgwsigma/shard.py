@@ -7,8 +7,9 @@ kernels is over independent (band, G', G) terms, so rank r evaluates the
 contiguous column block [p0, p1) with its own GPU -- its slice of
 inv_igp_index and of the [ngpown][...] arrays (wtilde_array, I_eps_array,
 or I_epsR/I_epsA[:, p0:p1, :]) plus the replicated band arrays -- and the
-only exchange is the gather of the partial outputs: 3 complex (GPP) or
-1 + 2 nfreqeval complex (FF) per rank.  The partials are all-gathered and
+only exchange is the gather of the partial outputs: 3 complex (GPP
+achtemp; 6 with the screened exchange) or 1 + 2 nfreqeval complex (FF) per
+rank.  The partials are all-gathered and
 summed in rank order, so the result is bitwise reproducible for a given
 world size.  One process per GPU; `torch.distributed` (NCCL on GPUs, gloo
 on CPU) carries the gather.
@@ -78,6 +79,24 @@ def gpp_sharded(inp: GppInputs, world: int, rank: int, group=None,
             else noflagOCC_solver
     local = np.asarray(compute(shard), dtype=np.complex128)
     return gather_sum(local, group)
+
+
+def gpp_sigma_sharded(inp: GppInputs, world: int, rank: int, group=None,
+                      compute: Optional[Callable] = None, device=None):
+    """(achtemp[3], asxtemp[3]) of the whole problem (bgw_gpp_sigma: the
+    Coulomb-hole sum and the occupied bands' screened exchange, both sums
+    over G' columns); this rank computes its column block with `compute`
+    (default: the GPU library), which returns the two outputs."""
+    shard = gpp_shard(inp, world, rank)
+    if compute is None:
+        from . import gpp_sigma, to_device
+
+        def compute(s):
+            src = to_device(s, device) if device is not None else s
+            return tuple(np.asarray(o.cpu().numpy() if hasattr(o, "cpu") else o) for o in gpp_sigma(src))
+    ach, asx = compute(shard)
+    tot = gather_sum(np.concatenate([np.atleast_1d(ach), np.atleast_1d(asx)]), group)
+    return tot[:3], tot[3:6]
 
 
 def ff_sharded(inp: FFInputs, world: int, rank: int, group=None,

@@ -52,7 +52,9 @@ def _worker(rank, world, port, result_path):
     got_g = S.gpp_sharded(g, world, rank, compute=orc.gpp)
     f = I.ff_seeded(20, 4, 600, 45, 6, 3, seed=32)       # ngpown 45 (odd split)
     got_f = S.ff_sharded(f, world, rank, compute=lambda s: (orc.achs(s), orc.asx(s), orc.cor(s)))
-    np.save(f"{result_path}.{rank}.npy", np.concatenate([got_g, [got_f[0]], got_f[1], got_f[2]]))
+    got_s = S.gpp_sigma_sharded(g, world, rank, compute=lambda s: (orc.gpp(s), orc.gpp_sx(s)))
+    np.save(f"{result_path}.{rank}.npy",
+            np.concatenate([got_g, [got_f[0]], got_f[1], got_f[2], got_s[0], got_s[1]]))
     dist.barrier()
     dist.destroy_process_group()
 
@@ -66,7 +68,8 @@ def test_two_rank_gather_matches_whole_problem(tmp_path, oracle):
     assert np.array_equal(r0, r1)                           # every rank holds the same total
     g = I.gpp_seeded(16, 2, 1000, 10, seed=31)
     f = I.ff_seeded(20, 4, 600, 45, 6, 3, seed=32)
-    want = np.concatenate([oracle.gpp(g), [oracle.achs(f)], oracle.asx(f), oracle.cor(f)])
+    want = np.concatenate([oracle.gpp(g), [oracle.achs(f)], oracle.asx(f), oracle.cor(f), oracle.gpp(g),
+                           oracle.gpp_sx(g)])
     err = np.max(np.abs(r0 - want) / np.maximum(np.abs(want), 1e-300))
     assert err < 1e-13, err
 
