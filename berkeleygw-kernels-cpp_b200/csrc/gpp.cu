@@ -110,13 +110,15 @@ __global__ void gpp_wx_kernel(int nb, const double *__restrict__ wx, long long s
 // a frequency x:
 //   dr  = x - wr,  |wdiff|^2 = dr^2 + wi^2,
 //   conj(wdiff) * I_eps = (dr*Ir + a) + i (dr*Ii + b).
-// Elements per thread: FP64 4, mixed 8 (the FP32 quotients are cheap, so a
-// longer run per band amortises the band combination).  Threads per CTA:
-// FP64 256 (2 CTAs per SM); mixed 384 (one CTA per SM: 12 warps, as many as
-// its registers allow, to hide the MUFU latency; 223 KB of staging).
+// Elements per thread: 8 (a longer run per band amortises the per-band
+// combination with sch_store1: FP64 53.6 ms at 8 vs 58.0 ms at 4 and 55.8 ms
+// at 6 on the 512-band benchmark).  Threads per CTA: FP64 256 (one CTA per
+// SM: 210 registers, 153 KB of staging); mixed 384 (one CTA per SM: 12
+// warps, as many as its registers allow, to hide the MUFU latency; 223 KB of
+// staging).
 template <bool MIXED>
 struct BandCfg {
-  static constexpr int kE = MIXED ? 8 : 4;
+  static constexpr int kE = 8;
   static constexpr int kNT = MIXED ? 384 : kThreads;
   static constexpr int kCH = kNT * kE;
 };
@@ -145,7 +147,7 @@ struct BandSmem {
 // (near_elems / near_sweep), which also applies the cut-off (guard_d =
 // sqrt(guard2)); GUARD is not used.
 template <int BCH, bool MIXED, bool GUARD>
-__global__ void __launch_bounds__(BandCfg<MIXED>::kNT, MIXED ? 1 : 2)
+__global__ void __launch_bounds__(BandCfg<MIXED>::kNT, 1)
     gpp_bandloop_kernel(int nb, int G, long long items, int nchunks_g, const double2 *__restrict__ wtilde,
                         const double2 *__restrict__ ieps, const double2 *__restrict__ st,
                         const double4 *__restrict__ wx4, double *__restrict__ partials, int *status,
