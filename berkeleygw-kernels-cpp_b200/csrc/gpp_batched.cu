@@ -15,8 +15,9 @@
 //
 // Tuning.  The elements per thread (kE) and with it the chunk width and the
 // occupancy are chosen per batch by timing the candidate kernels on a sample
-// prefix of the work list (bgw_gpp_batch_create); choices are cached per
-// batch signature for the process.
+// prefix of the work list (bgw_gpp_batch_create): FP64 8, 4 or 2 (8: one CTA
+// per SM, the per-band combination amortised over 24 terms), mixed 8 or 4;
+// choices are cached per batch signature for the process.
 #include <algorithm>
 #include <climits>
 #include <cmath>
@@ -142,7 +143,7 @@ __device__ __forceinline__ void flush(double (&acc_r)[3], double (&acc_i)[3], do
 // Band loop over this CTA's range [range[b], range[b+1]) of the global item
 // list.  Steps are (item, band chunk); step s+1 is staged while s computes.
 template <int BCH, int KE, bool MIXED>
-__global__ void __launch_bounds__(kBThreads, (MIXED && KE == 8) ? 1 : 2)
+__global__ void __launch_bounds__(kBThreads, KE == 8 ? 1 : 2)
     batch_bandloop_kernel(const BatchInst *__restrict__ inst, int n, const long long *__restrict__ range,
                           int max_seg, double *__restrict__ partials, int *status) {
   constexpr int kCH = kBThreads * KE;
@@ -474,8 +475,10 @@ int enqueue_batch(bgw_gpp_batch *B, cudaStream_t s) {
       else launch_band<4, true>(s, B->grid, B->smem, B->d_inst, ninst, B->d_range, B->max_seg, B->d_partials,
                                 B->d_status);
     } else {
-      if (B->ke == 4) launch_band<4, false>(s, B->grid, B->smem, B->d_inst, ninst, B->d_range, B->max_seg,
+      if (B->ke == 8) launch_band<8, false>(s, B->grid, B->smem, B->d_inst, ninst, B->d_range, B->max_seg,
                                            B->d_partials, B->d_status);
+      else if (B->ke == 4) launch_band<4, false>(s, B->grid, B->smem, B->d_inst, ninst, B->d_range, B->max_seg,
+                                                B->d_partials, B->d_status);
       else launch_band<2, false>(s, B->grid, B->smem, B->d_inst, ninst, B->d_range, B->max_seg, B->d_partials,
                                  B->d_status);
     }
@@ -576,10 +579,11 @@ extern "C" int bgw_gpp_batch_create(const bgw_gpp_instance *instances, int64_t n
     BGW_TRY((band_variant<4, true>(&b)));
     cands = {a, b};
   } else {
-    Variant a, b;
-    BGW_TRY((band_variant<4, false>(&a)));
-    BGW_TRY((band_variant<2, false>(&b)));
-    cands = {a, b};
+    Variant a, b, c;
+    BGW_TRY((band_variant<8, false>(&a)));
+    BGW_TRY((band_variant<4, false>(&b)));
+    BGW_TRY((band_variant<2, false>(&c)));
+    cands = {a, b, c};
   }
 
   bgw_gpp_batch *B = new (std::nothrow) bgw_gpp_batch();
