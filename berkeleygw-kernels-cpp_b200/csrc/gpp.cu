@@ -20,6 +20,7 @@
 // single-block kernel sums the partials in a fixed order.  No atomics, so
 // reruns are bitwise identical.
 #include <algorithm>
+#include <numeric>
 #include <cstdio>
 #include <cstring>
 #include <functional>
@@ -569,6 +570,32 @@ int gpp_run_host(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *
   RowChunks rc;
   rc.n = (int)std::max<int64_t>(1, std::min<int64_t>(RowChunks::kMax, P / 64));
   for (int c = 0; c <= rc.n; ++c) rc.p0[c] = P * c / rc.n;
+  // With the band loop each chunk is one launch of `ctas` persistent CTAs
+  // over rows x ng items (ng G chunks per row).  Chunks whose item count is a
+  // multiple of ctas end without a partial last round: 1638 rows, 16 G chunks
+  // and 148 CTAs give 15 chunks of 111 rows (12 full rounds each) instead of
+  // 16 of about 102 rows (11.07 rounds each, an 8 % tail per launch).
+  const bool factored = env->opt.gpp_algorithm == BGW_GPP_FACTORED ||
+                        (env->opt.gpp_algorithm == BGW_GPP_AUTO && wx_stride == 0 &&
+                         env->opt.precision == BGW_PRECISION_FP64);
+  if (!factored && rc.n > 1) {
+    const bool mixed = env->opt.precision == BGW_PRECISION_MIXED, guard = env->opt.pole_guard > 0.0;
+    int per_sm = 0;
+    if (mixed) BGW_TRY((bandloop_per_sm<256, true, false>(&per_sm)));
+    else if (guard) BGW_TRY((bandloop_per_sm<256, false, true>(&per_sm)));
+    else BGW_TRY((bandloop_per_sm<256, false, false>(&per_sm)));
+    const int64_t ctas = (int64_t)ws->sm_count * std::max(per_sm, 1);
+    const int64_t kch = mixed ? BandCfg<true>::kCH : BandCfg<false>::kCH;
+    const int64_t ng = std::max<int64_t>(1, (G + kch - 1) / kch);
+    const int64_t m = ctas / std::gcd(ng, ctas);  // rows per full round set
+    const int64_t even = (P + rc.n - 1) / rc.n;
+    const int64_t rows = std::max<int64_t>(1, (even + m / 2) / m) * m;
+    const int64_t n = (P + rows - 1) / rows;
+    if (n >= 2 && n <= RowChunks::kMax) {
+      rc.n = (int)n;
+      for (int c = 0; c <= rc.n; ++c) rc.p0[c] = std::min<int64_t>(P, (int64_t)c * rows);
+    }
+  }
   for (int c = 0; c < rc.n; ++c) rc.ready[c] = ws->chunk_ready[c];
   // Pageable wtilde / I_eps (the reference drivers' new[] buffers) are
   // staged through two page-locked slots filled by several host threads:
