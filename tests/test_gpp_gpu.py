@@ -85,6 +85,21 @@ def test_empty_bands_and_columns(bgw, cuda):
     assert np.all(bgw.noflagOCC_solver(g) == 0)
 
 
+@pytest.mark.parametrize("dims", [(0, 0, 512, 8), (5, 2, 64, 128)])   # no bands; no G' columns
+@pytest.mark.parametrize("algorithm,precision", [("bandloop", "fp64"), ("factored", "fp64"), ("bandloop", "mixed")])
+def test_empty_sums_every_path(bgw, cuda, dims, algorithm, precision):
+    """An empty sum is exactly zero on every path, host and device memory,
+    and in both outputs of bgw_gpp_sigma."""
+    g = I.gpp_seeded(*dims, seed=2)
+    for src in (g, bgw.to_device(g, cuda)):
+        out = bgw.noflagOCC_solver(src, algorithm=algorithm, precision=precision)
+        out = out.cpu().numpy() if hasattr(out, "cpu") else out
+        assert np.all(out == 0)
+        for o in bgw.gpp_sigma(src, algorithm=algorithm, precision=precision):
+            o = o.cpu().numpy() if hasattr(o, "cpu") else o
+            assert np.all(o == 0)
+
+
 def test_async_flag_with_device_status(bgw, oracle, cuda):
     import torch
     g = I.gpp_seeded(16, 2, 1024, 16, seed=8)
