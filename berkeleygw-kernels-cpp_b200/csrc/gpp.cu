@@ -591,7 +591,14 @@ int gpp_run_host(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *
     const int64_t even = (P + rc.n - 1) / rc.n;
     const int64_t rows = std::max<int64_t>(1, (even + m / 2) / m) * m;
     const int64_t n = (P + rows - 1) / rows;
-    if (n >= 2 && n <= RowChunks::kMax) {
+    // The first chunk is one round set (m rows): its copy is the part of the
+    // H2D transfer that no computation hides.
+    const int64_t n0 = rows > m ? 1 + (P - m + rows - 1) / rows : n;
+    if (rows > m && P > m && n0 >= 2 && n0 <= RowChunks::kMax) {
+      rc.n = (int)n0;
+      rc.p0[0] = 0;
+      for (int c = 1; c <= rc.n; ++c) rc.p0[c] = std::min<int64_t>(P, m + (int64_t)(c - 1) * rows);
+    } else if (n >= 2 && n <= RowChunks::kMax) {
       rc.n = (int)n;
       for (int c = 0; c <= rc.n; ++c) rc.p0[c] = std::min<int64_t>(P, (int64_t)c * rows);
     }
@@ -643,51 +650,75 @@ int gpp_run_host(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *
   BGW_TRY(copy_rows(0));
 
   // The kernels read aqsmtemp / aqsntemp / vcoul only at the columns
-  // igp(p) = indinv[inv_igp_index[p]]: those are gathered here into a
-  // page-locked buffer ([nb][P] complex twice, then P doubles), so nb*P
-  // instead of nb*G values cross PCIe before the first chunk can start.  An
+  // igp(p) = indinv[inv_igp_index[p]]: those are gathered into a page-locked
+  // buffer ([nb][P] complex twice, then P doubles), so nb*P instead of nb*G
+  // values cross PCIe.  With the band loop the gather and its copies go chunk
+  // by chunk (columns [p0[c], p0[c+1])), so chunk c's columns are gathered
+  // while the GPU works on chunk c-1 and chunk 0 waits only for its own.  An
   // out-of-range index gathers zeros; the device still resolves and checks
   // every index and reports BGW_ERR_INDEX as for device-memory inputs.
   double2 *g_am = static_cast<double2 *>(pinned), *g_an = g_am + nbp;
   double *g_vc = reinterpret_cast<double *>(g_an + nbp);
-  {
-    std::vector<int64_t> igp((size_t)P);
-    std::vector<int32_t> order;  // valid columns, ascending igp (monotone reads per band row)
-    order.reserve((size_t)P);
-    for (int64_t p = 0; p < P; ++p) {
-      const int32_t a = inv[p];
-      const int64_t g = (a >= 0 && (int64_t)a < indinv_len) ? (int64_t)indinv[a] : -1;
-      igp[(size_t)p] = (g >= 0 && g < G) ? g : -1;
-      g_vc[p] = igp[(size_t)p] >= 0 ? vc[igp[(size_t)p]] : 0.0;
+  std::vector<int64_t> igp((size_t)P);
+  std::vector<int32_t> order;  // valid columns by chunk, ascending igp within a chunk
+  std::vector<size_t> order_at((size_t)rc.n + 1, 0);
+  order.reserve((size_t)P);
+  for (int64_t p = 0; p < P; ++p) {
+    const int32_t a = inv[p];
+    const int64_t g = (a >= 0 && (int64_t)a < indinv_len) ? (int64_t)indinv[a] : -1;
+    igp[(size_t)p] = (g >= 0 && g < G) ? g : -1;
+    g_vc[p] = igp[(size_t)p] >= 0 ? vc[igp[(size_t)p]] : 0.0;
+    if (igp[(size_t)p] < 0)
+      for (int64_t n1 = 0; n1 < nb; ++n1) g_am[(size_t)n1 * P + p] = g_an[(size_t)n1 * P + p] = double2{0.0, 0.0};
+  }
+  for (int c = 0; c < rc.n; ++c) {
+    order_at[(size_t)c] = order.size();
+    for (int64_t p = rc.p0[c]; p < rc.p0[c + 1]; ++p)
       if (igp[(size_t)p] >= 0) order.push_back((int32_t)p);
-      else
-        for (int64_t n1 = 0; n1 < nb; ++n1) g_am[(size_t)n1 * P + p] = g_an[(size_t)n1 * P + p] = double2{0.0, 0.0};
-    }
-    std::sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return igp[(size_t)x] < igp[(size_t)y]; });
-    const double2 *am2 = reinterpret_cast<const double2 *>(am), *an2 = reinterpret_cast<const double2 *>(an);
+    std::sort(order.begin() + (std::ptrdiff_t)order_at[(size_t)c], order.end(),
+              [&](int32_t x, int32_t y) { return igp[(size_t)x] < igp[(size_t)y]; });
+  }
+  order_at[(size_t)rc.n] = order.size();
+  const double2 *am2 = reinterpret_cast<const double2 *>(am), *an2 = reinterpret_cast<const double2 *>(an);
+  // Gathers the columns of chunks [c0, c1) and queues their copies.
+  auto gather_cols = [&](int c0, int c1) -> int {
+    const int64_t p0 = rc.p0[c0], w = rc.p0[c1] - p0;
+    if (w <= 0) return BGW_OK;
+    const int32_t *ob = order.data() + order_at[(size_t)c0], *oe = order.data() + order_at[(size_t)c1];
     auto gather = [&](int64_t b0, int64_t b1) {
       for (int64_t n1 = b0; n1 < b1; ++n1) {
         const double2 *ra = am2 + (size_t)n1 * G, *rn = an2 + (size_t)n1 * G;
         double2 *da = g_am + (size_t)n1 * P, *dn = g_an + (size_t)n1 * P;
-        for (int32_t p : order) {
-          const int64_t g = igp[(size_t)p];
-          da[p] = ra[g];
-          dn[p] = rn[g];
+        for (const int32_t *q = ob; q < oe; ++q) {
+          const int64_t g = igp[(size_t)*q];
+          da[*q] = ra[g];
+          dn[*q] = rn[g];
         }
       }
     };
-    parallel_ranges(nb, host_threads((int64_t)nbp, 65536), gather);
-  }
+    parallel_ranges(nb, host_threads(nb * w, 4096), gather);  // scattered reads: many threads
+    if (nb > 0) {
+      const size_t pitch = (size_t)P * 16;
+      BGW_CUDA_TRY(cudaMemcpy2DAsync(static_cast<double2 *>(d_am) + p0, pitch, g_am + p0, pitch, (size_t)w * 16,
+                                     (size_t)nb, cudaMemcpyHostToDevice, cs));
+      BGW_CUDA_TRY(cudaMemcpy2DAsync(static_cast<double2 *>(d_an) + p0, pitch, g_an + p0, pitch, (size_t)w * 16,
+                                     (size_t)nb, cudaMemcpyHostToDevice, cs));
+    }
+    BGW_TRY(h2d(static_cast<double *>(d_vc) + p0, g_vc + p0, sizeof(double) * (size_t)w));
+    return BGW_OK;
+  };
   BGW_TRY(h2d(d_inv, inv, sizeof(int32_t) * (size_t)P));
   BGW_TRY(h2d(d_ind, indinv, sizeof(int32_t) * (size_t)indinv_len));
   BGW_TRY(h2d(d_wx, wx, sizeof(double) * wx_n));
-  BGW_TRY(h2d(d_vc, g_vc, sizeof(double) * (size_t)P));
-  BGW_TRY(h2d(d_am, g_am, nbp * 16));
-  BGW_TRY(h2d(d_an, g_an, nbp * 16));
+  // Band loop: chunk by chunk, hidden behind the previous chunk's kernels.
+  // Factored (PCIe-bound, little GPU work per chunk): all columns at once, so
+  // the host's staging of later chunks is not held up by gathers.
+  BGW_TRY(gather_cols(0, factored ? rc.n : 1));
   BGW_CUDA_TRY(cudaEventRecord(ws->chunk_ready[0], cs));  // chunk 0 and the per-band inputs
   auto issue = [&](int c) -> int {
     if (c == 0) return BGW_OK;
     BGW_TRY(copy_rows(c));
+    if (!factored) BGW_TRY(gather_cols(c, c + 1));
     BGW_CUDA_TRY(cudaEventRecord(ws->chunk_ready[c], cs));
     return BGW_OK;
   };
