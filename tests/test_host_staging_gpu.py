@@ -50,3 +50,21 @@ def test_gpp_host_gather_reports_bad_index(bgw, cuda):
     assert e.value.status == -2
     ok = I.gpp_seeded(8, 2, 4096, 20, seed=33)
     assert np.all(np.isfinite(bgw.noflagOCC_solver(ok)))
+
+
+@pytest.mark.parametrize("algorithm", ["bandloop", "factored"])
+def test_gpp_repeated_and_unordered_columns(bgw, oracle, cuda, algorithm):
+    """inv_igp_index with repeated entries (several G' columns reading the same
+    igp) and in no particular order: the host path gathers each column per
+    row chunk; host, device and the oracle agree."""
+    g = I.gpp_seeded(40, 2, 8192, 20, seed=34)                 # ngpown 409: several row chunks
+    rng = np.random.default_rng(35)
+    inv = g.inv_igp_index.copy()
+    inv[::7] = inv[3]                                          # collisions
+    g.inv_igp_index = np.ascontiguousarray(rng.permutation(inv).astype(np.int32))
+    ref = oracle.gpp(g)
+    host = bgw.noflagOCC_solver(g, algorithm=algorithm)
+    assert rel_err(host, ref) < FP64_RTOL
+    assert np.array_equal(host, bgw.noflagOCC_solver(bgw.to_pinned(g), algorithm=algorithm))
+    dev = bgw.noflagOCC_solver(bgw.to_device(g, cuda), algorithm=algorithm).cpu().numpy()
+    assert rel_err(dev, ref) < FP64_RTOL
