@@ -573,8 +573,9 @@ int gpp_run_host(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *
   // With the band loop each chunk is one launch of `ctas` persistent CTAs
   // over rows x ng items (ng G chunks per row).  Chunks whose item count is a
   // multiple of ctas end without a partial last round: 1638 rows, 16 G chunks
-  // and 148 CTAs give 15 chunks of 111 rows (12 full rounds each) instead of
-  // 16 of about 102 rows (11.07 rounds each, an 8 % tail per launch).
+  // and 148 CTAs give a first chunk of 37 rows (4 rounds) and 15 of 111 rows
+  // (12 rounds each; the last one shorter) instead of 16 of about 102 rows
+  // (11.07 rounds each, an 8 % tail per launch).
   const bool factored = env->opt.gpp_algorithm == BGW_GPP_FACTORED ||
                         (env->opt.gpp_algorithm == BGW_GPP_AUTO && wx_stride == 0 &&
                          env->opt.precision == BGW_PRECISION_FP64);
