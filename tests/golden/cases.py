@@ -40,3 +40,13 @@ FF_CASES = {
     "ff_many_occupied": lambda: I.ff_seeded(40, 20, 640, 70, 6, 2, seed=13),
     "ff_fact_edges": _ff_edges,
 }
+
+
+# The benchmark sizes (outputs only: the reference's own results at full size,
+# regenerated by make_golden.py --full).
+FULL_GPP_CASES = {
+    "gpp_benchmark": lambda: I.gpp_seeded(512, 2, 32768, 20, seed=1234),
+}
+FULL_FF_CASES = {
+    "ff_benchmark": lambda: I.ff_seeded(512, 2, 8192, 512, 15, 10, seed=1234),
+}

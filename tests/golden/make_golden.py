@@ -3,11 +3,15 @@
 Run where the reference tree is available (it builds oracle/_ref/libbgwref.so
 from the reference sources, see oracle/Makefile):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # every small case
+    python tests/golden/make_golden.py --full   # adds the benchmark sizes
 
 For every case of tests/golden/cases.py it records the input fingerprint,
 the reference build's outputs (OpenMP 3.0 build, all host threads) and the
-long-double oracle's outputs.  Complex numbers are stored as [re, im].
+long-double oracle's outputs.  The benchmark-size cases (FULL_*_CASES) keep
+the fingerprint and the reference's outputs only, in the "full" section,
+which --full fills in place without recomputing the rest.  Complex numbers
+are stored as [re, im].
 """
 from __future__ import annotations
 
@@ -24,7 +28,7 @@ sys.path.insert(0, str(HERE))
 import numpy as np  # noqa: E402
 
 from bgwsigma import inputs as I  # noqa: E402
-from cases import FF_CASES, GPP_CASES  # noqa: E402
+from cases import FF_CASES, FULL_FF_CASES, FULL_GPP_CASES, GPP_CASES  # noqa: E402
 from oracle.oracle import Oracle, Reference, build_oracle  # noqa: E402
 
 
@@ -77,9 +81,41 @@ def main():
     out["reference_symbols"] = sorted(syms)
     out["compute_fact_grid"] = grid.tolist()
     out["compute_fact"] = probes
+    prev = HERE / "golden.json"
+    if prev.exists():  # keep the benchmark-size section (make_golden.py --full)
+        old = json.loads(prev.read_text())
+        if "full" in old:
+            out["full"] = old["full"]
     (HERE / "golden.json").write_text(json.dumps(out, indent=1) + "\n")
     print("wrote", HERE / "golden.json")
 
 
+def main_full():
+    build_oracle(ref=True)
+    ref = Reference()
+    path = HERE / "golden.json"
+    out = json.loads(path.read_text())
+    full = {"reference_threads": ref.num_threads()}
+    for name, mk in FULL_GPP_CASES.items():
+        g = mk()
+        full[name] = {"fingerprint": I.fingerprint(g), "dims": [g.number_bands, g.ngpown, g.ncouls],
+                      "reference": c2l(ref.gpp(g))}
+        print(name, full[name]["reference"][0])
+        del g
+    for name, mk in FULL_FF_CASES.items():
+        f = mk()
+        full[name] = {"fingerprint": I.fingerprint(f),
+                      "dims": [f.number_bands, f.nvband, f.ncouls, f.ngpown, f.nFreq, f.nfreqeval],
+                      "reference": {"achs": c2l(ref.achs(f)), "asx": c2l(ref.asx(f)), "cor": c2l(ref.cor(f))}}
+        print(name, full[name]["reference"]["achs"][0])
+        del f
+    out["full"] = full
+    path.write_text(json.dumps(out, indent=1) + "\n")
+    print("wrote", path)
+
+
 if __name__ == "__main__":
-    main()
+    if "--full" in sys.argv[1:]:
+        main_full()
+    else:
+        main()

@@ -79,7 +79,7 @@ def test_zero_eval_points_and_no_valence(bgw, oracle, cuda):
     assert rel_err(achs, oracle.achs(f)) < FP64_RTOL
 
 
-def test_benchmark_size(bgw, oracle, cuda):
+def test_benchmark_size(bgw, oracle, golden, cuda):
     """512 bands, nvband 2, ncouls 8192, ngpown 512, nFreq 15, nfreqeval 10."""
     f = I.ff_seeded(512, 2, 8192, 512, 15, 10, seed=1234)
     d = bgw.to_device(f, cuda)
@@ -87,3 +87,8 @@ def test_benchmark_size(bgw, oracle, cuda):
     assert rel_err(achs.cpu().numpy(), oracle.achs(f)) < FP64_RTOL
     assert rel_err(asx.cpu().numpy(), oracle.asx(f)) < FP64_RTOL
     assert rel_err(cor.cpu().numpy(), oracle.cor(f)) < FP64_RTOL
+    # ... and against the reference build's own outputs on the same inputs.
+    ref = golden["full"]["ff_benchmark"]["reference"]
+    assert rel_err(achs.cpu().numpy(), l2c(ref["achs"])) < FP64_RTOL
+    assert rel_err(asx.cpu().numpy()[:f.nfreqeval], l2c(ref["asx"])) < FP64_RTOL
+    assert rel_err(cor.cpu().numpy()[:f.nfreqeval], l2c(ref["cor"])) < FP64_RTOL

@@ -116,7 +116,7 @@ def test_async_flag_with_device_status(bgw, oracle, cuda):
 
 
 @pytest.mark.parametrize("algorithm", ["bandloop", "factored"])
-def test_benchmark_size(bgw, oracle, cuda, algorithm):
+def test_benchmark_size(bgw, oracle, golden, cuda, algorithm):
     """512 bands, ncouls 32768, nodes_per_group 20 (ngpown 1638): 2.7e10
     (band, G', G) terms, checked against the long-double oracle's factored
     evaluation (exact algebraic identity for the band-independent wx)."""
@@ -124,6 +124,8 @@ def test_benchmark_size(bgw, oracle, cuda, algorithm):
     ref = oracle.gpp(g, factored=True)
     got = bgw.noflagOCC_solver(bgw.to_device(g, cuda), algorithm=algorithm).cpu().numpy()
     assert rel_err(got, ref) < FP64_RTOL
+    # ... and against the reference build's own output on the same inputs.
+    assert rel_err(got, l2c(golden["full"]["gpp_benchmark"]["reference"])) < FP64_RTOL
 
 
 def test_launch_counter_advances(bgw, cuda):

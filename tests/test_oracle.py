@@ -8,7 +8,7 @@ import pytest
 from conftest import FP64_RTOL, l2c, rel_err
 
 from bgwsigma import inputs as I
-from cases import FF_CASES, GPP_CASES
+from cases import FF_CASES, FULL_FF_CASES, FULL_GPP_CASES, GPP_CASES
 
 
 @pytest.mark.parametrize("name", sorted(GPP_CASES))
@@ -209,3 +209,22 @@ def test_gpp_sx_pole_guard_partial_fractions(oracle, delta):
     pf = -(oracle.gpp(_occupied(g, 3, False), pole_guard=delta) + oracle.gpp(_occupied(g, 3, True), pole_guard=delta))
     assert rel_err(sx, pf) < 1e-13
     assert rel_err(oracle.gpp_sx(g, factored=True, pole_guard=delta), sx) < 1e-13
+
+
+# ------------------------------------------------------ benchmark sizes --
+# The reference build's own outputs at the benchmark sizes (golden "full",
+# make_golden.py --full): the inputs regenerate bit for bit, and the oracle
+# matches the reference there too.
+
+def test_full_size_oracle_vs_reference(golden, oracle):
+    full = golden["full"]
+    g = FULL_GPP_CASES["gpp_benchmark"]()
+    assert I.fingerprint(g) == full["gpp_benchmark"]["fingerprint"]
+    assert rel_err(oracle.gpp(g, factored=True), l2c(full["gpp_benchmark"]["reference"])) < FP64_RTOL
+    del g
+    f = FULL_FF_CASES["ff_benchmark"]()
+    assert I.fingerprint(f) == full["ff_benchmark"]["fingerprint"]
+    ref = full["ff_benchmark"]["reference"]
+    assert rel_err(oracle.achs(f), l2c(ref["achs"])) < FP64_RTOL
+    assert rel_err(oracle.asx(f), l2c(ref["asx"])) < FP64_RTOL
+    assert rel_err(oracle.cor(f), l2c(ref["cor"])) < FP64_RTOL
