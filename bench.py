@@ -539,6 +539,16 @@ def run_ours(args, world, rank, local):
         from oracle.oracle import Oracle
         ref = Oracle().gpp(g, factored=True)
         extra["rel_err_vs_oracle"] = {"bandloop": rel_err(result, ref), "e2e_host_path": rel_err(host_res, ref)}
+        # The reference build's own output on these inputs (seed 1234), stored
+        # with their fingerprint by tests/golden/make_golden.py --full.
+        try:
+            full = json.loads((REPO / "tests" / "golden" / "golden.json").read_text())["full"]["gpp_benchmark"]
+            if full["fingerprint"] == I.fingerprint(g):
+                want = np.array([complex(*z) for z in full["reference"]])
+                extra["rel_err_vs_reference"] = {"bandloop": rel_err(result, want),
+                                                 "e2e_host_path": rel_err(host_res, want)}
+        except (OSError, KeyError, ValueError):
+            pass
         if world == 1:
             per_sigma, desc = cpu_reference_gpp(g, args.cpu_seconds)
             cpu_baseline = {"value": per_sigma, "unit": "s", "cores": desc["cores"], "kind": desc["kind"],
