@@ -32,7 +32,9 @@
 extern "C" {
 #endif
 
-#define BGW_SIGMA_ABI_VERSION 1
+/* 2: bgw_options gained pole_guard (bgw_options_init writes the whole
+ * current struct, so it must be given a struct of this header's size). */
+#define BGW_SIGMA_ABI_VERSION 2
 
 typedef enum bgw_status {
   BGW_OK = 0,
@@ -101,8 +103,9 @@ typedef struct bgw_options {
  * of the two partial fractions 1/(wx - wtilde) and 1/(-wx - wtilde).
  * Supported by bgw_noflagOCC_solver and bgw_gpp_sigma; the adjoint and the
  * batched calls return BGW_ERR_UNSUPPORTED for delta > 0; the FF calls
- * ignore it.  Callers compiled against an older, shorter bgw_options (a
- * smaller struct_size) get delta = 0. */
+ * ignore it.  An entry point given an older, shorter bgw_options (a smaller
+ * struct_size, filled by the caller) reads only that many bytes and uses
+ * delta = 0; bgw_options_init itself always writes the current layout. */
 
 /* Fills *opt with the defaults (host memory, FP64, AUTO, stride 0,
  * current device, default stream, synchronous). */
