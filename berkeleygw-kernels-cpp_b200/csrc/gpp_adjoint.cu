@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2)
 // (Dpart) and added to grad_wtilde[p][igp] by gpp_adjoint_diag_kernel, in a
 // fixed order.
 constexpr int kAbBCH = 256;
-constexpr int kAbE = 2;
+constexpr int kAbE = 4;  // one CTA per SM (255 registers): 98 ms vs 102 ms at 2 and 101 ms at 3
 constexpr int kAbChunk = kAdjThreads * kAbE;
 
 // C(n1, p) table [P][nb], wtilde[p][igp] and igp(p) (-1 if out of range).
@@ -264,7 +264,7 @@ struct AdjBandSmem {
   double red[(kAdjThreads / 32) * 6];
 };
 
-__global__ void __launch_bounds__(kAdjThreads, 2)
+__global__ void __launch_bounds__(kAdjThreads, 1)
     gpp_adjoint_bandloop_kernel(int nb, int G, long long items, int nchunk_e, const double2 *__restrict__ wtilde,
                                 const double2 *__restrict__ ieps, const double2 *__restrict__ Ctab,
                                 const double2 *__restrict__ wpp, const double4 *__restrict__ wx4,
