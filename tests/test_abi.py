@@ -153,3 +153,40 @@ def test_gpp_sigma_nvband_validation(bgw):
         with pytest.raises(bgw.BgwError) as e:
             bgw.gpp_sigma(g, nvband=nv)
         assert e.value.status == -1
+
+
+C_CALLER = r"""
+#include <stdio.h>
+#include <string.h>
+#include "bgw_sigma.h"
+
+int main(void) {
+  bgw_options opt;
+  bgw_options_init(&opt);
+  if (opt.struct_size != (int32_t)sizeof(bgw_options) || bgw_abi_version() != BGW_SIGMA_ABI_VERSION) return 10;
+  int32_t inv[1] = {0}, indinv[3] = {0, 1, 1};
+  double wx[3] = {1.0, 2.0, 3.0}, wt[4] = {0.5, 0.0, 0.7, 0.0}, am[4] = {1, 0, 1, 0}, an[4] = {1, 0, 1, 0};
+  double ie[4] = {0.1, 0.0, 0.2, 0.0}, vc[2] = {1.0, 0.5}, ach[6], asx[6];
+  int st = bgw_noflagOCC_solver(1, 1, 2, inv, indinv, 3, wx, wt, am, an, ie, vc, ach, &opt);
+  int st2 = bgw_gpp_sigma(1, 1, 1, 2, inv, indinv, 3, wx, wt, am, an, ie, vc, ach, asx, &opt);
+  printf("%d %d %s\n", st, st2, bgw_status_string(st));
+  return 0;
+}
+"""
+
+
+def test_plain_c_caller_builds_and_links(bgw, tmp_path):
+    """The header is plain C (C99) and a C program links against the library
+    and calls it; without a GPU every compute call returns BGW_ERR_NO_DEVICE."""
+    import torch
+    src = tmp_path / "caller.c"
+    src.write_text(C_CALLER)
+    exe = tmp_path / "caller"
+    libdir = bgw.lib_path().parent
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", str(HEADER.parent), str(src), "-o", str(exe),
+                    "-L", str(libdir), "-lbgwsigma", f"-Wl,-rpath,{libdir}"], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    if torch.cuda.is_available():
+        assert out[0] == "0" and out[1] == "0"
+    else:
+        assert out[0] == "-5" and out[1] == "-5"
