@@ -42,7 +42,8 @@ EXPORTS = ("bgw_options_init", "bgw_noflagOCC_solver", "bgw_achsDtemp_Kernel", "
            "bgw_achDtemp_cor_Kernel", "bgw_ff_sigma", "bgw_status_string", "bgw_abi_version",
            "bgw_launch_count", "bgw_measure_fp64_peak", "bgw_release_workspace", "bgw_last_profile",
            "bgw_noflagOCC_solver_noalloc", "bgw_noflagOCC_solver_backward", "bgw_gpp_batch_create",
-           "bgw_gpp_batch_execute", "bgw_gpp_batch_info", "bgw_gpp_batch_destroy")
+           "bgw_gpp_batch_execute", "bgw_gpp_batch_info", "bgw_gpp_batch_destroy", "bgw_gpp_sigma",
+           "bgw_debug_inject_stall")
 
 
 class BgwError(RuntimeError):
@@ -106,6 +107,7 @@ def load(build_if_needed: bool = True) -> ctypes.CDLL:
     lib.bgw_launch_count.restype = ctypes.c_uint64
     lib.bgw_measure_fp64_peak.argtypes = [ctypes.c_int32, ctypes.POINTER(_D), ctypes.POINTER(_D)]
     lib.bgw_release_workspace.argtypes = [ctypes.c_int32]
+    lib.bgw_debug_inject_stall.argtypes = [ctypes.c_int64]
     lib.bgw_last_profile.argtypes = [ctypes.POINTER(Profile)]
     opt = ctypes.POINTER(Options)
     lib.bgw_noflagOCC_solver.argtypes = [_I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, opt]
@@ -142,6 +144,13 @@ def measure_fp64_peak(device: int = -1):
     a, b = _D(), _D()
     _check("bgw_measure_fp64_peak", load().bgw_measure_fp64_peak(device, ctypes.byref(a), ctypes.byref(b)))
     return a.value, b.value
+
+
+def inject_stall(step: int = -1):
+    """Test hook of the timeout path (bgw_debug_inject_stall): the staged
+    kernels launched from now on let the wait of CTA-local step `step` run
+    out, and their calls raise BgwError(BGW_ERR_TIMEOUT); -1 turns it off."""
+    _check("bgw_debug_inject_stall", load().bgw_debug_inject_stall(int(step)))
 
 
 def last_profile() -> dict:

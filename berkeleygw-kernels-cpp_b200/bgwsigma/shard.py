@@ -24,6 +24,10 @@ import numpy as np
 from .inputs import FFInputs, GppInputs
 
 
+def _on_host(inp) -> bool:
+    return isinstance(inp.wtilde_array if isinstance(inp, GppInputs) else inp.aqsmtemp, np.ndarray)
+
+
 def column_range(ngpown: int, world: int, rank: int) -> tuple[int, int]:
     """Contiguous, balanced block of G' columns owned by `rank`."""
     base, extra = divmod(ngpown, world)
@@ -31,34 +35,46 @@ def column_range(ngpown: int, world: int, rank: int) -> tuple[int, int]:
     return p0, p0 + base + (1 if rank < extra else 0)
 
 
+def _rows(a, p0: int, p1: int, axis: int = 0):
+    """Contiguous copy of rows [p0, p1) along `axis` (numpy or torch)."""
+    sl = (slice(None),) * axis + (slice(p0, p1),)
+    if type(a).__module__.startswith("torch"):
+        return a[sl].contiguous()
+    return np.ascontiguousarray(a[sl])
+
+
 def gpp_shard(inp: GppInputs, world: int, rank: int) -> GppInputs:
     p0, p1 = column_range(inp.ngpown, world, rank)
     return dataclasses.replace(
         inp, ngpown=p1 - p0,
-        inv_igp_index=np.ascontiguousarray(inp.inv_igp_index[p0:p1]),
-        wtilde_array=np.ascontiguousarray(inp.wtilde_array[p0:p1]),
-        I_eps_array=np.ascontiguousarray(inp.I_eps_array[p0:p1]))
+        inv_igp_index=_rows(inp.inv_igp_index, p0, p1),
+        wtilde_array=_rows(inp.wtilde_array, p0, p1),
+        I_eps_array=_rows(inp.I_eps_array, p0, p1))
 
 
 def ff_shard(inp: FFInputs, world: int, rank: int) -> FFInputs:
     p0, p1 = column_range(inp.ngpown, world, rank)
     return dataclasses.replace(
         inp, ngpown=p1 - p0,
-        inv_igp_index=np.ascontiguousarray(inp.inv_igp_index[p0:p1]),
-        I_epsR_array=np.ascontiguousarray(inp.I_epsR_array[:, p0:p1, :]),
-        I_epsA_array=np.ascontiguousarray(inp.I_epsA_array[:, p0:p1, :]))
+        inv_igp_index=_rows(inp.inv_igp_index, p0, p1),
+        I_epsR_array=_rows(inp.I_epsR_array, p0, p1, axis=1),
+        I_epsA_array=_rows(inp.I_epsA_array, p0, p1, axis=1))
 
 
-def gather_sum(partial: np.ndarray, group=None, device=None) -> np.ndarray:
+def gather_sum(partial, group=None, device=None) -> np.ndarray:
     """All-gathers a complex partial from every rank and sums it in rank
     order (fixed order: bitwise reproducible).  Collective: every rank of
-    `group` must call it."""
+    `group` must call it.  `partial`: numpy array or torch tensor.  Under
+    NCCL the gather runs on `device` (default: the current CUDA device),
+    since NCCL takes CUDA tensors only; under gloo it runs on the host."""
     import torch
     import torch.distributed as dist
+    if type(partial).__module__.startswith("torch"):
+        partial = partial.detach().cpu().numpy()
     x = np.ascontiguousarray(np.atleast_1d(partial).astype(np.complex128)).view(np.float64)
     t = torch.from_numpy(x.copy())
-    if device is not None:
-        t = t.to(device)
+    if dist.get_backend(group) == "nccl":
+        t = t.to(device if device is not None else torch.device("cuda", torch.cuda.current_device()))
     world = dist.get_world_size(group)
     parts = [torch.empty_like(t) for _ in range(world)]
     dist.all_gather(parts, t, group=group)
@@ -75,10 +91,13 @@ def gpp_sharded(inp: GppInputs, world: int, rank: int, group=None,
     shard = gpp_shard(inp, world, rank)
     if compute is None:
         from . import noflagOCC_solver, to_device
-        compute = (lambda s: noflagOCC_solver(to_device(s, device)).cpu().numpy()) if device is not None \
-            else noflagOCC_solver
-    local = np.asarray(compute(shard), dtype=np.complex128)
-    return gather_sum(local, group)
+
+        def compute(s):
+            return noflagOCC_solver(to_device(s, device) if device is not None and _on_host(s) else s)
+    local = compute(shard)
+    if hasattr(local, "cpu"):
+        local = local.cpu().numpy()
+    return gather_sum(np.asarray(local, dtype=np.complex128), group, device)
 
 
 def gpp_sigma_sharded(inp: GppInputs, world: int, rank: int, group=None,
@@ -92,10 +111,10 @@ def gpp_sigma_sharded(inp: GppInputs, world: int, rank: int, group=None,
         from . import gpp_sigma, to_device
 
         def compute(s):
-            src = to_device(s, device) if device is not None else s
+            src = to_device(s, device) if device is not None and _on_host(s) else s
             return tuple(np.asarray(o.cpu().numpy() if hasattr(o, "cpu") else o) for o in gpp_sigma(src))
     ach, asx = compute(shard)
-    tot = gather_sum(np.concatenate([np.atleast_1d(ach), np.atleast_1d(asx)]), group)
+    tot = gather_sum(np.concatenate([np.atleast_1d(ach), np.atleast_1d(asx)]), group, device)
     return tot[:3], tot[3:6]
 
 
@@ -109,11 +128,11 @@ def ff_sharded(inp: FFInputs, world: int, rank: int, group=None,
         from . import ff_sigma, to_device
 
         def compute(s):
-            src = to_device(s, device) if device is not None else s
+            src = to_device(s, device) if device is not None and _on_host(s) else s
             out = ff_sigma(src)
             return tuple(np.asarray(o.cpu().numpy() if hasattr(o, "cpu") else o) for o in out)
     achs, asx, cor = compute(shard)
     E = inp.nfreqeval
     flat = np.concatenate([np.atleast_1d(achs)[:1], np.atleast_1d(asx)[:E], np.atleast_1d(cor)[:E]])
-    tot = gather_sum(flat, group)
+    tot = gather_sum(flat, group, device)
     return tot[0], tot[1:1 + E], tot[1 + E:1 + 2 * E]

@@ -210,4 +210,35 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
 // About 2 s at the B200's 1.965 GHz boost clock.
 constexpr long long kWaitCycles = 4000000000LL;
 
+// Stall injection (bgw_debug_inject_stall; tests of the timeout path).
+// Kernels that stage step j into buffer j & 1 of a double buffer take the
+// CTA-local step index at which to stall (-1: never).  At that step the
+// main-loop wait is made on `never`, an mbarrier no thread or copy ever
+// arrives on, with a short budget: it runs out, and the kernel takes the
+// same path as a real timeout (BGW_ERR_TIMEOUT, drain, exit).
+constexpr long long kStallCycles = 200000;  // ~0.1 ms
+
+// The main-loop wait of a double-buffered kernel for step j: phase
+// (j >> 1) & 1 of `bar` (the buffer's barrier), or the injected stall.
+__device__ __forceinline__ bool staged_wait(uint64_t *bar, long long j, long long stall, uint64_t *never) {
+  if (j == stall) return mbar_wait_bounded(never, 0, kStallCycles);
+  return mbar_wait_bounded(bar, (uint32_t)((j >> 1) & 1), kWaitCycles);
+}
+
+// After the wait for step j ran out: the copies still in flight are step
+// j's, on bar[j & 1] with phase parity (j >> 1) & 1, and, if it was issued,
+// step j + 1's, on bar[(j + 1) & 1] with parity ((j + 1) >> 1) & 1.  Both
+// are waited for with the full budget, so no bulk copy writes into the
+// CTA's shared memory after the CTA has exited.  (A wait for parity 0 on
+// both barriers would be wrong: when a barrier's outstanding phase is odd,
+// its completed parity-0 phase satisfies the wait at once.)
+__device__ __forceinline__ void drain_staged(uint64_t *bar0, uint64_t *bar1, long long j, bool next_issued) {
+  uint64_t *bar[2] = {bar0, bar1};
+  (void)mbar_wait_bounded(bar[j & 1], (uint32_t)((j >> 1) & 1), kWaitCycles);
+  if (next_issued) (void)mbar_wait_bounded(bar[(j + 1) & 1], (uint32_t)(((j + 1) >> 1) & 1), kWaitCycles);
+}
+
+// Host side: the stall step for kernels launched from now on (-1: off).
+long long stall_step();
+
 }  // namespace bgw

@@ -130,7 +130,7 @@ struct BandSmem {
   double2 ie[2][BandCfg<MIXED>::kCH];
   double2 st[2][BCH];
   double4 wx[2][BCH];
-  unsigned long long bar[2];
+  unsigned long long bar[3];  // [2]: never arrived on (stall injection)
   double red[(BandCfg<MIXED>::kNT / 32) * 6];
   double xr_lo[BandCfg<MIXED>::kNT / 32], xr_hi[BandCfg<MIXED>::kNT / 32];  // MIXED: chunk frequency range
   float4 xf[MIXED ? BCH : 1];                                                 // MIXED: FP32 frequency rows
@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(BandCfg<MIXED>::kNT, 1)
     gpp_bandloop_kernel(int nb, int G, long long items, int nchunks_g, const double2 *__restrict__ wtilde,
                         const double2 *__restrict__ ieps, const double2 *__restrict__ st,
                         const double4 *__restrict__ wx4, double *__restrict__ partials, int *status,
-                        double guard2, double guard_d) {
+                        double guard2, double guard_d, long long stall) {
   constexpr int kE = BandCfg<MIXED>::kE;
   constexpr int kCH = BandCfg<MIXED>::kCH;
   constexpr int kThreads = BandCfg<MIXED>::kNT;  // shadows the file-wide 256
@@ -169,6 +169,7 @@ __global__ void __launch_bounds__(BandCfg<MIXED>::kNT, 1)
   if (tid == 0) {
     mbar_init(reinterpret_cast<uint64_t *>(&sm.bar[0]), 1);
     mbar_init(reinterpret_cast<uint64_t *>(&sm.bar[1]), 1);
+    mbar_init(reinterpret_cast<uint64_t *>(&sm.bar[2]), 1);
     fence_mbar_init();
   }
   __syncthreads();
@@ -195,17 +196,22 @@ __global__ void __launch_bounds__(BandCfg<MIXED>::kNT, 1)
   double acc_r[3] = {0.0, 0.0, 0.0}, acc_i[3] = {0.0, 0.0, 0.0};
   double lo_r[3] = {0.0, 0.0, 0.0}, lo_i[3] = {0.0, 0.0, 0.0};  // TwoSum tails (MIXED)
   bool ok = true;
+  long long j_fail = 0;  // the step whose wait ran out
   if (tid == 0 && nsteps > 0) issue(0);
 
   for (long long j = 0; j < nsteps; ++j) {
     if (tid == 0 && j + 1 < nsteps) issue(j + 1);
     const int buf = (int)(j & 1);
-    if (!mbar_wait_bounded(reinterpret_cast<uint64_t *>(&sm.bar[buf]), (uint32_t)((j >> 1) & 1), kWaitCycles)) {
+    if (!staged_wait(reinterpret_cast<uint64_t *>(&sm.bar[buf]), j, stall,
+                     reinterpret_cast<uint64_t *>(&sm.bar[2]))) {
       raise_status(status, BGW_ERR_TIMEOUT, blockIdx.x);
       ok = false;
     }
     // Every thread must agree before leaving the loop.
-    if (__syncthreads_or(!ok)) break;
+    if (__syncthreads_or(!ok)) {
+      j_fail = j;
+      break;
+    }
 
     const long long item = blockIdx.x + (j / nbc) * (long long)gridDim.x;
     const int c = (int)(j % nbc);
@@ -230,10 +236,10 @@ __global__ void __launch_bounds__(BandCfg<MIXED>::kNT, 1)
     __syncthreads();  // buffer `buf` is free for step j + 2
   }
   if (!ok && tid == 0) {
-    // Let copies still in flight land before the CTA's shared memory is
-    // released (bounded as well).
-    (void)mbar_wait_bounded(reinterpret_cast<uint64_t *>(&sm.bar[0]), 0, kWaitCycles);
-    (void)mbar_wait_bounded(reinterpret_cast<uint64_t *>(&sm.bar[1]), 0, kWaitCycles);
+    // Copies still in flight (steps j_fail and j_fail + 1) land before the
+    // CTA's shared memory is released.
+    drain_staged(reinterpret_cast<uint64_t *>(&sm.bar[0]), reinterpret_cast<uint64_t *>(&sm.bar[1]), j_fail,
+                 j_fail + 1 < nsteps);
   }
 
   double v[6] = {acc_r[0] + lo_r[0], acc_i[0] + lo_i[0], acc_r[1] + lo_r[1],
@@ -385,9 +391,8 @@ int launch_bandloop(cudaStream_t stream, int max_grid, int nb, int G, const doub
   long long grid = std::min<long long>(items, (long long)max_grid);
   if (grid < 1) grid = 1;
   *grid_out = (int)grid;
-  gpp_bandloop_kernel<BCH, MIXED, GUARD><<<(int)grid, BandCfg<MIXED>::kNT, smem, stream>>>(nb, G, items, nchunks_g, wt, ie, st,
-                                                                                 wx4, partials, status, guard2,
-                                                                                 guard_d);
+  gpp_bandloop_kernel<BCH, MIXED, GUARD><<<(int)grid, BandCfg<MIXED>::kNT, smem, stream>>>(
+      nb, G, items, nchunks_g, wt, ie, st, wx4, partials, status, guard2, guard_d, stall_step());
   count_launch();
   BGW_CUDA_TRY(cudaGetLastError());
   return BGW_OK;

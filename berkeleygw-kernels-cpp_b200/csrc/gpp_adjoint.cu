@@ -71,7 +71,7 @@ constexpr int kAdjChunk = 1024;  // G elements of a row per staged step
 struct AdjSmem {
   double2 wt[2][kAdjChunk];
   double2 ie[2][kAdjChunk];
-  unsigned long long bar[2];
+  unsigned long long bar[3];  // [2]: never arrived on (stall injection)
   double red[(kAdjThreads / 32) * 6];
 };
 
@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2)
                        const double2 *__restrict__ Cp, const double2 *__restrict__ Sp, const int *__restrict__ igp,
                        const double *__restrict__ wx3, const double2 *__restrict__ gcot,
                        double2 *__restrict__ grad_wt, double2 *__restrict__ grad_ie, double *__restrict__ partials,
-                       int *status) {
+                       int *status, long long stall) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   AdjSmem &sm = *reinterpret_cast<AdjSmem *>(smem_raw);
   const int tid = threadIdx.x;
@@ -101,6 +101,7 @@ __global__ void __launch_bounds__(kAdjThreads, 2)
   if (tid == 0) {
     mbar_init(reinterpret_cast<uint64_t *>(&sm.bar[0]), 1);
     mbar_init(reinterpret_cast<uint64_t *>(&sm.bar[1]), 1);
+    mbar_init(reinterpret_cast<uint64_t *>(&sm.bar[2]), 1);
     fence_mbar_init();
   }
   __syncthreads();
@@ -115,17 +116,22 @@ __global__ void __launch_bounds__(kAdjThreads, 2)
     bulk_g2s(sm.ie[buf], ieps + p * G + g0, (uint32_t)nvalid * 16u, bar);
   };
   bool ok = true;
+  long long j_fail = 0;  // the step whose wait ran out
   if (tid == 0 && nsteps > 0) issue(0);
   double t_r[3] = {0.0, 0.0, 0.0}, t_i[3] = {0.0, 0.0, 0.0};  // T(p, iw) (this thread)
   double u_r[3] = {0.0, 0.0, 0.0}, u_i[3] = {0.0, 0.0, 0.0};  // sum_ig I q^2 (this thread)
   for (long long j = 0; j < nsteps; ++j) {
     if (tid == 0 && j + 1 < nsteps) issue(j + 1);
     const int buf = (int)(j & 1);
-    if (!mbar_wait_bounded(reinterpret_cast<uint64_t *>(&sm.bar[buf]), (uint32_t)((j >> 1) & 1), kWaitCycles)) {
+    if (!staged_wait(reinterpret_cast<uint64_t *>(&sm.bar[buf]), j, stall,
+                     reinterpret_cast<uint64_t *>(&sm.bar[2]))) {
       raise_status(status, BGW_ERR_TIMEOUT, blockIdx.x);
       ok = false;
     }
-    if (__syncthreads_or(!ok)) break;  // every thread agrees before leaving
+    if (__syncthreads_or(!ok)) {  // every thread agrees before leaving
+      j_fail = j;
+      break;
+    }
     const long long p = blockIdx.x + (j / nch) * (long long)gridDim.x;
     const int c = (int)(j % nch);
     const int g0 = c * kAdjChunk;
@@ -185,10 +191,10 @@ __global__ void __launch_bounds__(kAdjThreads, 2)
     }
   }
   if (!ok && tid == 0) {
-    // Let copies still in flight land before the CTA's shared memory is
-    // released (bounded as well).
-    (void)mbar_wait_bounded(reinterpret_cast<uint64_t *>(&sm.bar[0]), 0, kWaitCycles);
-    (void)mbar_wait_bounded(reinterpret_cast<uint64_t *>(&sm.bar[1]), 0, kWaitCycles);
+    // Copies still in flight (steps j_fail and j_fail + 1) land before the
+    // CTA's shared memory is released.
+    drain_staged(reinterpret_cast<uint64_t *>(&sm.bar[0]), reinterpret_cast<uint64_t *>(&sm.bar[1]), j_fail,
+                 j_fail + 1 < nsteps);
   }
   double vv[6] = {-dw_r[0], -dw_i[0], -dw_r[1], -dw_i[1], -dw_r[2], -dw_i[2]};
   block_sum<6, kAdjThreads>(vv, sm.red);
@@ -260,7 +266,7 @@ __global__ void gpp_adjoint_wx_kernel(int nb, const double *__restrict__ wx, lon
 struct AdjBandSmem {
   double2 C[2][kAbBCH];
   double4 wx[2][kAbBCH];
-  unsigned long long bar[2];
+  unsigned long long bar[3];  // [2]: never arrived on (stall injection)
   double red[(kAdjThreads / 32) * 6];
 };
 
@@ -270,7 +276,7 @@ __global__ void __launch_bounds__(kAdjThreads, 1)
                                 const double2 *__restrict__ wpp, const double4 *__restrict__ wx4,
                                 const double2 *__restrict__ gcot, double2 *__restrict__ grad_wt,
                                 double2 *__restrict__ grad_ie, double *__restrict__ Dpart,
-                                double *__restrict__ partials, int *status) {
+                                double *__restrict__ partials, int *status, long long stall) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   AdjBandSmem &sm = *reinterpret_cast<AdjBandSmem *>(smem_raw);
   const int tid = threadIdx.x;
@@ -282,6 +288,7 @@ __global__ void __launch_bounds__(kAdjThreads, 1)
   if (tid == 0) {
     mbar_init(reinterpret_cast<uint64_t *>(&sm.bar[0]), 1);
     mbar_init(reinterpret_cast<uint64_t *>(&sm.bar[1]), 1);
+    mbar_init(reinterpret_cast<uint64_t *>(&sm.bar[2]), 1);
     fence_mbar_init();
   }
   __syncthreads();
@@ -297,6 +304,7 @@ __global__ void __launch_bounds__(kAdjThreads, 1)
     bulk_g2s(sm.wx[buf], wx4 + b0, (uint32_t)nbv * 32u, bar);
   };
   bool ok = true;
+  long long j_fail = 0;  // the step whose wait ran out
   if (tid == 0 && nsteps > 0) issue(0);
   double dw_r[3] = {0.0, 0.0, 0.0}, dw_i[3] = {0.0, 0.0, 0.0};  // sum wpp I B' (sign at the end)
   double2 w[kAbE], v[kAbE];
@@ -304,11 +312,15 @@ __global__ void __launch_bounds__(kAdjThreads, 1)
   for (long long j = 0; j < nsteps; ++j) {
     if (tid == 0 && j + 1 < nsteps) issue(j + 1);
     const int buf = (int)(j & 1);
-    if (!mbar_wait_bounded(reinterpret_cast<uint64_t *>(&sm.bar[buf]), (uint32_t)((j >> 1) & 1), kWaitCycles)) {
+    if (!staged_wait(reinterpret_cast<uint64_t *>(&sm.bar[buf]), j, stall,
+                     reinterpret_cast<uint64_t *>(&sm.bar[2]))) {
       raise_status(status, BGW_ERR_TIMEOUT, blockIdx.x);
       ok = false;
     }
-    if (__syncthreads_or(!ok)) break;  // every thread agrees before leaving
+    if (__syncthreads_or(!ok)) {  // every thread agrees before leaving
+      j_fail = j;
+      break;
+    }
     const long long item = blockIdx.x + (j / nbc) * (long long)gridDim.x;
     const long long p = item / nchunk_e;
     const int g0 = (int)(item % nchunk_e) * kAbChunk;
@@ -385,8 +397,10 @@ __global__ void __launch_bounds__(kAdjThreads, 1)
     }
   }
   if (!ok && tid == 0) {
-    (void)mbar_wait_bounded(reinterpret_cast<uint64_t *>(&sm.bar[0]), 0, kWaitCycles);
-    (void)mbar_wait_bounded(reinterpret_cast<uint64_t *>(&sm.bar[1]), 0, kWaitCycles);
+    // Copies still in flight (steps j_fail and j_fail + 1) land before the
+    // CTA's shared memory is released.
+    drain_staged(reinterpret_cast<uint64_t *>(&sm.bar[0]), reinterpret_cast<uint64_t *>(&sm.bar[1]), j_fail,
+                 j_fail + 1 < nsteps);
   }
   double vv[6] = {-dw_r[0], -dw_i[0], -dw_r[1], -dw_i[1], -dw_r[2], -dw_i[2]};
   block_sum<6, kAdjThreads>(vv, sm.red);
@@ -470,7 +484,7 @@ int gpp_adjoint_bandloop_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G,
   BGW_TRY(prof_mark(env, 1));
   gpp_adjoint_bandloop_kernel<<<grid, kAdjThreads, smem, stream>>>(
       (int)nb, (int)G, items, nchunk_e, wt, ie, Ctab, wpp, (const double4 *)wx4v, gcot, grad_wt, grad_ie,
-      (double *)dpart, (double *)partials, env->d_status);
+      (double *)dpart, (double *)partials, env->d_status, stall_step());
   count_launch();
   BGW_CUDA_TRY(cudaGetLastError());
   BGW_TRY(prof_mark(env, 2));
@@ -524,7 +538,8 @@ int gpp_adjoint_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const in
   }
   BGW_TRY(prof_mark(env, 1));
   gpp_adjoint_kernel<<<grid, kAdjThreads, smem, stream>>>((int)P, (int)G, wt, ie, Cp, Sp, igp, wx, gcot, grad_wt,
-                                                          grad_ie, (double *)partials, env->d_status);
+                                                          grad_ie, (double *)partials, env->d_status,
+                                                          stall_step());
   count_launch();
   BGW_CUDA_TRY(cudaGetLastError());
   BGW_TRY(prof_mark(env, 2));

@@ -119,7 +119,7 @@ struct BatchSmem {
   double2 ie[2][kBThreads * KE];
   double2 st[2][BCH];
   double4 wx[2][BCH];
-  unsigned long long bar[2];
+  unsigned long long bar[3];  // [2]: never arrived on (stall injection)
   double red[(kBThreads / 32) * 6];
   double xr_lo[kBThreads / 32], xr_hi[kBThreads / 32];  // MIXED: chunk frequency range
   float4 xf[MIXED ? BCH : 1];                            // MIXED: FP32 frequency rows
@@ -145,7 +145,7 @@ __device__ __forceinline__ void flush(double (&acc_r)[3], double (&acc_i)[3], do
 template <int BCH, int KE, bool MIXED>
 __global__ void __launch_bounds__(kBThreads, KE == 8 ? 1 : 2)
     batch_bandloop_kernel(const BatchInst *__restrict__ inst, int n, const long long *__restrict__ range,
-                          int max_seg, double *__restrict__ partials, int *status) {
+                          int max_seg, double *__restrict__ partials, int *status, long long stall) {
   constexpr int kCH = kBThreads * KE;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   auto &sm = *reinterpret_cast<BatchSmem<BCH, KE, MIXED> *>(smem_raw);
@@ -155,6 +155,7 @@ __global__ void __launch_bounds__(kBThreads, KE == 8 ? 1 : 2)
   if (tid == 0) {
     mbar_init(reinterpret_cast<uint64_t *>(&sm.bar[0]), 1);
     mbar_init(reinterpret_cast<uint64_t *>(&sm.bar[1]), 1);
+    mbar_init(reinterpret_cast<uint64_t *>(&sm.bar[2]), 1);
     fence_mbar_init();
   }
   __syncthreads();
@@ -198,17 +199,24 @@ __global__ void __launch_bounds__(kBThreads, KE == 8 ? 1 : 2)
   double lo_r[3] = {0.0, 0.0, 0.0}, lo_i[3] = {0.0, 0.0, 0.0};
   Step cur{j0, inst_lo, 0};
   bool ok = true;
+  long long s_fail = 0;     // the step whose wait ran out
+  bool next_issued = false;  // whether step s_fail + 1 was staged
   if (tid == 0) issue(cur, 0);
   for (long long s = 0;; ++s) {
     const int buf = (int)(s & 1);
     const Step nx = next(cur);
     const bool more = nx.j < j1;
     if (tid == 0 && more) issue(nx, buf ^ 1);
-    if (!mbar_wait_bounded(reinterpret_cast<uint64_t *>(&sm.bar[buf]), (uint32_t)((s >> 1) & 1), kWaitCycles)) {
+    if (!staged_wait(reinterpret_cast<uint64_t *>(&sm.bar[buf]), s, stall,
+                     reinterpret_cast<uint64_t *>(&sm.bar[2]))) {
       raise_status(status, BGW_ERR_TIMEOUT, blockIdx.x);
       ok = false;
     }
-    if (__syncthreads_or(!ok)) break;
+    if (__syncthreads_or(!ok)) {
+      s_fail = s;
+      next_issued = more;
+      break;
+    }
     const BatchInst &I = inst[cur.i];
     const long long local = cur.j - I.item0;
     const int g0 = (int)(local % I.nchunk) * kCH;
@@ -234,8 +242,10 @@ __global__ void __launch_bounds__(kBThreads, KE == 8 ? 1 : 2)
     cur = nx;
   }
   if (!ok && tid == 0) {
-    (void)mbar_wait_bounded(reinterpret_cast<uint64_t *>(&sm.bar[0]), 0, kWaitCycles);
-    (void)mbar_wait_bounded(reinterpret_cast<uint64_t *>(&sm.bar[1]), 0, kWaitCycles);
+    // Copies still in flight (steps s_fail and, if staged, s_fail + 1) land
+    // before the CTA's shared memory is released.
+    drain_staged(reinterpret_cast<uint64_t *>(&sm.bar[0]), reinterpret_cast<uint64_t *>(&sm.bar[1]), s_fail,
+                 next_issued);
   }
 }
 
@@ -358,8 +368,9 @@ int band_variant(Variant *v) {
 
 template <int KE, bool MIXED>
 void launch_band(cudaStream_t s, int grid, size_t smem, const BatchInst *inst, int n, const long long *range,
-                 int max_seg, double *partials, int *status) {
-  batch_bandloop_kernel<256, KE, MIXED><<<grid, kBThreads, smem, s>>>(inst, n, range, max_seg, partials, status);
+                 int max_seg, double *partials, int *status, long long stall) {
+  batch_bandloop_kernel<256, KE, MIXED><<<grid, kBThreads, smem, s>>>(inst, n, range, max_seg, partials, status,
+                                                                      stall);
 }
 
 std::mutex g_tune_mu;
@@ -460,7 +471,9 @@ void assign_slots(std::vector<BatchInst> &inst, const std::vector<long long> &ra
   (void)n;
 }
 
-int enqueue_batch(bgw_gpp_batch *B, cudaStream_t s) {
+// stall: the band loop's injected stall step (-1 when tuning, so a test's
+// stall never reaches the tuner's timings or its cache).
+int enqueue_batch(bgw_gpp_batch *B, cudaStream_t s, long long stall = -1) {
   BGW_CUDA_TRY(cudaMemsetAsync(B->d_status, 0, sizeof(int32_t) * STATUS_WORDS, s));
   const int ninst = B->n;
   int pg = (int)std::min<long long>(std::max<long long>((B->total_cols + 7) / 8, 1), 148LL * 16);
@@ -471,16 +484,16 @@ int enqueue_batch(bgw_gpp_batch *B, cudaStream_t s) {
     BGW_CUDA_TRY(cudaGetLastError());
     if (B->mixed) {
       if (B->ke == 8) launch_band<8, true>(s, B->grid, B->smem, B->d_inst, ninst, B->d_range, B->max_seg,
-                                          B->d_partials, B->d_status);
+                                          B->d_partials, B->d_status, stall);
       else launch_band<4, true>(s, B->grid, B->smem, B->d_inst, ninst, B->d_range, B->max_seg, B->d_partials,
-                                B->d_status);
+                                B->d_status, stall);
     } else {
       if (B->ke == 8) launch_band<8, false>(s, B->grid, B->smem, B->d_inst, ninst, B->d_range, B->max_seg,
-                                           B->d_partials, B->d_status);
+                                           B->d_partials, B->d_status, stall);
       else if (B->ke == 4) launch_band<4, false>(s, B->grid, B->smem, B->d_inst, ninst, B->d_range, B->max_seg,
-                                                B->d_partials, B->d_status);
+                                                B->d_partials, B->d_status, stall);
       else launch_band<2, false>(s, B->grid, B->smem, B->d_inst, ninst, B->d_range, B->max_seg, B->d_partials,
-                                 B->d_status);
+                                 B->d_status, stall);
     }
   } else {
     batch_factored_kernel<4><<<B->grid, kBThreads, 0, s>>>(B->d_inst, ninst, B->d_range, B->max_seg,
@@ -741,7 +754,7 @@ extern "C" int bgw_gpp_batch_create(const bgw_gpp_instance *instances, int64_t n
     bgw_gpp_batch_destroy(B);
     return BGW_ERR_CUDA;
   }
-  rc = enqueue_batch(B, B->capture);
+  rc = enqueue_batch(B, B->capture, stall_step());
   cudaGraph_t graph = nullptr;
   const cudaError_t ce = cudaStreamEndCapture(B->capture, &graph);
   if (rc != BGW_OK || ce != cudaSuccess || !graph ||

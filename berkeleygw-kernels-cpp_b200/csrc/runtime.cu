@@ -16,6 +16,11 @@ namespace bgw {
 
 std::atomic<uint64_t> g_launches{0};
 
+namespace {
+std::atomic<long long> g_stall_step{-1};  // bgw_debug_inject_stall
+}  // namespace
+long long stall_step() { return g_stall_step.load(std::memory_order_relaxed); }
+
 void note_cuda_error(cudaError_t e, const char *what, const char *file, int line) {
   if (std::getenv("BGW_SIGMA_QUIET") == nullptr)
     std::fprintf(stderr, "libbgwsigma: %s failed: %s (%s:%d)\n", what, cudaGetErrorString(e), file, line);
@@ -300,6 +305,12 @@ int bgw_last_profile(bgw_profile *out) {
 }
 
 uint64_t bgw_launch_count(void) { return bgw::g_launches.load(); }
+
+int bgw_debug_inject_stall(int64_t step) {
+  if (step < -1) return BGW_ERR_INVALID_ARG;
+  bgw::g_stall_step.store((long long)step, std::memory_order_relaxed);
+  return BGW_OK;
+}
 
 int bgw_release_workspace(int32_t device) {
   int ndev = 0;

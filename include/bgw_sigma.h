@@ -361,6 +361,19 @@ int bgw_measure_fp64_peak(int32_t device, double *dfma_tflops,
 /* Releases the library's cached device workspace on `device` (-1: all). */
 int bgw_release_workspace(int32_t device);
 
+/* Test hook of the timeout path (no counterpart in the reference, whose
+ * only failure handling is exit() on bad command-line sizes).  The kernels
+ * that stage their inputs through double-buffered bulk copies -- the GPP
+ * band loop (FP64 and mixed), both GPP adjoint kernels and the batched band
+ * loop -- wait for each staged step with a bounded wait.  After
+ * bgw_debug_inject_stall(step), every such kernel launched later (any call,
+ * any device; a batch's kernels are fixed when bgw_gpp_batch_create captures
+ * them) makes the wait of CTA-local step `step` on a barrier that never
+ * completes, with a ~0.1 ms budget.  The wait runs out, the kernel lets its
+ * copies in flight land and exits, and the call returns BGW_ERR_TIMEOUT; the
+ * context stays usable.  step = -1 (the default) turns the stall off. */
+int bgw_debug_inject_stall(int64_t step);
+
 #ifdef __cplusplus
 }
 #endif

@@ -13,6 +13,7 @@ Both take the arrays of bgwsigma.inputs.GppInputs / FFInputs (host numpy).
 from __future__ import annotations
 
 import ctypes
+import os
 import subprocess
 from pathlib import Path
 
@@ -21,7 +22,8 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_LIB = HERE / "_build" / "liboracle.so"
 REF_LIB = HERE / "_ref" / "libbgwref.so"
-REF_SRC = Path("/root/reference")
+# The reference source tree: $BGW_REFERENCE_DIR, else the build container's mount.
+REF_SRC = Path(os.environ.get("BGW_REFERENCE_DIR", "/root/reference"))
 
 _P = ctypes.c_void_p
 _L = ctypes.c_long
@@ -34,7 +36,7 @@ def build_oracle(ref: bool | None = None) -> None:
     if ref is None:
         ref = (REF_SRC / "GPP" / "gpp.cpp").exists()
     if ref:
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref"], check=True)
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={REF_SRC}"], check=True)
 
 
 def _p(a) -> int:
