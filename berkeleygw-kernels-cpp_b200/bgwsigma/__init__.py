@@ -43,7 +43,7 @@ EXPORTS = ("bgw_options_init", "bgw_noflagOCC_solver", "bgw_achsDtemp_Kernel", "
            "bgw_launch_count", "bgw_measure_fp64_peak", "bgw_release_workspace", "bgw_last_profile",
            "bgw_noflagOCC_solver_noalloc", "bgw_noflagOCC_solver_backward", "bgw_gpp_batch_create",
            "bgw_gpp_batch_execute", "bgw_gpp_batch_info", "bgw_gpp_batch_destroy", "bgw_gpp_sigma",
-           "bgw_debug_inject_stall")
+           "bgw_debug_inject_stall", "bgw_fill_uniform")
 
 
 class BgwError(RuntimeError):
@@ -108,6 +108,7 @@ def load(build_if_needed: bool = True) -> ctypes.CDLL:
     lib.bgw_measure_fp64_peak.argtypes = [ctypes.c_int32, ctypes.POINTER(_D), ctypes.POINTER(_D)]
     lib.bgw_release_workspace.argtypes = [ctypes.c_int32]
     lib.bgw_debug_inject_stall.argtypes = [ctypes.c_int64]
+    lib.bgw_fill_uniform.argtypes = [_P, _I64, ctypes.c_uint64, ctypes.c_uint64, _I64, _D, _D, _D, _D, opt]
     lib.bgw_last_profile.argtypes = [ctypes.POINTER(Profile)]
     opt = ctypes.POINTER(Options)
     lib.bgw_noflagOCC_solver.argtypes = [_I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, opt]
@@ -151,6 +152,26 @@ def inject_stall(step: int = -1):
     kernels launched from now on let the wait of CTA-local step `step` run
     out, and their calls raise BgwError(BGW_ERR_TIMEOUT); -1 turns it off."""
     _check("bgw_debug_inject_stall", load().bgw_debug_inject_stall(int(step)))
+
+
+def fill_uniform(out, seed: int, stream_id: int, offset: int, lo_even: float, hi_even: float, lo_odd: float,
+                 hi_odd: float, *, stream=None):
+    """Fills `out` (a float64 CUDA tensor or host numpy array, contiguous)
+    with words offset .. offset + out.size - 1 of Philox stream (seed,
+    stream_id), mapped to the given ranges (bgw_fill_uniform)."""
+    lib = load()
+    if _is_torch(out):
+        n, mem = out.numel(), ("device" if out.is_cuda else "host")
+        ok = out.dtype.is_floating_point and out.element_size() == 8
+    else:
+        n, mem, ok = out.size, "host", out.dtype == np.float64
+    if not ok:
+        raise ValueError("out must hold float64 values")
+    dev = out.device.index if mem == "device" and out.device.index is not None else -1
+    o = make_options(mem, device=dev, stream=_stream_handle(None, stream))
+    _check("bgw_fill_uniform", lib.bgw_fill_uniform(_ptr(out), n, seed, stream_id, offset, lo_even, hi_even, lo_odd,
+                                                    hi_odd, ctypes.byref(o)))
+    return out
 
 
 def last_profile() -> dict:

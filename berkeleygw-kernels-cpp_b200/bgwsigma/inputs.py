@@ -157,6 +157,79 @@ def gpp_seeded(number_bands: int, nvband: int, ncouls: int, nodes_per_group: int
                      vcoul=vcoul, wx_band_stride=stride)
 
 
+# ------------------------------------------- counter-based (Philox) family --
+#
+# The same distributions as gpp_seeded, drawn from Philox4x64-10 streams
+# keyed by (seed, stream id), one stream per array, word w of an array being
+# its w-th double (interleaved re/im).  Every value depends only on (seed,
+# array, index), so a G' row block [p0, p1) of wtilde_array / I_eps_array is
+# generated without the rest, on the host (numpy's Philox, below) or on the
+# GPU (bgw_fill_uniform, bgwsigma.fill_uniform) with identical bits.
+# indinv (a permutation of ncouls entries) is drawn on the host from PCG64.
+PHILOX_STREAMS = {"aqsmtemp": 1, "aqsntemp": 2, "I_eps_array": 3, "wtilde_array": 4}
+# (lo_even, hi_even, lo_odd, hi_odd): real and imaginary ranges per array.
+GPP_RANGES = {"aqsmtemp": (-1.0, 1.0, -1.0, 1.0), "aqsntemp": (-1.0, 1.0, -1.0, 1.0),
+              "I_eps_array": (-0.5, 0.5, -0.5, 0.5), "wtilde_array": (0.5, 2.0, -0.01, 0.01)}
+
+
+def philox_uniform(n: int, seed: int, stream: int, offset: int, lo_even: float, hi_even: float, lo_odd: float,
+                   hi_odd: float) -> np.ndarray:
+    """Host twin of bgw_fill_uniform: words offset .. offset + n - 1 of
+    numpy's Philox(key=seed + stream * 2**64) mapped to [lo, hi) by
+    lo + (hi - lo) * ((word >> 11) * 2**-53) (even words: the real range,
+    odd words: the imaginary range), in pieces of at most 2**22 words."""
+    out = np.empty(n, dtype=np.float64)
+    piece = 1 << 22
+    for i in range(0, n, piece):
+        m = min(piece, n - i)
+        w0 = offset + i
+        bg = np.random.Philox(key=int(seed) + (int(stream) << 64), counter=[w0 // 4, 0, 0, 0])
+        skip = w0 % 4
+        u = (bg.random_raw(m + skip)[skip:] >> np.uint64(11)).astype(np.float64) * (2.0 ** -53)
+        even = ((w0 + np.arange(m)) & 1) == 0
+        v = out[i:i + m]
+        v[even] = u[even] * (hi_even - lo_even) + lo_even
+        v[~even] = u[~even] * (hi_odd - lo_odd) + lo_odd
+    return out
+
+
+def gpp_philox(number_bands: int, nvband: int, ncouls: int, nodes_per_group: int, seed: int = 1234,
+               rows: tuple[int, int] | None = None, device=None) -> GppInputs:
+    """GPP inputs with the benchmark distributions from Philox streams.
+    rows=(p0, p1): only G' rows [p0, p1) of the whole problem (ngpown =
+    p1 - p0; inv_igp_index, wtilde_array and I_eps_array sliced), as one
+    rank of a G'-sharded run holds them.  device (a torch device): the large
+    arrays are generated there by bgw_fill_uniform; else on the host."""
+    nb, G = number_bands, ncouls
+    P_all = G // nodes_per_group
+    p0, p1 = rows if rows is not None else (0, P_all)
+    P = p1 - p0
+    rng = np.random.default_rng(seed)
+    indinv = np.concatenate([rng.permutation(G).astype(np.int32), np.array([G - 1], dtype=np.int32)])
+    inv = (np.arange(p0, p1, dtype=np.int64) * nodes_per_group).astype(np.int32)
+    vcoul = 1.0 / (1.0 + np.arange(G, dtype=np.float64))
+    wx = 10.0 + np.array([-0.5, 0.0, 0.5])
+    shapes = {"aqsmtemp": (nb, G, 0), "aqsntemp": (nb, G, 0), "I_eps_array": (P, G, p0), "wtilde_array": (P, G, p0)}
+    big = {}
+    for name, (r, c, r0) in shapes.items():
+        n, off = 2 * r * c, 2 * r0 * c
+        if device is None:
+            big[name] = philox_uniform(n, seed, PHILOX_STREAMS[name], off, *GPP_RANGES[name]).view(
+                np.complex128).reshape(r, c)
+        else:
+            import torch
+
+            from . import fill_uniform
+            t = torch.empty((r, c), dtype=torch.complex128, device=device)
+            fill_uniform(torch.view_as_real(t), seed, PHILOX_STREAMS[name], off, *GPP_RANGES[name])
+            big[name] = t
+    small = dict(inv_igp_index=inv, indinv=indinv, wx_array=wx, vcoul=vcoul)
+    if device is not None:
+        import torch
+        small = {k: torch.as_tensor(v).to(device) for k, v in small.items()}
+    return GppInputs(number_bands=nb, nvband=nvband, ncouls=G, ngpown=P, wx_band_stride=0, **small, **big)
+
+
 # ------------------------------------------------------------------ FF --
 
 def ff_uniform(number_bands: int, nvband: int, ncouls: int, ngpown: int, nFreq: int, nfreqeval: int) -> FFInputs:

@@ -5,6 +5,7 @@
 // the kernels of gpp.cu / ff.cu on the caller's stream and, unless
 // BGW_FLAG_ASYNC, synchronises and returns the device-side status.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -38,6 +39,9 @@ int gpp_adjoint_enqueue(CallEnv *env, int64_t nb, int64_t P, int64_t G, const in
                         int64_t indinv_len, const double *wx, const double2 *wt, const double2 *am,
                         const double2 *an, const double2 *ie, const double *vc, const double2 *gcot,
                         double2 *grad_wt, double2 *grad_ie, double *domega);
+
+int fill_uniform_enqueue(CallEnv *env, double *out, int64_t n, uint64_t seed, uint64_t stream, int64_t off,
+                         double lo_even, double hi_even, double lo_odd, double hi_odd);
 
 }  // namespace bgw
 
@@ -427,4 +431,33 @@ extern "C" int bgw_ff_sigma(int64_t number_bands, int64_t nvband, int64_t nfreqe
   return ff_call(number_bands, nvband, nfreqeval, ncouls, ngpown, nFreq, freqevalmin, freqevalstep, occ, ekq,
                  dFreqGrid, inv_igp_index, indinv, indinv_len, aqsmtemp, aqsntemp, vcoul, I_epsR_array,
                  I_epsA_array, achsDtemp, asxDtemp, achDtemp_cor, opt);
+}
+
+extern "C" int bgw_fill_uniform(double *out, int64_t n, uint64_t seed, uint64_t stream, int64_t offset,
+                                double lo_even, double hi_even, double lo_odd, double hi_odd,
+                                const bgw_options *opt) {
+  if (n < 0 || offset < 0 || offset > INT64_MAX - n - 4) return BGW_ERR_INVALID_ARG;
+  if (n > 0 && !out) return BGW_ERR_INVALID_ARG;
+  if (!std::isfinite(lo_even) || !std::isfinite(hi_even) || !std::isfinite(lo_odd) || !std::isfinite(hi_odd))
+    return BGW_ERR_INVALID_ARG;
+  Call c(opt);
+  if (c.st != BGW_OK) return c.st;
+  CallEnv *env = &c.env;
+  if (!env->host) {
+    BGW_TRY(fill_uniform_enqueue(env, out, n, seed, stream, offset, lo_even, hi_even, lo_odd, hi_odd));
+    return finish_call(env);
+  }
+  // Host memory: generated on the GPU in 32 MiB pieces, each copied back
+  // before the next is generated into the same buffer (same stream).
+  constexpr int64_t kPiece = int64_t(4) << 20;  // doubles
+  void *buf = nullptr;
+  BGW_TRY(ws_reserve(env->ws, SLOT_OUT, sizeof(double) * (size_t)std::min<int64_t>(std::max<int64_t>(n, 1), kPiece),
+                     &buf));
+  for (int64_t i = 0; i < n; i += kPiece) {
+    const int64_t m = std::min<int64_t>(kPiece, n - i);
+    BGW_TRY(fill_uniform_enqueue(env, static_cast<double *>(buf), m, seed, stream, offset + i, lo_even, hi_even,
+                                 lo_odd, hi_odd));
+    BGW_CUDA_TRY(cudaMemcpyAsync(out + i, buf, sizeof(double) * (size_t)m, cudaMemcpyDeviceToHost, env->stream));
+  }
+  return finish_call(env);
 }

@@ -330,6 +330,26 @@ int bgw_ff_sigma(int64_t number_bands, int64_t nvband, int64_t nfreqeval,
                  double *achsDtemp, double *asxDtemp, double *achDtemp_cor,
                  const bgw_options *opt);
 
+/* ------------------------------------------------------- input generation --
+ * Replaces the drivers' host-side, single-threaded fills of their inputs
+ * (GPP/gpp.cpp:246-275, FF/ff.cpp:585-633) for seeded synthetic runs: the
+ * values are generated on the GPU by a counter-based generator, so a
+ * sub-block of an array (one rank's G' rows, a chunk) is generated on its
+ * own and every value is independent of the device, grid and order.
+ *   out[i], 0 <= i < n, is word offset + i of stream (seed, stream) of
+ *   Philox4x64-10 (Salmon et al., SC'11): word w is word w % 4 of the block
+ *   with counter (w / 4 + 1, 0, 0, 0) and key (seed, stream) -- numpy's
+ *   np.random.Philox(key=seed + stream * 2**64).random_raw() sequence.
+ *   It is mapped to u = (word >> 11) * 2^-53 in [0, 1) and then to
+ *   lo + (hi - lo) * u, two roundings and no fused multiply-add, with
+ *   (lo_even, hi_even) for even words and (lo_odd, hi_odd) for odd words
+ *   (real and imaginary parts of an interleaved complex array).
+ * opt->memory: DEVICE fills device memory on opt->stream (asynchronous with
+ * BGW_FLAG_ASYNC); HOST generates on the GPU and copies into `out`. */
+int bgw_fill_uniform(double *out, int64_t n, uint64_t seed, uint64_t stream,
+                     int64_t offset, double lo_even, double hi_even,
+                     double lo_odd, double hi_odd, const bgw_options *opt);
+
 /* ------------------------------------------------------------- profiling --
  * Filled by a synchronous call made with BGW_FLAG_PROFILE; per thread. */
 typedef struct bgw_profile {
