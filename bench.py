@@ -1,15 +1,23 @@
 #!/usr/bin/env python
 """bench.py -- seconds per self-energy (Sigma) evaluation on B200.
 
-Workload (N=1): the GPP plain-FP64 benchmark configuration -- 512 bands,
-nvband 2, ncouls 32768, nodes_per_group 20 (ngpown 1638), 3 frequencies,
-seeded inputs with the benchmark distributions (bgwsigma.inputs.gpp_seeded),
-evaluated by the band-loop kernel (every (band, G', G, frequency) quotient, as
-the reference loop nest GPP/gpp.cpp:343-390).  One step = one Sigma
-evaluation through the C ABI with inputs resident in HBM (2.25 GB, larger than
-the 126 MB L2, so no flush is needed).  With --gpus N each rank evaluates its
-own instance (seed + rank); no data-path collective; value = max-over-ranks
-time / (N * steps).
+Workload: the GPP plain-FP64 benchmark configuration -- 512 bands, nvband 2,
+ncouls 32768, nodes_per_group 20 (ngpown 1638), 3 frequencies, seeded inputs
+with the benchmark distributions, evaluated by the band-loop kernel (every
+(band, G', G, frequency) quotient, as the reference loop nest
+GPP/gpp.cpp:343-390).  One step = one Sigma evaluation through the C ABI with
+inputs resident in HBM (2.25 GB, larger than the 126 MB L2, so no flush is
+needed).
+
+N = 1: the inputs are bgwsigma.inputs.gpp_seeded (PCG64, seed 1234; the
+reference build's own output on them is stored in tests/golden/golden.json).
+N > 1 (torchrun, one rank per GPU): one Sigma is split over G' columns, as
+BerkeleyGW splits ngpown over MPI tasks (GPP/gpp.cpp:144, 162): rank r
+generates its contiguous row block of wtilde / I_eps on its GPU
+(gpp_philox(rows=...), counter-based, so no rank generates another's rows),
+evaluates its partial achtemp, and the partials are all-gathered over NCCL
+and summed in rank order; value = max-over-ranks time per Sigma ("scaling":
+"strong").  --replicas instead runs one independent Sigma per GPU ("weak").
 
 Extra lines in the JSON: the factored GPP path, the FF sums at 512 bands /
 nvband 2 / ncouls 8192 / ngpown 512 / nFreq 15 / nfreqeval 10, the end-to-end
@@ -135,58 +143,43 @@ def dist_setup(args):
 
 # ------------------------------------------------------- reference (CPU) --
 
-def cpu_reference_gpp(g_full, target_s: float, threads_note: bool = True):
-    """Times the reference's OpenMP build (oracle/_ref) -- or, where it was not
-    built, the oracle port -- on the first nb_s bands of the workload, sized
-    to about target_s seconds; returns (seconds per full Sigma, descriptor)."""
-    from bgwsigma import inputs as I
-    from oracle.oracle import Oracle, Reference
-    if Reference.available():
-        impl, kind, cores = Reference(), "reference", None
-        cores = impl.num_threads()
-    else:
-        impl, kind, cores = Oracle(), "port", os.cpu_count()
+def cpu_reference_gpp(reps: int, warmup: int) -> dict:
+    """Times `reps` whole noflagOCC_solver calls of the reference's OpenMP
+    build (or, where it was not built, the oracle port) on the benchmark
+    workload, in a process of its own (oracle/cpu_baseline.py: no torch or
+    GPU-library threads share the cores).  Returns its JSON record."""
+    d = GPP_DIMS
+    cmd = [sys.executable, "-m", "oracle.cpu_baseline", "--bands", str(d["number_bands"]), "--nvband",
+           str(d["nvband"]), "--ncouls", str(d["ncouls"]), "--npg", str(d["nodes_per_group"]), "--seed", "1234",
+           "--reps", str(reps), "--warmup", str(warmup)]
+    r = subprocess.run(cmd, cwd=str(REPO), capture_output=True, text=True, check=True)
+    return json.loads(r.stdout.strip().splitlines()[-1])
 
-    def sample(nb_s):
-        g = I.GppInputs(**{**g_full.__dict__, "number_bands": nb_s,
-                            "aqsmtemp": np.ascontiguousarray(g_full.aqsmtemp[:nb_s]),
-                            "aqsntemp": np.ascontiguousarray(g_full.aqsntemp[:nb_s])})
-        t0 = time.perf_counter()
-        impl.gpp(g)
-        return time.perf_counter() - t0
 
-    nb = g_full.number_bands
-    t4 = sample(4)
-    nb_s = int(min(nb, max(4, round(4 * target_s / max(t4, 1e-6)))))
-    t = sample(nb_s)
-    per_sigma = t * nb / nb_s
-    desc = {"kind": kind, "cores": cores,
-            "sample": f"first {nb_s} of {nb} bands of the same workload ({t:.2f} s), scaled by {nb}/{nb_s} "
-                      f"(the reference's work is linear in bands)",
-            "nb_sample": nb_s, "sample_s": t}
-    return per_sigma, desc
+def config_of(world: int) -> dict:
+    """The `config` of both arms' lines (identical keys and values)."""
+    return {"workload": WORKLOAD, "global_batch": 1,
+            "l2": "inputs 2.25 GB resident in HBM (> 126 MB L2); no flush",
+            "parallelism": "one Sigma per step" if world == 1 else f"one Sigma per step over {world} ranks"}
 
 
 def run_reference_arm(args, world, rank):
     if rank != 0:
         return 0
-    from bgwsigma import inputs as I
-    g = I.gpp_seeded(**GPP_DIMS, seed=1234)
-    budget = 150.0  # seconds for the whole run
-    per_step_target = max(1.0, budget / (args.steps + args.warmup))
-    vals = []
-    desc = None
-    for i in range(args.warmup + args.steps):
-        v, desc = cpu_reference_gpp(g, per_step_target)
-        if i >= args.warmup:
-            vals.append(v)
-    value = statistics.median(vals)
+    rec = cpu_reference_gpp(args.steps, args.warmup)
+    times = rec["times_s"]
+    value = statistics.median(times)
+    sample = (f"{len(times)} whole noflagOCC_solver calls (512 bands each, GPP/gpp.cpp:282-289), one per step, "
+              f"median {value:.2f} s (min {min(times):.2f}, max {max(times):.2f}); {args.warmup} untimed warm-up "
+              f"calls on the first {rec['warmup_bands']} bands")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded PCG64)",
-            "config": {"workload": WORKLOAD, "parallelism": "OpenMP 3.0 on the host cores"},
-            "cpu_baseline": {"value": value, "unit": "s", "cores": desc["cores"], "kind": desc["kind"],
-                             "sample": desc["sample"]},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(times) * 1e3,
+            "higher_is_better": False, "scaling": "weak" if world == 1 or args.replicas else "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded PCG64, benchmark distributions)",
+            "config": config_of(world),
+            "execution": f"OpenMP 3.0 build of the reference on {rec['cores']} host threads (rank 0 only)",
+            "cpu_baseline": {"value": value, "unit": "s", "cores": rec["cores"], "kind": rec["kind"],
+                             "sample": sample, "times_s": times},
             "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -223,15 +216,45 @@ def run_ours(args, world, rank, local):
     bgw.load()
     dfma_peak, dmma_peak = bgw.measure_fp64_peak(local)
 
-    g = I.gpp_seeded(**GPP_DIMS, seed=1234 + rank)
-    d = bgw.to_device(g, dev)
+    sharded = world > 1 and not args.replicas
+    if sharded:
+        # This rank's G' row block of the one Sigma, generated on its GPU.
+        from bgwsigma import shard as SH
+        P_all = GPP_DIMS["ncouls"] // GPP_DIMS["nodes_per_group"]
+        rows = SH.column_range(P_all, world, rank)
+        d = I.gpp_philox(**GPP_DIMS, seed=1234, rows=rows, device=dev)
+        g = d.map_arrays(lambda t: t.cpu().numpy())
+        args.quick = True
+    else:
+        g = I.gpp_seeded(**GPP_DIMS, seed=1234 + rank)
+        d = bgw.to_device(g, dev)
+        if world > 1:
+            args.quick = True
     stream = torch.cuda.Stream(device=dev)
     sh = stream.cuda_stream
     out = torch.zeros(3, dtype=torch.complex128, device=dev)
+    parts = [torch.zeros(3, dtype=torch.complex128, device=dev) for _ in range(world)]
+    total = torch.zeros(3, dtype=torch.complex128, device=dev)
+
+    def gather(local_out):
+        """Sharded: all-gathers the ranks' partial achtemp (NCCL, after this
+        rank's kernels on `stream`) and sums them in rank order."""
+        if not sharded:
+            return local_out
+        with torch.cuda.stream(stream):
+            pg.all_gather(parts, local_out)
+            total.copy_(parts[0])
+            for q in parts[1:]:
+                total.add_(q)
+        return total
+
+    def sigma_step():
+        bgw.noflagOCC_solver(d, stream=sh, out=out, algorithm="bandloop", flags=bgw.FLAG_PROFILE)
+        return gather(out)
 
     # Warm-up.
     for _ in range(args.warmup):
-        bgw.noflagOCC_solver(d, stream=sh, out=out, algorithm="bandloop", flags=bgw.FLAG_PROFILE)
+        sigma_step()
     torch.cuda.synchronize(dev)
     barrier()
     torch.cuda.synchronize(dev)
@@ -245,7 +268,7 @@ def run_ours(args, world, rank, local):
     main_ms = []
     e0.record(stream)
     for _ in range(args.steps):
-        bgw.noflagOCC_solver(d, stream=sh, out=out, algorithm="bandloop", flags=bgw.FLAG_PROFILE)
+        res_t = sigma_step()
         main_ms.append(bgw.last_profile()["main_kernel_ms"])
     e1.record(stream)
     torch.cuda.synchronize(dev)
@@ -256,8 +279,8 @@ def run_ours(args, world, rank, local):
     elapsed_ms = max_over_ranks(e0.elapsed_time(e1))
     prof = bgw.last_profile()
     ms_per_step = elapsed_ms / args.steps
-    value = elapsed_ms / 1e3 / (args.steps * world)
-    result = out.cpu().numpy()
+    value = elapsed_ms / 1e3 / (args.steps * (1 if sharded else world))
+    result = res_t.cpu().numpy()
 
     kernel_ms = statistics.mean(main_ms)
     achieved = prof["flops"] / (kernel_ms * 1e-3) / 1e12
@@ -273,8 +296,14 @@ def run_ours(args, world, rank, local):
     # End to end: host (pinned) inputs, H2D + kernels + D2H inside the timed region.
     gp = bgw.to_pinned(g)
 
+    def e2e_call(algorithm):
+        r = bgw.noflagOCC_solver(gp, stream=sh, algorithm=algorithm)
+        if sharded:  # this rank's partial, gathered and summed on the GPUs, read back
+            r = gather(torch.as_tensor(r).to(dev)).cpu().numpy()
+        return r
+
     def time_e2e(algorithm):
-        bgw.noflagOCC_solver(gp, stream=sh, algorithm=algorithm)
+        e2e_call(algorithm)
         torch.cuda.synchronize(dev)
         barrier()
         h0 = torch.cuda.Event(enable_timing=True)
@@ -282,10 +311,10 @@ def run_ours(args, world, rank, local):
         n = max(3, min(args.steps, 10))
         h0.record(stream)
         for _ in range(n):
-            res = bgw.noflagOCC_solver(gp, stream=sh, algorithm=algorithm)
+            res = e2e_call(algorithm)
         h1.record(stream)
         torch.cuda.synchronize(dev)
-        return max_over_ranks(h0.elapsed_time(h1)) / 1e3 / (n * world), n, res
+        return max_over_ranks(h0.elapsed_time(h1)) / 1e3 / (n * (1 if sharded else world)), n, res
 
     e2e_s, e2e_steps, host_res = time_e2e("bandloop")
     # Bytes the call moves host -> device: wtilde and I_eps whole; of aqsmtemp,
@@ -294,7 +323,11 @@ def run_ours(args, world, rank, local):
     nbp = g.number_bands * g.ngpown
     h2d = (g.wtilde_array.nbytes + g.I_eps_array.nbytes + 2 * 16 * nbp + 8 * g.ngpown + g.inv_igp_index.nbytes
            + g.indinv.nbytes + g.wx_array.nbytes)
-    e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 48,
+    if pg is not None:  # whole job: every rank's copies
+        hb = torch.tensor([float(h2d)], dtype=torch.float64, device=dev)
+        pg.all_reduce(hb)
+        h2d = float(hb.item())
+    e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 48 * world,
            "steps": e2e_steps, "note": "bgw_noflagOCC_solver (band loop) with BGW_MEMORY_HOST on pinned buffers: "
                                        "per step the call reads the host inputs (aqsmtemp / aqsntemp gathered to "
                                        "the ngpown columns used), copies them H2D, runs the kernels and copies "
@@ -537,7 +570,8 @@ def run_ours(args, world, rank, local):
     cpu_baseline = None
     if rank == 0 and not args.no_cpu:
         from oracle.oracle import Oracle
-        ref = Oracle().gpp(g, factored=True)
+        # Sharded: the gathered result is the whole problem's sum.
+        ref = Oracle().gpp(I.gpp_philox(**GPP_DIMS, seed=1234) if sharded else g, factored=True)
         extra["rel_err_vs_oracle"] = {"bandloop": rel_err(result, ref), "e2e_host_path": rel_err(host_res, ref)}
         # The reference build's own output on these inputs (seed 1234), stored
         # with their fingerprint by tests/golden/make_golden.py --full.
@@ -550,17 +584,21 @@ def run_ours(args, world, rank, local):
         except (OSError, KeyError, ValueError):
             pass
         if world == 1:
-            per_sigma, desc = cpu_reference_gpp(g, args.cpu_seconds)
-            cpu_baseline = {"value": per_sigma, "unit": "s", "cores": desc["cores"], "kind": desc["kind"],
-                            "sample": desc["sample"]}
+            rec = cpu_reference_gpp(1, 1)
+            cpu_baseline = {"value": rec["times_s"][0], "unit": "s", "cores": rec["cores"], "kind": rec["kind"],
+                            "sample": "one whole noflagOCC_solver call of the workload (512 bands, "
+                                      "GPP/gpp.cpp:282-289) in a process of its own, after one untimed warm-up "
+                                      f"call on the first {rec['warmup_bands']} bands"}
 
     if rank == 0:
+        data = ("synthetic (seeded Philox4x64-10 generated on the GPUs, benchmark distributions)" if sharded
+                else "synthetic (seeded PCG64, benchmark distributions)")
         line = {"metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded PCG64, benchmark distributions)",
-                "config": {"workload": WORKLOAD, "global_batch": world, "l2": "inputs 2.25 GB resident in HBM per "
-                           "GPU (> 126 MB L2); no flush", "parallelism": f"{world} independent instance(s), one "
-                           "per GPU"},
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False,
+                "scaling": "strong" if sharded else "weak", "vs_baseline": None, "dtype": "f64", "data": data,
+                "config": config_of(world),
+                "execution": (f"G' columns split over {world} GPUs (one NCCL all-gather of the partials per step)"
+                              if sharded else f"{world} independent Sigma evaluation(s), one per GPU"),
                 "roofline": roofline, "cpu_baseline": cpu_baseline, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clk, "extra": extra}
         print(json.dumps(line), flush=True)
@@ -722,7 +760,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--quick", action="store_true", help="GPP band loop + e2e only")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and oracle check")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--replicas", action="store_true",
+                    help="with N > 1: one independent Sigma per GPU instead of one Sigma split over G'")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-instances extra")
     ap.add_argument("--only", choices=["gpp_bandloop", "gpp_mixed", "gpp_factored", "gpp_adjoint",
                                        "gpp_adjoint_bandloop", "gpp_sigma", "ff", "ff_mixed",
