@@ -56,7 +56,7 @@ class Options(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_int32), ("memory", ctypes.c_int32), ("precision", ctypes.c_int32),
                 ("gpp_algorithm", ctypes.c_int32), ("wx_band_stride", ctypes.c_int64), ("device", ctypes.c_int32),
                 ("flags", ctypes.c_int32), ("stream", ctypes.c_void_p), ("device_status", ctypes.c_void_p),
-                ("pole_guard", ctypes.c_double)]
+                ("pole_guard", ctypes.c_double), ("mixed_order", ctypes.c_int32)]
 
 
 class Profile(ctypes.Structure):
@@ -108,9 +108,9 @@ def load(build_if_needed: bool = True) -> ctypes.CDLL:
     lib.bgw_measure_fp64_peak.argtypes = [ctypes.c_int32, ctypes.POINTER(_D), ctypes.POINTER(_D)]
     lib.bgw_release_workspace.argtypes = [ctypes.c_int32]
     lib.bgw_debug_inject_stall.argtypes = [ctypes.c_int64]
-    lib.bgw_fill_uniform.argtypes = [_P, _I64, ctypes.c_uint64, ctypes.c_uint64, _I64, _D, _D, _D, _D, opt]
     lib.bgw_last_profile.argtypes = [ctypes.POINTER(Profile)]
     opt = ctypes.POINTER(Options)
+    lib.bgw_fill_uniform.argtypes = [_P, _I64, ctypes.c_uint64, ctypes.c_uint64, _I64, _D, _D, _D, _D, opt]
     lib.bgw_noflagOCC_solver.argtypes = [_I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, opt]
     lib.bgw_gpp_sigma.argtypes = [_I64, _I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P, _P, opt]
     lib.bgw_noflagOCC_solver_noalloc.argtypes = [_I64, _I64, _I64, _P, _P, _I64, _P, _P, _P, _P, _P, _P, _P,
@@ -211,7 +211,7 @@ def _where(inp) -> str:
 
 
 def make_options(memory="host", precision="fp64", algorithm="auto", wx_band_stride=0, device=-1, stream=None,
-                 flags=0, device_status=None, pole_guard=0.0) -> Options:
+                 flags=0, device_status=None, pole_guard=0.0, mixed_order=None) -> Options:
     o = Options()
     load().bgw_options_init(ctypes.byref(o))
     o.memory = MEMORY[memory]
@@ -223,6 +223,8 @@ def make_options(memory="host", precision="fp64", algorithm="auto", wx_band_stri
     o.stream = stream
     o.device_status = device_status
     o.pole_guard = float(pole_guard)
+    if mixed_order is not None:
+        o.mixed_order = int(mixed_order)
     return o
 
 
@@ -233,7 +235,7 @@ def _stream_handle(inp, stream):
 
 
 def noflagOCC_solver(inp: GppInputs, *, precision="fp64", algorithm="auto", stream=None, out=None,
-                     flags=0, device_status=None, pole_guard=0.0) -> np.ndarray:
+                     flags=0, device_status=None, pole_guard=0.0, mixed_order=None) -> np.ndarray:
     """achtemp[3] (complex128).  `out`: optional preallocated output (host
     numpy complex128[3] or a CUDA tensor for device-resident inputs).
     `pole_guard` > 0: terms with |wx - wtilde| below it contribute zero."""
@@ -246,7 +248,7 @@ def noflagOCC_solver(inp: GppInputs, *, precision="fp64", algorithm="auto", stre
             import torch
             out = torch.zeros(3, dtype=torch.complex128, device=inp.wtilde_array.device)
     o = make_options(mem, precision, algorithm, inp.wx_band_stride, stream=_stream_handle(inp, stream),
-                     flags=flags, device_status=device_status, pole_guard=pole_guard)
+                     flags=flags, device_status=device_status, pole_guard=pole_guard, mixed_order=mixed_order)
     st = lib.bgw_noflagOCC_solver(inp.number_bands, inp.ngpown, inp.ncouls, _ptr(inp.inv_igp_index),
                                   _ptr(inp.indinv), len(inp.indinv), _ptr(inp.wx_array), _ptr(inp.wtilde_array),
                                   _ptr(inp.aqsmtemp), _ptr(inp.aqsntemp), _ptr(inp.I_eps_array), _ptr(inp.vcoul),
@@ -256,7 +258,7 @@ def noflagOCC_solver(inp: GppInputs, *, precision="fp64", algorithm="auto", stre
 
 
 def gpp_sigma(inp: GppInputs, nvband=None, *, want_ach=True, want_asx=True, precision="fp64", algorithm="auto",
-              stream=None, flags=0, device_status=None, pole_guard=0.0):
+              stream=None, flags=0, device_status=None, pole_guard=0.0, mixed_order=None):
     """(achtemp[3], asxtemp[3]) complex128: the Coulomb-hole sum over all
     bands and the GPP screened exchange of the occupied bands n1 < nvband
     (default: inp.nvband).  A result not asked for is None."""
@@ -273,7 +275,7 @@ def gpp_sigma(inp: GppInputs, nvband=None, *, want_ach=True, want_asx=True, prec
     ach = buf() if want_ach else None
     asx = buf() if want_asx else None
     o = make_options(mem, precision, algorithm, inp.wx_band_stride, stream=_stream_handle(inp, stream),
-                     flags=flags, device_status=device_status, pole_guard=pole_guard)
+                     flags=flags, device_status=device_status, pole_guard=pole_guard, mixed_order=mixed_order)
     st = lib.bgw_gpp_sigma(inp.number_bands, nv, inp.ngpown, inp.ncouls, _ptr(inp.inv_igp_index),
                            _ptr(inp.indinv), len(inp.indinv), _ptr(inp.wx_array), _ptr(inp.wtilde_array),
                            _ptr(inp.aqsmtemp), _ptr(inp.aqsntemp), _ptr(inp.I_eps_array), _ptr(inp.vcoul),
@@ -317,7 +319,8 @@ class GppBatch:
     """Many device-resident GPP instances in one persistent launch (a CUDA
     graph replayed by execute()).  `instances`: GppInputs with CUDA tensors."""
 
-    def __init__(self, instances, *, precision="fp64", algorithm="auto", stream=None, pole_guard=0.0):
+    def __init__(self, instances, *, precision="fp64", algorithm="auto", stream=None, pole_guard=0.0,
+                 mixed_order=None):
         import torch
         lib = load()
         self.instances = list(instances)
@@ -333,7 +336,8 @@ class GppBatch:
                                  self.out[k].data_ptr())
         self._arr = arr
         o = make_options("device", precision, algorithm, stream=_stream_handle(None, stream),
-                         device=dev.index if dev.index is not None else -1, pole_guard=pole_guard)
+                         device=dev.index if dev.index is not None else -1, pole_guard=pole_guard,
+                         mixed_order=mixed_order)
         h = _P()
         _check("bgw_gpp_batch_create", lib.bgw_gpp_batch_create(arr, len(self.instances), ctypes.byref(o),
                                                                 ctypes.byref(h)))

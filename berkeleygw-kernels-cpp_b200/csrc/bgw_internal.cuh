@@ -233,9 +233,8 @@ __device__ __forceinline__ bool staged_wait(uint64_t *bar, long long j, long lon
 // both barriers would be wrong: when a barrier's outstanding phase is odd,
 // its completed parity-0 phase satisfies the wait at once.)
 __device__ __forceinline__ void drain_staged(uint64_t *bar0, uint64_t *bar1, long long j, bool next_issued) {
-  uint64_t *bar[2] = {bar0, bar1};
-  (void)mbar_wait_bounded(bar[j & 1], (uint32_t)((j >> 1) & 1), kWaitCycles);
-  if (next_issued) (void)mbar_wait_bounded(bar[(j + 1) & 1], (uint32_t)(((j + 1) >> 1) & 1), kWaitCycles);
+  (void)mbar_wait_bounded((j & 1) ? bar1 : bar0, (uint32_t)((j >> 1) & 1), kWaitCycles);
+  if (next_issued) (void)mbar_wait_bounded((j & 1) ? bar0 : bar1, (uint32_t)(((j + 1) >> 1) & 1), kWaitCycles);
 }
 
 // Host side: the stall step for kernels launched from now on (-1: off).

@@ -113,14 +113,13 @@ __global__ void gpp_wx_kernel(int nb, const double *__restrict__ wx, long long s
 //   conj(wdiff) * I_eps = (dr*Ir + a) + i (dr*Ii + b).
 // Elements per thread: 8 (a longer run per band amortises the per-band
 // combination with sch_store1: FP64 53.6 ms at 8 vs 58.0 ms at 4 and 55.8 ms
-// at 6 on the 512-band benchmark).  Threads per CTA: FP64 256 (one CTA per
-// SM: 210 registers, 153 KB of staging); mixed 384 (one CTA per SM: 12
-// warps, as many as its registers allow, to hide the MUFU latency; 223 KB of
-// staging).
+// at 6 on the 512-band benchmark).  256 threads per CTA, one CTA per SM
+// (FP64: 210 registers, 153 KB of staging; mixed: 194 KB of staging with
+// the per-band remainder rows).
 template <bool MIXED>
 struct BandCfg {
   static constexpr int kE = 8;
-  static constexpr int kNT = MIXED ? 384 : kThreads;
+  static constexpr int kNT = kThreads;
   static constexpr int kCH = kNT * kE;
 };
 
@@ -131,28 +130,28 @@ struct BandSmem {
   double2 st[2][BCH];
   double4 wx[2][BCH];
   unsigned long long bar[3];  // [2]: never arrived on (stall injection)
-  double red[(BandCfg<MIXED>::kNT / 32) * 6];
+  double red[(BandCfg<MIXED>::kNT / 32) * 18];
   double xr_lo[BandCfg<MIXED>::kNT / 32], xr_hi[BandCfg<MIXED>::kNT / 32];  // MIXED: chunk frequency range
-  float4 xf[MIXED ? BCH : 1];                                                 // MIXED: FP32 frequency rows
-  float2 sf[MIXED ? BCH : 1];                                                 // MIXED: FP32 sch_store1
+  RemRow rows[MIXED ? BCH : 1];                                               // MIXED: per-band remainder rows
 };
 
 // Every band reads its own frequencies from the staged wx4 rows (for the
 // reference's band-independent wx the rows repeat one triple), so each
 // (band, G', G, frequency) quotient is evaluated, as in gpp.cpp:343-390.
-// MIXED: quotients in FP32 (rcp.approx.ftz.f32), their products with
-// sch_store1 summed in FP32 over groups of 8 bands, the group sums
-// accumulated in FP64 with TwoSum compensation (band_sweep_mixed).
+// MIXED: each step's quotients are expanded about the centre of the step's
+// frequencies; K Taylor terms are hoisted into FP64 per element (rem_stage /
+// rem_elems) and the remainder, |t|^K of each term, is a per-term complex
+// quotient in packed FP32 (rem_sweep) whose group sums are accumulated in
+// FP64 with TwoSum.  Elements near a pole take the FP64 path (near_sweep),
+// which also applies the pole_guard cut-off.
 // GUARD (FP64): near-pole cut-off, terms with |wdiff|^2 < guard2 contribute
-// zero.  MIXED: elements near the chunk's frequencies take an FP64 path
-// (near_elems / near_sweep), which also applies the cut-off (guard_d =
-// sqrt(guard2)); GUARD is not used.
-template <int BCH, bool MIXED, bool GUARD>
+// zero.  MIXED applies the guard in its FP64 near path; GUARD is not used.
+template <int BCH, bool MIXED, bool GUARD, int K = 3>
 __global__ void __launch_bounds__(BandCfg<MIXED>::kNT, 1)
     gpp_bandloop_kernel(int nb, int G, long long items, int nchunks_g, const double2 *__restrict__ wtilde,
                         const double2 *__restrict__ ieps, const double2 *__restrict__ st,
                         const double4 *__restrict__ wx4, double *__restrict__ partials, int *status,
-                        double guard2, double guard_d, long long stall) {
+                        double guard2, long long stall) {
   constexpr int kE = BandCfg<MIXED>::kE;
   constexpr int kCH = BandCfg<MIXED>::kCH;
   constexpr int kThreads = BandCfg<MIXED>::kNT;  // shadows the file-wide 256
@@ -221,11 +220,11 @@ __global__ void __launch_bounds__(BandCfg<MIXED>::kNT, 1)
     const int nbv = min(BCH, nb - b0);
 
     if constexpr (MIXED) {
-      Elem<float> e[kE];
-      load_elems<float, kE>(e, sm.wt[buf], sm.ie[buf], nvalid, kThreads, tid);
-      const double2 xr = stage_mixed_rows<kThreads>(sm.wx[buf], sm.st[buf], nbv, sm.xf, sm.sf, sm.xr_lo, sm.xr_hi);
-      const uint32_t near = near_elems<kE>(e, sm.wt[buf], nvalid, kThreads, tid, xr, guard_d);
-      band_sweep_mixed<kE>(e, sm.xf, sm.sf, nbv, acc_r, acc_i, lo_r, lo_i);
+      const RemStep rs = rem_stage<kThreads, K>(sm.wx[buf], sm.st[buf], nbv, sm.rows, sm.red, sm.xr_lo, sm.xr_hi);
+      RemElems<kE> e;
+      const uint32_t near = rem_elems<kE, K>(e, sm.wt[buf], sm.ie[buf], nvalid, kThreads, tid, rs, guard2, acc_r,
+                                             acc_i);
+      rem_sweep<kE>(e, sm.rows, nbv, acc_r, acc_i, lo_r, lo_i);
       if (near) near_sweep(near, sm.wt[buf], sm.ie[buf], kThreads, tid, sm.wx[buf], sm.st[buf], nbv, guard2, acc_r,
                            acc_i, lo_r, lo_i);
     } else {
@@ -368,11 +367,11 @@ __global__ void __launch_bounds__(kThreads, SX ? 2 : 4)
   }
 }
 
-template <int BCH, bool MIXED, bool GUARD = false>
+template <int BCH, bool MIXED, bool GUARD = false, int K = 3>
 int bandloop_per_sm(int *per_sm) {
   using Smem = BandSmem<BCH, MIXED>;
   const size_t smem = sizeof(Smem);
-  auto kfn = gpp_bandloop_kernel<BCH, MIXED, GUARD>;
+  auto kfn = gpp_bandloop_kernel<BCH, MIXED, GUARD, K>;
   BGW_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   BGW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kfn, BandCfg<MIXED>::kNT, smem));
   return *per_sm >= 1 ? BGW_OK : BGW_ERR_UNSUPPORTED;
@@ -380,10 +379,10 @@ int bandloop_per_sm(int *per_sm) {
 
 // Launches the band loop over rows [0, P) of the given (already offset)
 // arrays; writes `grid` partials (6 doubles each) starting at `partials`.
-template <int BCH, bool MIXED, bool GUARD>
+template <int BCH, bool MIXED, bool GUARD, int K = 3>
 int launch_bandloop(cudaStream_t stream, int max_grid, int nb, int G, const double2 *wt, const double2 *ie,
                     const double2 *st, const double4 *wx4, int64_t P, double *partials, int *grid_out,
-                    int *status, double guard2, double guard_d) {
+                    int *status, double guard2) {
   using Smem = BandSmem<BCH, MIXED>;
   const size_t smem = sizeof(Smem);
   const int nchunks_g = (int)((G + BandCfg<MIXED>::kCH - 1) / BandCfg<MIXED>::kCH);
@@ -391,11 +390,53 @@ int launch_bandloop(cudaStream_t stream, int max_grid, int nb, int G, const doub
   long long grid = std::min<long long>(items, (long long)max_grid);
   if (grid < 1) grid = 1;
   *grid_out = (int)grid;
-  gpp_bandloop_kernel<BCH, MIXED, GUARD><<<(int)grid, BandCfg<MIXED>::kNT, smem, stream>>>(
-      nb, G, items, nchunks_g, wt, ie, st, wx4, partials, status, guard2, guard_d, stall_step());
+  gpp_bandloop_kernel<BCH, MIXED, GUARD, K><<<(int)grid, BandCfg<MIXED>::kNT, smem, stream>>>(
+      nb, G, items, nchunks_g, wt, ie, st, wx4, partials, status, guard2, stall_step());
   count_launch();
   BGW_CUDA_TRY(cudaGetLastError());
   return BGW_OK;
+}
+
+// The instantiation a call's options select: FP64 (guarded or not) or mixed
+// with K = opt.mixed_order hoisted terms.
+int bandloop_per_sm_for(const bgw_options &o, int *per_sm) {
+  if (o.precision == BGW_PRECISION_MIXED) {
+    switch (o.mixed_order) {
+      case 0: return bandloop_per_sm<256, true, false, 0>(per_sm);
+      case 1: return bandloop_per_sm<256, true, false, 1>(per_sm);
+      case 2: return bandloop_per_sm<256, true, false, 2>(per_sm);
+      default: return bandloop_per_sm<256, true, false, 3>(per_sm);
+    }
+  }
+  if (o.pole_guard > 0.0) return bandloop_per_sm<256, false, true>(per_sm);
+  return bandloop_per_sm<256, false, false>(per_sm);
+}
+
+int launch_bandloop_for(const bgw_options &o, cudaStream_t stream, int max_grid, int nb, int G, const double2 *wt,
+                        const double2 *ie, const double2 *st, const double4 *wx4, int64_t P, double *partials,
+                        int *grid_out, int *status) {
+  const double guard2 = o.pole_guard * o.pole_guard;
+  if (o.precision == BGW_PRECISION_MIXED) {
+    switch (o.mixed_order) {
+      case 0:
+        return launch_bandloop<256, true, false, 0>(stream, max_grid, nb, G, wt, ie, st, wx4, P, partials, grid_out,
+                                                    status, guard2);
+      case 1:
+        return launch_bandloop<256, true, false, 1>(stream, max_grid, nb, G, wt, ie, st, wx4, P, partials, grid_out,
+                                                    status, guard2);
+      case 2:
+        return launch_bandloop<256, true, false, 2>(stream, max_grid, nb, G, wt, ie, st, wx4, P, partials, grid_out,
+                                                    status, guard2);
+      default:
+        return launch_bandloop<256, true, false, 3>(stream, max_grid, nb, G, wt, ie, st, wx4, P, partials, grid_out,
+                                                    status, guard2);
+    }
+  }
+  if (o.pole_guard > 0.0)
+    return launch_bandloop<256, false, true>(stream, max_grid, nb, G, wt, ie, st, wx4, P, partials, grid_out, status,
+                                             guard2);
+  return launch_bandloop<256, false, false>(stream, max_grid, nb, G, wt, ie, st, wx4, P, partials, grid_out, status,
+                                            0.0);
 }
 
 }  // namespace
@@ -442,9 +483,7 @@ int gpp_enqueue_chunks(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int
   } else {
     int per_sm = 0;
     // Also sets the launched instantiation's shared-memory limit.
-    if (mixed) BGW_TRY((bandloop_per_sm<256, true, false>(&per_sm)));
-    else if (guard) BGW_TRY((bandloop_per_sm<256, false, true>(&per_sm)));
-    else BGW_TRY((bandloop_per_sm<256, false, false>(&per_sm)));
+    BGW_TRY(bandloop_per_sm_for(env->opt, &per_sm));
     per_launch = ws->sm_count * per_sm;
   }
   void *partials_v = nullptr, *tab = nullptr, *wx4 = nullptr;
@@ -500,18 +539,8 @@ int gpp_enqueue_chunks(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int
       BGW_CUDA_TRY(cudaGetLastError());
       if (c == 0) BGW_TRY(prof_mark(env, 1));
       int grid = 0;
-      const double4 *w4 = (const double4 *)wx4;
-      const double gd = env->opt.pole_guard;
-      if (mixed) {
-        BGW_TRY((launch_bandloop<256, true, false>(stream, per_launch, (int)nb, (int)G, wt_c, ie_c, st_c, w4, rows,
-                                                   part_c, &grid, env->d_status, guard2, gd)));
-      } else if (guard) {
-        BGW_TRY((launch_bandloop<256, false, true>(stream, per_launch, (int)nb, (int)G, wt_c, ie_c, st_c, w4, rows,
-                                                   part_c, &grid, env->d_status, guard2, gd)));
-      } else {
-        BGW_TRY((launch_bandloop<256, false, false>(stream, per_launch, (int)nb, (int)G, wt_c, ie_c, st_c, w4, rows,
-                                                    part_c, &grid, env->d_status, 0.0, 0.0)));
-      }
+      BGW_TRY(launch_bandloop_for(env->opt, stream, per_launch, (int)nb, (int)G, wt_c, ie_c, st_c,
+                                  (const double4 *)wx4, rows, part_c, &grid, env->d_status));
       total += grid;
     }
   }
@@ -585,11 +614,9 @@ int gpp_run_host(CallEnv *env, int64_t nb, int64_t P, int64_t G, const int32_t *
                         (env->opt.gpp_algorithm == BGW_GPP_AUTO && wx_stride == 0 &&
                          env->opt.precision == BGW_PRECISION_FP64);
   if (!factored && rc.n > 1) {
-    const bool mixed = env->opt.precision == BGW_PRECISION_MIXED, guard = env->opt.pole_guard > 0.0;
+    const bool mixed = env->opt.precision == BGW_PRECISION_MIXED;
     int per_sm = 0;
-    if (mixed) BGW_TRY((bandloop_per_sm<256, true, false>(&per_sm)));
-    else if (guard) BGW_TRY((bandloop_per_sm<256, false, true>(&per_sm)));
-    else BGW_TRY((bandloop_per_sm<256, false, false>(&per_sm)));
+    BGW_TRY(bandloop_per_sm_for(env->opt, &per_sm));
     const int64_t ctas = (int64_t)ws->sm_count * std::max(per_sm, 1);
     const int64_t kch = mixed ? BandCfg<true>::kCH : BandCfg<false>::kCH;
     const int64_t ng = std::max<int64_t>(1, (G + kch - 1) / kch);

@@ -16,8 +16,10 @@
 // Tuning.  The elements per thread (kE) and with it the chunk width and the
 // occupancy are chosen per batch by timing the candidate kernels on a sample
 // prefix of the work list (bgw_gpp_batch_create): FP64 8, 4 or 2 (8: one CTA
-// per SM, the per-band combination amortised over 24 terms), mixed 8 or 4;
-// choices are cached per batch signature for the process.
+// per SM, the per-band combination amortised over 24 terms); choices are
+// cached per batch signature for the process.  The mixed form (the hoisted
+// expansion of the single-instance band loop, K = mixed_order) runs at 8
+// elements per thread, as the single-instance kernel does.
 #include <algorithm>
 #include <climits>
 #include <cmath>
@@ -120,10 +122,9 @@ struct BatchSmem {
   double2 st[2][BCH];
   double4 wx[2][BCH];
   unsigned long long bar[3];  // [2]: never arrived on (stall injection)
-  double red[(kBThreads / 32) * 6];
+  double red[(kBThreads / 32) * 18];
   double xr_lo[kBThreads / 32], xr_hi[kBThreads / 32];  // MIXED: chunk frequency range
-  float4 xf[MIXED ? BCH : 1];                            // MIXED: FP32 frequency rows
-  float2 sf[MIXED ? BCH : 1];                            // MIXED: FP32 sch_store1
+  RemRow rows[MIXED ? BCH : 1];                          // MIXED: per-band remainder rows
 };
 
 // Flushes the running sums of instance slot `seg` of this CTA.
@@ -142,7 +143,7 @@ __device__ __forceinline__ void flush(double (&acc_r)[3], double (&acc_i)[3], do
 
 // Band loop over this CTA's range [range[b], range[b+1]) of the global item
 // list.  Steps are (item, band chunk); step s+1 is staged while s computes.
-template <int BCH, int KE, bool MIXED>
+template <int BCH, int KE, bool MIXED, int K = 3>
 __global__ void __launch_bounds__(kBThreads, KE == 8 ? 1 : 2)
     batch_bandloop_kernel(const BatchInst *__restrict__ inst, int n, const long long *__restrict__ range,
                           int max_seg, double *__restrict__ partials, int *status, long long stall) {
@@ -224,11 +225,11 @@ __global__ void __launch_bounds__(kBThreads, KE == 8 ? 1 : 2)
     const int nbv = max(0, min(BCH, I.nb - cur.c * BCH));
     // MIXED: elements near the chunk's frequencies are summed in FP64.
     if constexpr (MIXED) {
-      Elem<float> e[KE];
-      load_elems<float, KE>(e, sm.wt[buf], sm.ie[buf], nvalid, kBThreads, tid);
-      const double2 xr = stage_mixed_rows<kBThreads>(sm.wx[buf], sm.st[buf], nbv, sm.xf, sm.sf, sm.xr_lo, sm.xr_hi);
-      const uint32_t near = near_elems<KE>(e, sm.wt[buf], nvalid, kBThreads, tid, xr, 0.0);
-      band_sweep_mixed<KE>(e, sm.xf, sm.sf, nbv, acc_r, acc_i, lo_r, lo_i);
+      const RemStep rs = rem_stage<kBThreads, K>(sm.wx[buf], sm.st[buf], nbv, sm.rows, sm.red, sm.xr_lo, sm.xr_hi);
+      RemElems<KE> e;
+      const uint32_t near = rem_elems<KE, K>(e, sm.wt[buf], sm.ie[buf], nvalid, kBThreads, tid, rs, 0.0, acc_r,
+                                             acc_i);
+      rem_sweep<KE>(e, sm.rows, nbv, acc_r, acc_i, lo_r, lo_i);
       if (near) near_sweep(near, sm.wt[buf], sm.ie[buf], kBThreads, tid, sm.wx[buf], sm.st[buf], nbv, 0.0, acc_r,
                            acc_i, lo_r, lo_i);
     } else {
@@ -356,21 +357,21 @@ struct Variant {
   int per_sm;      // resident CTAs per SM
 };
 
-template <int KE, bool MIXED>
+template <int KE, bool MIXED, int K = 3>
 int band_variant(Variant *v) {
   v->ke = KE;
   v->smem = sizeof(BatchSmem<256, KE, MIXED>);
-  auto kfn = batch_bandloop_kernel<256, KE, MIXED>;
+  auto kfn = batch_bandloop_kernel<256, KE, MIXED, K>;
   BGW_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v->smem));
   BGW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v->per_sm, kfn, kBThreads, v->smem));
   return v->per_sm >= 1 ? BGW_OK : BGW_ERR_UNSUPPORTED;
 }
 
-template <int KE, bool MIXED>
+template <int KE, bool MIXED, int K = 3>
 void launch_band(cudaStream_t s, int grid, size_t smem, const BatchInst *inst, int n, const long long *range,
                  int max_seg, double *partials, int *status, long long stall) {
-  batch_bandloop_kernel<256, KE, MIXED><<<grid, kBThreads, smem, s>>>(inst, n, range, max_seg, partials, status,
-                                                                      stall);
+  batch_bandloop_kernel<256, KE, MIXED, K><<<grid, kBThreads, smem, s>>>(inst, n, range, max_seg, partials, status,
+                                                                         stall);
 }
 
 std::mutex g_tune_mu;
@@ -384,6 +385,7 @@ struct bgw_gpp_batch {
   int device = 0;
   int n = 0;
   bool factored = false, mixed = false;
+  int mixed_order = 3;
   int ke = 4;
   int grid = 1;
   int max_seg = 1;
@@ -483,10 +485,11 @@ int enqueue_batch(bgw_gpp_batch *B, cudaStream_t s, long long stall = -1) {
     batch_wx_kernel<<<std::min(ninst, 1024), 256, 0, s>>>(B->d_inst, ninst);
     BGW_CUDA_TRY(cudaGetLastError());
     if (B->mixed) {
-      if (B->ke == 8) launch_band<8, true>(s, B->grid, B->smem, B->d_inst, ninst, B->d_range, B->max_seg,
-                                          B->d_partials, B->d_status, stall);
-      else launch_band<4, true>(s, B->grid, B->smem, B->d_inst, ninst, B->d_range, B->max_seg, B->d_partials,
-                                B->d_status, stall);
+      auto *fn = B->mixed_order == 0   ? launch_band<8, true, 0>
+                 : B->mixed_order == 1 ? launch_band<8, true, 1>
+                 : B->mixed_order == 2 ? launch_band<8, true, 2>
+                                       : launch_band<8, true, 3>;
+      fn(s, B->grid, B->smem, B->d_inst, ninst, B->d_range, B->max_seg, B->d_partials, B->d_status, stall);
     } else {
       if (B->ke == 8) launch_band<8, false>(s, B->grid, B->smem, B->d_inst, ninst, B->d_range, B->max_seg,
                                            B->d_partials, B->d_status, stall);
@@ -587,10 +590,14 @@ extern "C" int bgw_gpp_batch_create(const bgw_gpp_instance *instances, int64_t n
   if (factored) {
     cands.push_back({4, 0, 8});
   } else if (mixed) {
-    Variant a, b;
-    BGW_TRY((band_variant<8, true>(&a)));
-    BGW_TRY((band_variant<4, true>(&b)));
-    cands = {a, b};
+    Variant a;
+    switch (env.opt.mixed_order) {
+      case 0: BGW_TRY((band_variant<8, true, 0>(&a))); break;
+      case 1: BGW_TRY((band_variant<8, true, 1>(&a))); break;
+      case 2: BGW_TRY((band_variant<8, true, 2>(&a))); break;
+      default: BGW_TRY((band_variant<8, true, 3>(&a))); break;
+    }
+    cands = {a};
   } else {
     Variant a, b, c;
     BGW_TRY((band_variant<8, false>(&a)));
@@ -605,6 +612,7 @@ extern "C" int bgw_gpp_batch_create(const bgw_gpp_instance *instances, int64_t n
   B->n = (int)n;
   B->factored = factored;
   B->mixed = mixed;
+  B->mixed_order = env.opt.mixed_order;
 
   auto layout = [&](const Variant &v, long long limit, std::vector<long long> *range, std::vector<int> *cta_lo,
                     int *grid, int *max_seg) {
@@ -671,7 +679,8 @@ extern "C" int bgw_gpp_batch_create(const bgw_gpp_instance *instances, int64_t n
 
   // Autotune: time each candidate on a sample prefix (about 1/16 of the
   // items, at least one item per CTA) unless this signature is cached.
-  std::string sig = std::string(factored ? "F" : (mixed ? "M" : "D")) + std::to_string(env.device);
+  std::string sig = std::string(factored ? "F" : (mixed ? "M" + std::to_string(env.opt.mixed_order) : "D")) +
+                    std::to_string(env.device);
   for (auto &I : h) sig += ":" + std::to_string(I.nb) + "x" + std::to_string(I.P) + "x" + std::to_string(I.G);
   int chosen = -1;
   {

@@ -49,12 +49,6 @@ struct Elem {
   T wr, wi2, Ir, Ii, a, b;
 };
 
-__device__ __forceinline__ float rcp_approx_f32(float d) {
-  float y;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(d));
-  return y;
-}
-
 // Error-free transformation of a + b (Knuth's TwoSum, TAOCP vol. 2,
 // 4.2.2): hi + lo == a + b exactly, no ordering assumption.
 __device__ __forceinline__ void two_sum_acc(double &hi, double &lo, double b) {
@@ -95,7 +89,7 @@ __device__ __forceinline__ void load_elems(Elem<T> (&e)[kE], const double2 *__re
 // nbv bands, the kE x 3 quotients q = conj(wdiff) I_eps / |wdiff|^2 of this
 // thread's elements are summed (reciprocal by rcp_refined) and multiplied by
 // sch_store1 (st[b]), and the product is accumulated per frequency.  (The
-// mixed form is band_sweep_mixed below.)
+// mixed form is rem_stage / rem_elems / rem_sweep below.)
 // GUARD: a term with |wdiff|^2 < guard2 contributes zero (near-pole cut-off;
 // the select discards the reciprocal, so a zero |wdiff| yields no NaN).
 template <int kE, bool GUARD = false>
@@ -131,32 +125,57 @@ __device__ __forceinline__ void band_sweep(const Elem<double> (&e)[kE], const do
   }
 }
 
-// ------------------------------------------- mixed band loop near poles --
-// The FP32 quotient's error grows like eps32 (|x| + |wr|) / |x - wr|: near a
-// pole the subtraction cancels.  The mixed band loop therefore sends every
-// element whose wtilde real part wr lies near the band chunk's frequency
-// range to an FP64 path.  With the chunk's frequencies in [lo, hi], an
-// element is "far" when
-//   wr >= hi + max(kNearFrac |hi|, delta)   or   wr <= lo - max(kNearFrac |lo|, delta);
-// then every term has |x - wr| >= kNearFrac |x| (so the FP32 relative error
-// is at most eps32 (2 / kNearFrac + 1)) and |wdiff| >= |x - wr| >= delta (so
-// the near-pole guard cannot fire and the FP32 path needs no test).  Near
-// elements are zeroed in the FP32 copy and summed in FP64, guard included.
-constexpr double kNearFrac = 0.25;
+// ----------------------------------- mixed band loop: hoisted expansion --
+//
+// The mixed-precision band loop evaluates each element's quotients about a
+// centre c of the step's band-chunk frequencies.  With w = wtilde[p][ig],
+// I = I_eps[p][ig], u = 1 / (c - w), Q0 = I u, delta = x - c and t = delta u,
+//   q = I / (x - w) = Q0 / (1 + t)
+//     = Q0 sum_{k<K} (-t)^k + (-t)^K Q0 / (1 + t)             (exact, any K),
+// so the band sum of a (p, ig) element is
+//   sum_b s_b q_b = Q0 sum_{k<K} (-u)^k S_k + sum_b s_b (-delta_b)^K (X + delta_b Y) / |1 + t_b|^2,
+// with band moments S_k = sum_b s_b delta_b^k (FP64, once per step),
+// X = Q0 u^K, Y = X conj(u) (per element) and |1 + t|^2 = 1 + 2 delta Re u +
+// delta^2 |u|^2.  The first part (the K hoisted Taylor terms) is evaluated in
+// FP64 once per element and step; the remainder is a per-term complex
+// quotient evaluated in FP32, whose value is |t|^K of the term, so its
+// FP32 rounding costs ~eps32 |t|^K of the term instead of eps32.  K = 0 is a
+// plain FP32 quotient.  Elements with |t| > kRemTau for some term of the
+// step (near a pole) take the FP64 path (near_sweep), as do elements a
+// pole_guard cut could reach.
+//
+// The remainder's denominators lie in [(1 - tau)^2, (1 + tau)^2], so one
+// reciprocal serves the three frequencies of an element: with d0, d1, d2,
+// R = 1 / (d0 d1 d2), 1/d0 = d1 d2 R, 1/d1 = d0 d2 R, 1/d2 = d0 d1 R (no
+// overflow or underflow can occur in that range).  Two elements are
+// processed per packed f32x2 instruction.
+constexpr double kRemTau = 0.125;
 
-// Per step of the mixed band loop: FP32 copies of the chunk's nbv frequency
-// rows (xf) and sch_store1 values (sf), and [lo, hi] of its frequencies,
-// broadcast to every thread (all threads must call; two warp-level folds and
-// one barrier, which also publishes xf / sf).
-template <int kThreads>
-__device__ __forceinline__ double2 stage_mixed_rows(const double4 *__restrict__ wx, const double2 *__restrict__ st,
-                                                    int nbv, float4 *xf, float2 *sf, double *s_lo, double *s_hi) {
+// Per band of a step: (2 delta, 2 delta), (delta^2, delta^2), (delta, delta)
+// for each frequency, and the band multiplier m = s_b (-delta)^K split into
+// (Re m, Re m), (Im m, Im m), (-Im m, -Im m) (pairs: operands of f32x2 ops).
+struct RemRow {
+  float2 d2x[3], dd[3], d[3], mr[3], mi[3], nmi[3];
+};
+
+// Centre, half-width and FP64 band moments of a step.
+struct RemStep {
+  double c, dmax;
+  double2 S[3][3];  // S[k][iw] = sum_b s_b delta_b^k (k < 3)
+};
+
+// Every thread calls: folds the frequency range of the step's nbv bands,
+// writes rows[b] and returns the centre, half-width and moments (identical
+// in every thread; fixed summation order).  red: (kThreads / 32) * 18
+// doubles; s_lo / s_hi: kThreads / 32 doubles each.
+template <int kThreads, int K>
+__device__ __forceinline__ RemStep rem_stage(const double4 *__restrict__ wx, const double2 *__restrict__ st, int nbv,
+                                             RemRow *rows, double *red, double *s_lo, double *s_hi) {
+  constexpr int kW = kThreads / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double lo = INFINITY, hi = -INFINITY;
   for (int b = threadIdx.x; b < nbv; b += kThreads) {
     const double4 w = wx[b];
-    const double2 v = st[b];
-    xf[b] = make_float4((float)w.x, (float)w.y, (float)w.z, 0.f);
-    sf[b] = make_float2((float)v.x, (float)v.y);
     lo = fmin(lo, fmin(w.x, fmin(w.y, w.z)));
     hi = fmax(hi, fmax(w.x, fmax(w.y, w.z)));
   }
@@ -165,89 +184,216 @@ __device__ __forceinline__ double2 stage_mixed_rows(const double4 *__restrict__ 
     lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
     hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
   }
-  if ((threadIdx.x & 31) == 0) {
-    s_lo[threadIdx.x >> 5] = lo;
-    s_hi[threadIdx.x >> 5] = hi;
+  if (lane == 0) {
+    s_lo[warp] = lo;
+    s_hi[warp] = hi;
   }
   __syncthreads();
 #pragma unroll
-  for (int w = 0; w < kThreads / 32; ++w) {
+  for (int w = 0; w < kW; ++w) {
     lo = fmin(lo, s_lo[w]);
     hi = fmax(hi, s_hi[w]);
   }
-  return make_double2(lo, hi);
-}
-
-// The band sweep of the mixed band loop: the quotients of band_sweep in
-// FP32 (rcp.approx.ftz.f32), their products with sch_store1 summed in FP32
-// over groups of kGroup bands, each group sum added to the FP64 accumulators
-// with TwoSum (one conversion and two TwoSums per kGroup bands and
-// frequency: the XU and FP64 pipes stay free for the reciprocals, which
-// bound this loop).
-template <int kE>
-__device__ __forceinline__ void band_sweep_mixed(const Elem<float> (&e)[kE], const float4 *__restrict__ xf,
-                                                 const float2 *__restrict__ sf, int nbv, double (&acc_r)[3],
-                                                 double (&acc_i)[3], double (&lo_r)[3], double (&lo_i)[3]) {
-  constexpr int kGroup = 8;
-  for (int b0 = 0; b0 < nbv; b0 += kGroup) {
-    const int b1 = min(b0 + kGroup, nbv);
-    float gr[3] = {0.f, 0.f, 0.f}, gi[3] = {0.f, 0.f, 0.f};
-    for (int bb = b0; bb < b1; ++bb) {
-      const float4 w4 = xf[bb];
-      const float x[3] = {w4.x, w4.y, w4.z};
-      const float2 s = sf[bb];
-      float tr[3] = {0.f, 0.f, 0.f}, ti[3] = {0.f, 0.f, 0.f};
+  RemStep r;
+  r.c = 0.5 * (lo + hi);
+  r.dmax = 0.5 * (hi - lo);
+  // Moments: v[(k * 3 + iw) * 2 + {re, im}] = sum_b s_b delta^k.
+  double v[18];
 #pragma unroll
-      for (int k = 0; k < kE; ++k) {
-#pragma unroll
-        for (int iw = 0; iw < 3; ++iw) {
-          const float dr = x[iw] - e[k].wr;
-          const float r = rcp_approx_f32(fmaf(dr, dr, e[k].wi2));
-          tr[iw] = fmaf(fmaf(dr, e[k].Ir, e[k].a), r, tr[iw]);
-          ti[iw] = fmaf(fmaf(dr, e[k].Ii, e[k].b), r, ti[iw]);
-        }
-      }
-#pragma unroll
-      for (int iw = 0; iw < 3; ++iw) {
-        gr[iw] = fmaf(tr[iw], s.x, gr[iw]);
-        gr[iw] = fmaf(-ti[iw], s.y, gr[iw]);
-        gi[iw] = fmaf(tr[iw], s.y, gi[iw]);
-        gi[iw] = fmaf(ti[iw], s.x, gi[iw]);
-      }
-    }
+  for (int i = 0; i < 18; ++i) v[i] = 0.0;
+  for (int b = threadIdx.x; b < nbv; b += kThreads) {
+    const double4 w4 = wx[b];
+    const double x[3] = {w4.x, w4.y, w4.z};
+    const double2 sb = st[b];
+    RemRow row;
 #pragma unroll
     for (int iw = 0; iw < 3; ++iw) {
-      two_sum_acc(acc_r[iw], lo_r[iw], (double)gr[iw]);
-      two_sum_acc(acc_i[iw], lo_i[iw], (double)gi[iw]);
+      const double d = x[iw] - r.c, d2 = d * d;
+      double pk = 1.0;  // (-delta)^K
+#pragma unroll
+      for (int k = 0; k < K; ++k) pk *= -d;
+      const float fd = (float)d, fd2 = (float)d2, f2d = (float)(2.0 * d);
+      row.d2x[iw] = make_float2(f2d, f2d);
+      row.dd[iw] = make_float2(fd2, fd2);
+      row.d[iw] = make_float2(fd, fd);
+      const float mr = (float)(sb.x * pk), mi = (float)(sb.y * pk);
+      row.mr[iw] = make_float2(mr, mr);
+      row.mi[iw] = make_float2(mi, mi);
+      row.nmi[iw] = make_float2(-mi, -mi);
+      v[(0 * 3 + iw) * 2 + 0] += sb.x;
+      v[(0 * 3 + iw) * 2 + 1] += sb.y;
+      v[(1 * 3 + iw) * 2 + 0] += sb.x * d;
+      v[(1 * 3 + iw) * 2 + 1] += sb.y * d;
+      v[(2 * 3 + iw) * 2 + 0] += sb.x * d2;
+      v[(2 * 3 + iw) * 2 + 1] += sb.y * d2;
     }
+    rows[b] = row;
   }
+  // Every thread forms the same totals: warp butterflies, then the warp
+  // partials in warp order.
+#pragma unroll
+  for (int i = 0; i < 18; ++i) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_xor_sync(0xffffffffu, v[i], o);
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int i = 0; i < 18; ++i) red[warp * 18 + i] = v[i];
+  }
+  __syncthreads();  // also publishes rows[]
+#pragma unroll
+  for (int i = 0; i < 18; ++i) {
+    double t = red[i];
+    for (int w = 1; w < kW; ++w) t += red[w * 18 + i];
+    v[i] = t;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int iw = 0; iw < 3; ++iw) r.S[k][iw] = make_double2(v[(k * 3 + iw) * 2], v[(k * 3 + iw) * 2 + 1]);
+  return r;
 }
 
-// Marks this thread's near elements (bit k for element k) and zeroes their
-// FP32 copies (the padding values: they then add exactly zero).
+// Per-element FP32 constants of the remainder, two elements per pair.
 template <int kE>
-__device__ __forceinline__ uint32_t near_elems(Elem<float> (&e)[kE], const double2 *__restrict__ wt, int nvalid,
-                                               int nthreads, int tid, double2 xr, double guard_d) {
-  const double m = 1.0 + 1e-9;  // covers the rounding of the bounds below
-  const double blo = xr.x - fmax(kNearFrac * fabs(xr.x), guard_d) * m;
-  const double bhi = xr.y + fmax(kNearFrac * fabs(xr.y), guard_d) * m;
+struct RemElems {
+  float2 ur[kE / 2], uu[kE / 2], Xr[kE / 2], Xi[kE / 2], Yr[kE / 2], Yi[kE / 2];
+};
+
+__device__ __forceinline__ double2 cmulc(double2 a, double2 b) {  // a * conj(b)
+  return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+
+// This thread's kE elements of the staged chunk (element k is chunk index
+// k * nthreads + tid): the FP64 hoisted part is added to acc_r / acc_i, the
+// FP32 constants of the remainder are set, and the near elements (returned
+// as a bit mask) get zero constants (their remainder then adds exactly
+// zero).  guard2 > 0: elements a pole_guard cut could reach are near too.
+template <int kE, int K>
+__device__ __forceinline__ uint32_t rem_elems(RemElems<kE> &e, const double2 *__restrict__ wt,
+                                              const double2 *__restrict__ ie, int nvalid, int nthreads, int tid,
+                                              const RemStep &r, double guard2, double (&acc_r)[3],
+                                              double (&acc_i)[3]) {
   uint32_t near = 0;
+  const double tau2 = kRemTau * kRemTau, far2 = (1.0 - kRemTau) * (1.0 - kRemTau);
 #pragma unroll
   for (int k = 0; k < kE; ++k) {
+    float ur = 0.f, uu = 0.f, xr = 0.f, xi = 0.f, yr = 0.f, yi = 0.f;
     const int idx = k * nthreads + tid;
     if (idx < nvalid) {
-      const double wr = wt[idx].x;
-      if (wr > blo && wr < bhi) {
+      const double2 w = wt[idx], v = ie[idx];
+      const double dr = r.c - w.x;
+      const double D = fma(dr, dr, w.y * w.y);  // |c - w|^2
+      const double rD = rcp_refined(D);
+      // |t| <= dmax |u| <= tau for every term; a guard cut needs
+      // |x - w| >= (1 - tau) / |u| < delta.  (D = 0 is near: rD = inf.)
+      const bool is_near = !(r.dmax * r.dmax * rD <= tau2) || (guard2 > 0.0 && guard2 * rD > far2);
+      if (is_near) {
         near |= 1u << k;
-        e[k].wr = 0.f;
-        e[k].wi2 = 1.f;
-        e[k].Ir = e[k].Ii = e[k].a = e[k].b = 0.f;
+      } else {
+        const double2 u = make_double2(dr * rD, w.y * rD);  // 1 / (c - w)
+        const double2 Q0 = cmul(v, u);
+        const double2 mu = make_double2(-u.x, -u.y);
+#pragma unroll
+        for (int iw = 0; iw < 3; ++iw) {
+          // Q0 (S_0 + (-u) (S_1 + (-u) S_2)) truncated to K terms (Horner).
+          double2 h = make_double2(0.0, 0.0);
+#pragma unroll
+          for (int j = K - 1; j >= 0; --j) {
+            const double2 t = cmul(mu, h);
+            h = make_double2(r.S[j][iw].x + t.x, r.S[j][iw].y + t.y);
+          }
+          const double2 p = cmul(Q0, h);
+          acc_r[iw] += p.x;
+          acc_i[iw] += p.y;
+        }
+        double2 X = Q0;
+#pragma unroll
+        for (int j = 0; j < K; ++j) X = cmul(X, u);
+        const double2 Y = cmulc(X, u);
+        ur = (float)u.x;
+        uu = (float)rD;  // |u|^2 = 1 / |c - w|^2
+        xr = (float)X.x;
+        xi = (float)X.y;
+        yr = (float)Y.x;
+        yi = (float)Y.y;
       }
+    }
+    if (k & 1) {
+      e.ur[k >> 1].y = ur, e.uu[k >> 1].y = uu, e.Xr[k >> 1].y = xr, e.Xi[k >> 1].y = xi;
+      e.Yr[k >> 1].y = yr, e.Yi[k >> 1].y = yi;
+    } else {
+      e.ur[k >> 1].x = ur, e.uu[k >> 1].x = uu, e.Xr[k >> 1].x = xr, e.Xi[k >> 1].x = xi;
+      e.Yr[k >> 1].x = yr, e.Yi[k >> 1].x = yi;
     }
   }
   return near;
 }
 
+// The remainder's band sweep: for each band, T_iw = sum over this thread's
+// elements of (X + delta Y) / |1 + t|^2 (packed FP32, one reciprocal per
+// element for the three frequencies), times the band multiplier m; the
+// products are summed in FP32 over groups of kRemGroup bands and each group
+// sum is added to the FP64 accumulators with TwoSum.
+constexpr int kRemGroup = 8;
+
+__device__ __forceinline__ float rcp_f32(float d) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(d));
+  return y;
+}
+
+template <int kE>
+__device__ __forceinline__ void rem_sweep(const RemElems<kE> &e, const RemRow *__restrict__ rows, int nbv,
+                                          double (&acc_r)[3], double (&acc_i)[3], double (&lo_r)[3],
+                                          double (&lo_i)[3]) {
+  const float2 one = make_float2(1.f, 1.f);
+  for (int b0 = 0; b0 < nbv; b0 += kRemGroup) {
+    const int b1 = min(b0 + kRemGroup, nbv);
+    float2 gr[3], gi[3];
+#pragma unroll
+    for (int iw = 0; iw < 3; ++iw) gr[iw] = gi[iw] = make_float2(0.f, 0.f);
+    for (int b = b0; b < b1; ++b) {
+      const RemRow &R = rows[b];
+      float2 tr[3], ti[3];
+#pragma unroll
+      for (int iw = 0; iw < 3; ++iw) tr[iw] = ti[iw] = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int q = 0; q < kE / 2; ++q) {
+        float2 den[3];
+#pragma unroll
+        for (int iw = 0; iw < 3; ++iw) den[iw] = __ffma2_rn(R.dd[iw], e.uu[q], __ffma2_rn(R.d2x[iw], e.ur[q], one));
+        const float2 d12 = __fmul2_rn(den[1], den[2]);
+        const float2 P = __fmul2_rn(den[0], d12);
+        const float2 Ri = make_float2(rcp_f32(P.x), rcp_f32(P.y));
+        const float2 t0 = __fmul2_rn(den[0], Ri);
+        float2 rc[3];
+        rc[0] = __fmul2_rn(d12, Ri);
+        rc[1] = __fmul2_rn(den[2], t0);
+        rc[2] = __fmul2_rn(den[1], t0);
+#pragma unroll
+        for (int iw = 0; iw < 3; ++iw) {
+          const float2 nr = __ffma2_rn(R.d[iw], e.Yr[q], e.Xr[q]);
+          const float2 ni = __ffma2_rn(R.d[iw], e.Yi[q], e.Xi[q]);
+          tr[iw] = __ffma2_rn(nr, rc[iw], tr[iw]);
+          ti[iw] = __ffma2_rn(ni, rc[iw], ti[iw]);
+        }
+      }
+#pragma unroll
+      for (int iw = 0; iw < 3; ++iw) {
+        gr[iw] = __ffma2_rn(R.mr[iw], tr[iw], __ffma2_rn(R.nmi[iw], ti[iw], gr[iw]));
+        gi[iw] = __ffma2_rn(R.mr[iw], ti[iw], __ffma2_rn(R.mi[iw], tr[iw], gi[iw]));
+      }
+    }
+#pragma unroll
+    for (int iw = 0; iw < 3; ++iw) {
+      two_sum_acc(acc_r[iw], lo_r[iw], (double)gr[iw].x + (double)gr[iw].y);
+      two_sum_acc(acc_i[iw], lo_i[iw], (double)gi[iw].x + (double)gi[iw].y);
+    }
+  }
+}
+
+// ------------------------------------------- mixed band loop near poles --
 // The FP64 sum of the near elements over the chunk's bands, each product
 // with sch_store1 added to the TwoSum accumulators; terms with |wdiff|^2 <
 // guard2 are skipped (guard2 = 0: none).

@@ -142,6 +142,7 @@ int begin_call(const bgw_options *user, CallEnv *env) {
     return BGW_ERR_INVALID_ARG;
   if (o.wx_band_stride < 0) return BGW_ERR_INVALID_ARG;
   if (!(o.pole_guard >= 0.0) || !std::isfinite(o.pole_guard)) return BGW_ERR_INVALID_ARG;
+  if (o.mixed_order < 0 || o.mixed_order > 3) return BGW_ERR_INVALID_ARG;
   if ((o.flags & BGW_FLAG_ASYNC) && (o.memory != BGW_MEMORY_DEVICE || o.device_status == nullptr))
     return BGW_ERR_INVALID_ARG;
   if ((o.flags & BGW_FLAG_PROFILE) && (o.flags & BGW_FLAG_ASYNC)) return BGW_ERR_INVALID_ARG;
@@ -280,6 +281,7 @@ void bgw_options_init(bgw_options *opt) {
   opt->stream = nullptr;
   opt->device_status = nullptr;
   opt->pole_guard = 0.0;
+  opt->mixed_order = 3;
 }
 
 const char *bgw_status_string(int status) {

@@ -32,9 +32,10 @@
 extern "C" {
 #endif
 
-/* 2: bgw_options gained pole_guard (bgw_options_init writes the whole
- * current struct, so it must be given a struct of this header's size). */
-#define BGW_SIGMA_ABI_VERSION 2
+/* 2: bgw_options gained pole_guard; 3: bgw_options gained mixed_order
+ * (bgw_options_init writes the whole current struct, so it must be given a
+ * struct of this header's size). */
+#define BGW_SIGMA_ABI_VERSION 3
 
 typedef enum bgw_status {
   BGW_OK = 0,
@@ -92,23 +93,37 @@ typedef struct bgw_options {
   void *stream;            /* cudaStream_t; NULL = legacy default stream    */
   int32_t *device_status;  /* device int written with BGW_FLAG_ASYNC        */
   double pole_guard;       /* GPP near-pole guard delta >= 0; 0 = off       */
+  int32_t mixed_order;     /* GPP band loop, BGW_PRECISION_MIXED: Taylor
+                              terms K (0..3) hoisted into FP64; default 3  */
 } bgw_options;
+/* mixed_order (GPP band loop with BGW_PRECISION_MIXED; not in the
+ * reference): each step's quotients q = I / (x - w) are expanded about the
+ * centre c of the step's band-chunk frequencies, t = (x - c) / (c - w):
+ *   q = Q0 (1 - t + ... + (-t)^(K-1)) + (-t)^K Q0 / (1 + t),  Q0 = I / (c - w).
+ * The K leading terms are summed over bands exactly, in FP64, through band
+ * moments; the remainder, |t|^K of the term, is a per-term complex quotient
+ * evaluated in FP32, so its rounding costs about 1e-7 |t|^K of the term.
+ * K = 0 is a plain FP32 quotient (~1e-7 relative).  Elements with
+ * |t| > 1/8 for some term (near a pole) are summed in FP64.  The cost per
+ * term does not depend on K. */
 /* pole_guard (GPP sums only; not in the reference, which has no guard and
  * only clamps wx >= 1e-6, GPP/gpp.cpp:273-274): with delta > 0 every
  * (band, G', G, frequency) term whose |wdiff|^2 = |wx - wtilde|^2 is below
  * delta^2 contributes zero -- the term's pole is excluded from the sum
  * (principal-value cut-off) instead of growing like 1/|wdiff|.  The test is
- * made on the |wdiff|^2 the kernel computes (FP64, or FP32 with
- * BGW_PRECISION_MIXED).  In bgw_gpp_sigma's asxtemp the cut applies to each
+ * made on |wdiff|^2 in FP64 (with BGW_PRECISION_MIXED, every element a cut
+ * could reach is summed in FP64).  In bgw_gpp_sigma's asxtemp the cut applies to each
  * of the two partial fractions 1/(wx - wtilde) and 1/(-wx - wtilde).
  * Supported by bgw_noflagOCC_solver and bgw_gpp_sigma; the adjoint and the
  * batched calls return BGW_ERR_UNSUPPORTED for delta > 0; the FF calls
  * ignore it.  An entry point given an older, shorter bgw_options (a smaller
- * struct_size, filled by the caller) reads only that many bytes and uses
- * delta = 0; bgw_options_init itself always writes the current layout. */
+ * struct_size, filled by the caller) reads only that many bytes and uses the
+ * defaults (delta = 0, mixed_order = 3) for the fields it lacks;
+ * bgw_options_init itself always writes the current layout. */
 
 /* Fills *opt with the defaults (host memory, FP64, AUTO, stride 0,
- * current device, default stream, synchronous). */
+ * current device, default stream, synchronous, no pole guard, mixed_order
+ * 3). */
 void bgw_options_init(bgw_options *opt);
 
 /* ------------------------------------------------------------------ GPP --

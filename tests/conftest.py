@@ -16,6 +16,9 @@ for p in (PKG, REPO, REPO / "tests" / "golden"):
 
 # Parity bar of the plain FP64 form against the reference / the oracle.
 FP64_RTOL = 1e-12
+# Bar of the mixed-precision GPP band loop (hoisted FP64 expansion terms,
+# FP32 remainder quotients) against the FP64 oracle: 1e-9 relative.
+MIXED_RTOL = 1e-9
 
 
 def pytest_configure(config):

@@ -47,7 +47,7 @@ def test_library_exports_every_header_symbol(bgw):
 
 def test_abi_version_and_status_strings(bgw):
     lib = bgw.load()
-    assert lib.bgw_abi_version() == 2
+    assert lib.bgw_abi_version() == 3
     for code in bgw.STATUS:
         assert lib.bgw_status_string(code)
     assert b"index" in lib.bgw_status_string(-2)

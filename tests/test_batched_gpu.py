@@ -4,7 +4,7 @@ from __future__ import annotations
 
 import numpy as np
 import pytest
-from conftest import FP64_RTOL, rel_err
+from conftest import FP64_RTOL, MIXED_RTOL, rel_err
 
 from bgwsigma import inputs as I
 
@@ -24,7 +24,7 @@ def _batch_inputs(cuda, wx_per_band=False):
 
 
 @pytest.mark.parametrize("algorithm,precision,rtol", [("bandloop", "fp64", FP64_RTOL), ("factored", "fp64", FP64_RTOL),
-                                                      ("bandloop", "mixed", 2e-6)])
+                                                      ("bandloop", "mixed", MIXED_RTOL)])
 def test_batch_matches_oracle_and_single_calls(bgw, oracle, cuda, algorithm, precision, rtol):
     hosts, devs = _batch_inputs(cuda)
     b = bgw.GppBatch(devs, algorithm=algorithm, precision=precision)

@@ -7,7 +7,7 @@ import ctypes
 
 import numpy as np
 import pytest
-from conftest import FP64_RTOL, l2c, rel_err
+from conftest import MIXED_RTOL, FP64_RTOL, l2c, rel_err
 
 from bgwsigma import inputs as I
 from cases import GPP_CASES
@@ -151,10 +151,26 @@ def test_ctypes_invalid_option_struct(bgw, cuda):
     assert st == -1
 
 
-# Mixed precision: FP32 per-term quotients, TwoSum-compensated FP64
-# accumulation.  Tolerance: the FP32 quotient rounding (~2^-24 per term)
-# propagates into the sum; 2e-6 relative is the bar written here.
-MIXED_RTOL = 2e-6
+# Mixed precision: K = 3 Taylor terms of each step's expansion in FP64, the
+# remainder quotients in FP32 (about 1e-7 |t|^3 of a term, |t| <= 1/8), the
+# group sums TwoSum-compensated in FP64.  Bar: MIXED_RTOL = 1e-9 relative.
+
+
+@pytest.mark.parametrize("order,bar", [(0, 2e-6), (1, 1e-7), (2, 1e-8), (3, MIXED_RTOL)])
+def test_mixed_order_error_falls_with_k(bgw, oracle, cuda, order, bar):
+    """mixed_order K: K hoisted Taylor terms; the FP32 remainder is |t|^K of
+    a term.  Band-dependent wx (a shift U[-0.25, 0.25] per band)."""
+    g = I.gpp_seeded(256, 2, 8192, 16, seed=19, wx_per_band=True)
+    got = bgw.noflagOCC_solver(g, precision="mixed", mixed_order=order)
+    assert rel_err(got, oracle.gpp(g)) < bar
+
+
+def test_mixed_order_checked(bgw, cuda):
+    for bad in (-1, 4):
+        with pytest.raises(bgw.BgwError) as e:
+            bgw.noflagOCC_solver(I.gpp_seeded(4, 2, 256, 16), precision="mixed", algorithm="bandloop",
+                                 mixed_order=bad)
+        assert e.value.status == -1
 
 
 @pytest.mark.parametrize("name", ["gpp_small_seeded", "gpp_ragged", "gpp_many_bands", "gpp_small_uniform"])
