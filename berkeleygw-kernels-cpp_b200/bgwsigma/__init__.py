@@ -43,7 +43,7 @@ EXPORTS = ("bgw_options_init", "bgw_noflagOCC_solver", "bgw_achsDtemp_Kernel", "
            "bgw_launch_count", "bgw_measure_fp64_peak", "bgw_release_workspace", "bgw_last_profile",
            "bgw_noflagOCC_solver_noalloc", "bgw_noflagOCC_solver_backward", "bgw_gpp_batch_create",
            "bgw_gpp_batch_execute", "bgw_gpp_batch_info", "bgw_gpp_batch_destroy", "bgw_gpp_sigma",
-           "bgw_debug_inject_stall", "bgw_fill_uniform")
+           "bgw_debug_inject_stall", "bgw_fill_uniform", "bgw_debug_rcp_probe")
 
 
 class BgwError(RuntimeError):
@@ -108,6 +108,7 @@ def load(build_if_needed: bool = True) -> ctypes.CDLL:
     lib.bgw_measure_fp64_peak.argtypes = [ctypes.c_int32, ctypes.POINTER(_D), ctypes.POINTER(_D)]
     lib.bgw_release_workspace.argtypes = [ctypes.c_int32]
     lib.bgw_debug_inject_stall.argtypes = [ctypes.c_int64]
+    lib.bgw_debug_rcp_probe.argtypes = [_P, _I64, _P, _P, _P, ctypes.c_int32]
     lib.bgw_last_profile.argtypes = [ctypes.POINTER(Profile)]
     opt = ctypes.POINTER(Options)
     lib.bgw_fill_uniform.argtypes = [_P, _I64, ctypes.c_uint64, ctypes.c_uint64, _I64, _D, _D, _D, _D, opt]
@@ -152,6 +153,15 @@ def inject_stall(step: int = -1):
     kernels launched from now on let the wait of CTA-local step `step` run
     out, and their calls raise BgwError(BGW_ERR_TIMEOUT); -1 turns it off."""
     _check("bgw_debug_inject_stall", load().bgw_debug_inject_stall(int(step)))
+
+
+def rcp_probe(values, device: int = -1):
+    """(refined, seed, f32) reciprocals of `values` evaluated by the
+    library's device code (bgw_debug_rcp_probe)."""
+    x = np.ascontiguousarray(np.asarray(values, dtype=np.float64))
+    r, s, f = np.empty_like(x), np.empty_like(x), np.empty(x.shape, np.float32)
+    _check("bgw_debug_rcp_probe", load().bgw_debug_rcp_probe(_ptr(x), x.size, _ptr(r), _ptr(s), _ptr(f), device))
+    return r, s, f
 
 
 def fill_uniform(out, seed: int, stream_id: int, offset: int, lo_even: float, hi_even: float, lo_odd: float,

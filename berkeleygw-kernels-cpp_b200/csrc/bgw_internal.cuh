@@ -152,8 +152,10 @@ int finish_call(CallEnv *env);
 // relative error drops from |e| to |e|^3 (A. S. Householder, "The Numerical
 // Treatment of a Single Nonlinear Equation", 1970, ch. 4; the same series
 // is used for division by P. Markstein, "IA-64 and Elementary Functions",
-// 2000, ch. 8).  Accuracy is checked against the IEEE reciprocal in the GPU
-// tests.
+// 2000, ch. 8).  Checked against the IEEE reciprocal on the GPU
+// (bgw_debug_rcp_probe): at most 1 ulp from 1/d whenever 1/d is a normal
+// double.  Flush to zero of the approximation: a zero or subnormal d gives a
+// non-finite result, a d whose reciprocal is subnormal gives 0.
 __device__ __forceinline__ double rcp_refined(double d) {
   double y0;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y0) : "d"(d));

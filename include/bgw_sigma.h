@@ -409,6 +409,17 @@ int bgw_release_workspace(int32_t device);
  * context stays usable.  step = -1 (the default) turns the stall off. */
 int bgw_debug_inject_stall(int64_t step);
 
+/* Accuracy probe of the kernels' reciprocals (no counterpart in the
+ * reference, which divides with std::complex / double division).  For each
+ * of the n host values in[i] it evaluates on the GPU, and copies back:
+ *   refined[i]  the FP64 kernels' reciprocal (rcp.approx.ftz.f64 refined by
+ *               one third-order Newton-Householder step);
+ *   seed[i]     its starting value, rcp.approx.ftz.f64(in[i]);
+ *   f32[i]      rcp.approx.ftz.f32((float)in[i]), the reciprocal of the
+ *               mixed-precision remainder quotients. */
+int bgw_debug_rcp_probe(const double *in, int64_t n, double *refined,
+                        double *seed, float *f32, int32_t device);
+
 #ifdef __cplusplus
 }
 #endif
