@@ -28,7 +28,8 @@ from .inputs import FFInputs, GppInputs  # noqa: F401
 
 BGW_OK = 0
 STATUS = {0: "BGW_OK", -1: "BGW_ERR_INVALID_ARG", -2: "BGW_ERR_INDEX", -3: "BGW_ERR_CUDA",
-          -4: "BGW_ERR_ALLOC", -5: "BGW_ERR_NO_DEVICE", -6: "BGW_ERR_TIMEOUT", -7: "BGW_ERR_UNSUPPORTED"}
+          -4: "BGW_ERR_ALLOC", -5: "BGW_ERR_NO_DEVICE", -6: "BGW_ERR_TIMEOUT", -7: "BGW_ERR_UNSUPPORTED",
+          -8: "BGW_ERR_CHECK"}
 MEMORY = {"host": 0, "device": 1}
 PRECISION = {"fp64": 0, "mixed": 1}
 GPP_ALGO = {"bandloop": 0, "factored": 1, "auto": 2}
@@ -85,7 +86,10 @@ _D = ctypes.c_double
 
 
 def lib_path() -> Path:
-    return _build.LIB
+    """The library to load: $BGW_SIGMA_LIB (e.g. the debug build
+    lib/libbgwsigma_check.so) or lib/libbgwsigma.so."""
+    env = os.environ.get("BGW_SIGMA_LIB")
+    return Path(env) if env else _build.LIB
 
 
 def load(build_if_needed: bool = True) -> ctypes.CDLL:
@@ -93,9 +97,12 @@ def load(build_if_needed: bool = True) -> ctypes.CDLL:
     global _LIB
     if _LIB is not None:
         return _LIB
+    path = lib_path()
     if build_if_needed and os.environ.get("BGW_SIGMA_NO_BUILD") != "1":
-        _build.build()
-    path = _build.LIB
+        if path == _build.CHECK_LIB:
+            _build.build_check()
+        elif path == _build.LIB:
+            _build.build()
     if not path.exists():
         raise RuntimeError(f"libbgwsigma.so not built ({path}); run berkeleygw-kernels-cpp_b200/bgwsigma/build.py")
     lib = ctypes.CDLL(str(path))

@@ -2,6 +2,9 @@
 
 Outputs (in-tree, next to the sources, so they travel with the working tree):
   lib/libbgwsigma.so          the CUDA kernels + C ABI (include/bgw_sigma.h)
+  lib/libbgwsigma_check.so    the same with -DBGW_CHECK: kernels check their
+                              staging ranges and tile / row / packed-buffer
+                              indices and report BGW_ERR_CHECK (debug build)
   lib/libbgwsigma_refshim.so  C++11 drop-in: the reference's four kernel
                               signatures over the C ABI
   lib/bgw_refshim.o           the same shim as a PIC object, for static links
@@ -25,6 +28,7 @@ LIB_DIR = PKG_DIR / "lib"
 INCLUDE = REPO / "include"
 
 LIB = LIB_DIR / "libbgwsigma.so"
+CHECK_LIB = LIB_DIR / "libbgwsigma_check.so"
 SHIM_LIB = LIB_DIR / "libbgwsigma_refshim.so"
 SHIM_OBJ = LIB_DIR / "bgw_refshim.o"
 
@@ -59,25 +63,35 @@ def _run(cmd, verbose):
     return r
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    """Compiles libbgwsigma.so and the shim if their sources changed."""
-    LIB_DIR.mkdir(parents=True, exist_ok=True)
+def _build_cuda_lib(lib: Path, flags, obj_dir: Path, stamp_file: Path, force: bool, verbose: bool) -> None:
     srcs = [CSRC / s for s in CUDA_SOURCES] + sorted(CSRC.glob("*.cuh")) + [INCLUDE / "bgw_sigma.h"]
-    stamp_file = LIB_DIR / ".libbgwsigma.stamp"
-    stamp = _stamp(srcs, NVCC_FLAGS)
-    if force or not LIB.exists() or not stamp_file.exists() or stamp_file.read_text() != stamp:
+    stamp = _stamp(srcs, flags)
+    if force or not lib.exists() or not stamp_file.exists() or stamp_file.read_text() != stamp:
         nvcc = _nvcc()
         objs = []
-        obj_dir = LIB_DIR / "obj"
         obj_dir.mkdir(exist_ok=True)
         for s in CUDA_SOURCES:
             o = obj_dir / (Path(s).stem + ".o")
-            _run([nvcc, *NVCC_FLAGS, "-c", CSRC / s, "-o", o], verbose)
+            _run([nvcc, *flags, "-c", CSRC / s, "-o", o], verbose)
             objs.append(o)
-        tmp = LIB.with_suffix(".so.tmp")
+        tmp = lib.with_suffix(".so.tmp")
         _run([nvcc, *ARCH, "-shared", "-o", tmp, *objs], verbose)
-        os.replace(tmp, LIB)
+        os.replace(tmp, lib)
         stamp_file.write_text(stamp)
+
+
+def build_check(force: bool = False, verbose: bool = False) -> Path:
+    """Compiles the debug build libbgwsigma_check.so (-DBGW_CHECK)."""
+    LIB_DIR.mkdir(parents=True, exist_ok=True)
+    _build_cuda_lib(CHECK_LIB, NVCC_FLAGS + ["-DBGW_CHECK"], LIB_DIR / "obj_check", LIB_DIR / ".check.stamp", force,
+                    verbose)
+    return CHECK_LIB
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    """Compiles libbgwsigma.so and the shim if their sources changed."""
+    LIB_DIR.mkdir(parents=True, exist_ok=True)
+    _build_cuda_lib(LIB, NVCC_FLAGS, LIB_DIR / "obj", LIB_DIR / ".libbgwsigma.stamp", force, verbose)
 
     shim_src = SHIM / "bgw_refshim.cpp"
     shim_stamp_file = LIB_DIR / ".refshim.stamp"
@@ -95,3 +109,5 @@ def build(force: bool = False, verbose: bool = False) -> Path:
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose=True)
     print(LIB)
+    if "--check" in sys.argv:
+        print(build_check(force="--force" in sys.argv, verbose=True))

@@ -45,6 +45,17 @@ __device__ __forceinline__ void raise_status(int *status, int code, int detail) 
   if (atomicCAS(status, 0, code) == 0) status[1] = detail;
 }
 
+// Debug build (-DBGW_CHECK, lib/libbgwsigma_check.so): BGW_CHECKED(cond,
+// status, site) is `cond`; when it is false the kernel raises BGW_ERR_CHECK
+// with the site code as the status detail, and the caller skips the access
+// the check guards.  In the product build it is `true` and compiles away.
+#ifdef BGW_CHECK
+#define BGW_CHECKED(cond, status, site) \
+  ((cond) ? true : (::bgw::raise_status((status), BGW_ERR_CHECK, (site)), false))
+#else
+#define BGW_CHECKED(cond, status, site) true
+#endif
+
 // ------------------------------------------------------------- workspace --
 //
 // One grow-only set of device buffers per device, reused across calls.  A

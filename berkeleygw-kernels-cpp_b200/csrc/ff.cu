@@ -322,7 +322,8 @@ __device__ __forceinline__ void contract_tile(FFSmem &sm, const FFTile &t, const
                                               int G, const double2 *__restrict__ aqsn,
                                               const double2 *__restrict__ R, int r_f0,
                                               const double2 *__restrict__ A, int a_f0,
-                                              const double2 *__restrict__ W, double *__restrict__ partials) {
+                                              const double2 *__restrict__ W, double *__restrict__ partials,
+                                              int nb, int *status) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g8 = lane >> 2, t4 = lane & 3;
 
@@ -342,7 +343,8 @@ __device__ __forceinline__ void contract_tile(FFSmem &sm, const FFTile &t, const
 #pragma unroll
   for (int q = 0; q < kAq; ++q) {
     const int r = (q * kFFThreads + tid) / kBK;
-    a_ok[q] = r < t.row_count;
+    a_ok[q] = r < t.row_count && BGW_CHECKED(r >= t.row_count || (unsigned)rows[t.row_begin + r].band < (unsigned)nb,
+                                             status, 42);
     a_src[q] = a_ok[q] ? aqsn + (size_t)rows[t.row_begin + r].band * G + t.k_begin + kc : aqsn;
   }
   const double2 *b_src[kBq];
@@ -507,25 +509,34 @@ __global__ void __launch_bounds__(kFFThreads, 2)
     ff_contract_kernel(const FFTile *__restrict__ tiles, const FFRow *__restrict__ rows, int P, int G,
                        const double2 *__restrict__ aqsn, const double2 *__restrict__ R, int r_f0,
                        const double2 *__restrict__ A, int a_f0, const double2 *__restrict__ W,
-                       double *__restrict__ partials, int per_row) {
+                       double *__restrict__ partials, int per_row, int nb, int n_rows, int *status) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   FFSmem &sm = *reinterpret_cast<FFSmem *>(smem_raw);
-  const FFTile t = tiles[blockIdx.x];
+  FFTile t = tiles[blockIdx.x];
+  // Debug build: the tile's rows, columns and k range lie inside the plan
+  // and the arrays (a failing tile contributes zero).
+  if (!BGW_CHECKED(t.row_count >= 0 && t.row_count <= kTM && t.row_begin >= 0 && t.row_begin + t.row_count <= n_rows &&
+                       t.p_begin >= 0 && t.p_begin < P && t.k_begin >= 0 && t.k_count >= 0 &&
+                       t.k_begin + t.k_count <= G,
+                   status, 41)) {
+    t.row_count = 0;
+    t.k_count = 0;
+  }
   const int mc = min(4, (t.row_count + 7) >> 3);  // uniform per CTA
   if (per_row) {
     switch (mc) {
-      case 1: contract_tile<1, true>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
-      case 2: contract_tile<2, true>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
-      case 3: contract_tile<3, true>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
-      default: contract_tile<4, true>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
+      case 1: contract_tile<1, true>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials, nb, status); break;
+      case 2: contract_tile<2, true>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials, nb, status); break;
+      case 3: contract_tile<3, true>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials, nb, status); break;
+      default: contract_tile<4, true>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials, nb, status); break;
     }
     return;
   }
   switch (mc) {
-    case 1: contract_tile<1, false>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
-    case 2: contract_tile<2, false>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
-    case 3: contract_tile<3, false>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
-    default: contract_tile<4, false>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials); break;
+    case 1: contract_tile<1, false>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials, nb, status); break;
+    case 2: contract_tile<2, false>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials, nb, status); break;
+    case 3: contract_tile<3, false>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials, nb, status); break;
+    default: contract_tile<4, false>(sm, t, rows, P, G, aqsn, R, r_f0, A, a_f0, W, partials, nb, status); break;
   }
 }
 
@@ -665,14 +676,15 @@ int ff_fp64_per_sm(int *per_sm) {
   return BGW_OK;
 }
 
-int ff_launch_fp64_tiles(cudaStream_t stream, const FFTile *d_tiles, int ntiles, const FFRow *d_rows, int64_t P,
-                         int64_t G, const double2 *an, const double2 *R, int r_f0, const double2 *A, int a_f0,
-                         const double2 *W, double *partials, bool per_row) {
+int ff_launch_fp64_tiles(cudaStream_t stream, const FFTile *d_tiles, int ntiles, const FFRow *d_rows, int n_rows,
+                         int64_t nb, int64_t P, int64_t G, const double2 *an, const double2 *R, int r_f0,
+                         const double2 *A, int a_f0, const double2 *W, double *partials, int *status, bool per_row) {
   if (ntiles <= 0) return BGW_OK;
   int per_sm = 0;
   BGW_TRY(ff_fp64_per_sm(&per_sm));
   ff_contract_kernel<<<ntiles, kFFThreads, sizeof(FFSmem), stream>>>(d_tiles, d_rows, (int)P, (int)G, an, R, r_f0,
-                                                                      A, a_f0, W, partials, per_row ? 1 : 0);
+                                                                      A, a_f0, W, partials, per_row ? 1 : 0, (int)nb,
+                                                                      n_rows, status);
   count_launch();
   BGW_CUDA_TRY(cudaGetLastError());
   return BGW_OK;
@@ -779,7 +791,8 @@ int ff_launch(CallEnv *env, const FFPlan &plan, int64_t nb_w, int64_t nE, int64_
   if (ntiles > 0) {
     ff_contract_kernel<<<ntiles, kFFThreads, smem, stream>>>(d_tiles, d_rows, (int)P, (int)G, an, R, r_f0, A, a_f0,
                                                              (const double2 *)W, (double *)partials,
-                                                             per_row ? 1 : 0);
+                                                             per_row ? 1 : 0, (int)nb_w, (int)plan.rows.size(),
+                                                             env->d_status);
     count_launch();
     BGW_CUDA_TRY(cudaGetLastError());
   }

@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(kSliceThreads)
     ff_slice_kernel(const MixGroup *__restrict__ groups, const MixRow *__restrict__ arows,
                     const MixX *__restrict__ xs, int n_arows, int x_rows_padded, int P, int G, int KB, int NW,
                     const double2 *__restrict__ aqsn, int8_t *__restrict__ pack, double *__restrict__ sA,
-                    double *__restrict__ sB) {
+                    double *__restrict__ sB, long long pack_bytes, int *status) {
   constexpr bool kA = MODE == 0, kSub = MODE == 2;
   __shared__ double2 stage[kSliceThreads * (kSliceK + 1)];
   __shared__ double red[kSliceThreads / 32];
@@ -209,6 +209,8 @@ __global__ void __launch_bounds__(kSliceThreads)
     mi[j >> 2] |= (v[j].y < 0.0 ? 0xffu : 0u) << (8 * (j & 3));
   }
   const long long off = base + (long long)(k0 / kBK) * tile_bytes + tile_off(r_in_tile, k0 % kBK, rows);
+  // Debug build: every digit plane this thread writes lies in the packed buffer.
+  if (!BGW_CHECKED(off >= 0 && off + ((kA ? 3LL : 2LL) * kS - 1) * plane_stride + 8 <= pack_bytes, status, 51)) return;
 #pragma unroll
   for (int s = 0; s < kS; ++s) {
     const int sh = 7 * (2 - s % 3);
@@ -262,7 +264,8 @@ __global__ void __launch_bounds__(kMixThreads, 1)
                        const MixGroup *__restrict__ groups, const MixRow *__restrict__ arows,
                        const MixX *__restrict__ xs, const int8_t *__restrict__ pack, const double *__restrict__ sA,
                        const double *__restrict__ sB, int n_arows, int x_rows_padded, const double2 *__restrict__ W,
-                       int P, int KB, int PT, double *__restrict__ partials, int *status) {
+                       int P, int KB, int PT, double *__restrict__ partials, int *status, long long pack_bytes,
+                       int nb_w) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   MixSmem &sm = *reinterpret_cast<MixSmem *>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -310,6 +313,13 @@ __global__ void __launch_bounds__(kMixThreads, 1)
             const int8_t *ap = a_base + s * a_plane;
             const int8_t *xp = x_base + (L - 2 - s) * x_plane;
             for (int kb = S.kb0; kb < S.kb1; ++kb) {
+              // Debug build: the stage's digit tiles lie in the packed buffer.
+              if (!BGW_CHECKED(ap >= pack && ap + (kAPlanes - 1) * kS * a_plane + kATile <= pack + pack_bytes &&
+                                   xp >= pack && xp + (kXPlanes - 1) * kS * x_plane + kXTile <= pack + pack_bytes,
+                               status, 52)) {
+                ok = false;
+                break;
+              }
               if (step >= kStages && !wait_or_flag(&sm.empty[st], ph ^ 1u, status)) {
                 ok = false;
                 break;
@@ -410,8 +420,10 @@ __global__ void __launch_bounds__(kMixThreads, 1)
       const MixSeg S = segs[sg];
       const MixGroup Gp = groups[S.g];
       const MixX X = xs[Gp.xid];
-      const long long prow = (long long)Gp.prow0 + (long long)S.rt * kM + row;
-      const MixRow ar = arows[prow];
+      long long prow = (long long)Gp.prow0 + (long long)S.rt * kM + row;
+      if (!BGW_CHECKED(prow >= 0 && prow < n_arows, status, 53)) prow = 0;
+      MixRow ar = arows[prow];
+      if (!BGW_CHECKED((unsigned)ar.band < (unsigned)nb_w, status, 54)) ar.band = 0;
       const double2 *wrow = W + (size_t)ar.band * P;
       const double *sb = sB + X.sb_off + (size_t)S.w * x_rows_padded;
       const int c0 = half * (kN / 2);  // first tile column of this warp
@@ -735,7 +747,8 @@ int ff_launch_mixed(CallEnv *env, const FFPlan &plan, int64_t nb, int64_t nb_w, 
     double *d_sa = (double *)(sb + o_sa), *d_sb = (double *)(sb + o_sb);
     const int na = (int)arows.size();
     ff_slice_kernel<0><<<(unsigned)((size_t)na * NW), kSliceThreads, 0, stream>>>(
-        d_mg, d_ar, d_xs, na, x_rows_padded, (int)P, (int)G, KB, NW, an, (int8_t *)pack, d_sa, d_sb);
+        d_mg, d_ar, d_xs, na, x_rows_padded, (int)P, (int)G, KB, NW, an, (int8_t *)pack, d_sa, d_sb, off,
+        env->d_status);
     count_launch();
     BGW_CUDA_TRY(cudaGetLastError());
     // X slices: xs holds the plain ones first, then the differences.
@@ -748,10 +761,12 @@ int ff_launch_mixed(CallEnv *env, const FFPlan &plan, int64_t nb, int64_t nb_w, 
       const MixX *d_x = d_xs + x0;
       if (sub)
         ff_slice_kernel<2><<<grid, kSliceThreads, 0, stream>>>(d_mg, d_ar, d_x, na, x_rows_padded, (int)P, (int)G,
-                                                              KB, NW, an, (int8_t *)pack, d_sa, d_sb);
+                                                              KB, NW, an, (int8_t *)pack, d_sa, d_sb, off,
+                                                              env->d_status);
       else
         ff_slice_kernel<1><<<grid, kSliceThreads, 0, stream>>>(d_mg, d_ar, d_x, na, x_rows_padded, (int)P, (int)G,
-                                                              KB, NW, an, (int8_t *)pack, d_sa, d_sb);
+                                                              KB, NW, an, (int8_t *)pack, d_sa, d_sb, off,
+                                                              env->d_status);
       count_launch();
       BGW_CUDA_TRY(cudaGetLastError());
     }
@@ -760,12 +775,13 @@ int ff_launch_mixed(CallEnv *env, const FFPlan &plan, int64_t nb, int64_t nb_w, 
     BGW_CUDA_TRY(cudaFuncSetAttribute(gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     gemm<<<nctas, kMixThreads, smem, stream>>>(
         (const MixSeg *)(sb + o_seg), (const int *)(sb + o_cta), d_mg, d_ar, d_xs, (const int8_t *)pack, d_sa, d_sb,
-        na, x_rows_padded, W, (int)P, KB, PT, part + 2 * seg_part0, env->d_status);
+        na, x_rows_padded, W, (int)P, KB, PT, part + 2 * seg_part0, env->d_status, off, (int)nb_w);
     count_launch();
     BGW_CUDA_TRY(cudaGetLastError());
   }
-  BGW_TRY(ff_launch_fp64_tiles(stream, (const FFTile *)(sb + o_ft), nft, (const FFRow *)(sb + o_rows), P, G, an, R,
-                               r_f0, A, a_f0, W, part, per_row));
+  BGW_TRY(ff_launch_fp64_tiles(stream, (const FFTile *)(sb + o_ft), nft, (const FFRow *)(sb + o_rows),
+                               (int)plan.rows.size(), nb_w, P, G, an, R, r_f0, A, a_f0, W, part, env->d_status,
+                               per_row));
   BGW_TRY(prof_mark(env, 2));
   if (per_row) {
     FFTermTables tt;

@@ -87,9 +87,12 @@ void ff_fp64_tiles(const std::vector<FFGroup> &groups, int64_t P, int64_t G, int
 // Launches the DMMA contraction over device tiles: one complex partial per
 // tile at `partials`, or with `per_row` one per tile row (ntiles x
 // ff_fp64_tile_rows(), zero for padding rows).
-int ff_launch_fp64_tiles(cudaStream_t stream, const FFTile *d_tiles, int ntiles, const FFRow *d_rows, int64_t P,
-                         int64_t G, const double2 *an, const double2 *R, int r_f0, const double2 *A, int a_f0,
-                         const double2 *W, double *partials, bool per_row = false);
+// n_rows: rows of the plan; nb: rows of aqsn and W (both bound the debug
+// build's checks, which report through `status`).
+int ff_launch_fp64_tiles(cudaStream_t stream, const FFTile *d_tiles, int ntiles, const FFRow *d_rows, int n_rows,
+                         int64_t nb, int64_t P, int64_t G, const double2 *an, const double2 *R, int r_f0,
+                         const double2 *A, int a_f0, const double2 *W, double *partials, int *status,
+                         bool per_row = false);
 int ff_fp64_tile_rows();
 // Plan row of every per-row partial of `tiles` (-1 for padding rows),
 // appended to `row_of`.

@@ -185,6 +185,13 @@ __global__ void __launch_bounds__(BandCfg<MIXED>::kNT, 1)
     const int buf = (int)(j & 1);
     uint32_t bytes = 2u * nvalid * 16u + nbv * 16u + nbv * 32u;
     uint64_t *bar = reinterpret_cast<uint64_t *>(&sm.bar[buf]);
+    // Debug build: the step's source ranges and the staging capacity.
+    if (!BGW_CHECKED(item < items && nvalid > 0 && nvalid <= kCH && g0 + nvalid <= G && nbv > 0 && nbv <= BCH &&
+                         b0 + nbv <= nb,
+                     status, 11)) {
+      mbar_expect_tx(bar, 0);  // completes the phase without copies
+      return;
+    }
     mbar_expect_tx(bar, bytes);
     bulk_g2s(sm.wt[buf], wtilde + p * G + g0, nvalid * 16u, bar);
     bulk_g2s(sm.ie[buf], ieps + p * G + g0, nvalid * 16u, bar);
@@ -215,9 +222,10 @@ __global__ void __launch_bounds__(BandCfg<MIXED>::kNT, 1)
     const long long item = blockIdx.x + (j / nbc) * (long long)gridDim.x;
     const int c = (int)(j % nbc);
     const int g0 = (int)(item % nchunks_g) * kCH;
-    const int nvalid = min(kCH, G - g0);
+    int nvalid = min(kCH, G - g0);
     const int b0 = c * BCH;
-    const int nbv = min(BCH, nb - b0);
+    int nbv = min(BCH, nb - b0);
+    if (!BGW_CHECKED(nvalid <= kCH && nbv <= BCH, status, 12)) nvalid = nbv = 0;
 
     if constexpr (MIXED) {
       const RemStep rs = rem_stage<kThreads, K>(sm.wx[buf], sm.st[buf], nbv, sm.rows, sm.red, sm.xr_lo, sm.xr_hi);

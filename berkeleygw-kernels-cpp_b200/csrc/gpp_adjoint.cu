@@ -111,6 +111,10 @@ __global__ void __launch_bounds__(kAdjThreads, 2)
     const int nvalid = min(kAdjChunk, G - g0);
     const int buf = (int)(j & 1);
     uint64_t *bar = reinterpret_cast<uint64_t *>(&sm.bar[buf]);
+    if (!BGW_CHECKED(p < P && nvalid > 0 && nvalid <= kAdjChunk && g0 + nvalid <= G, status, 21)) {
+      mbar_expect_tx(bar, 0);
+      return;
+    }
     mbar_expect_tx(bar, 2u * (uint32_t)nvalid * 16u);
     bulk_g2s(sm.wt[buf], wtilde + p * G + g0, (uint32_t)nvalid * 16u, bar);
     bulk_g2s(sm.ie[buf], ieps + p * G + g0, (uint32_t)nvalid * 16u, bar);
@@ -299,6 +303,10 @@ __global__ void __launch_bounds__(kAdjThreads, 1)
     const int nbv = min(kAbBCH, nb - b0);
     const int buf = (int)(j & 1);
     uint64_t *bar = reinterpret_cast<uint64_t *>(&sm.bar[buf]);
+    if (!BGW_CHECKED(item < items && nbv > 0 && nbv <= kAbBCH && b0 + nbv <= nb, status, 22)) {
+      mbar_expect_tx(bar, 0);
+      return;
+    }
     mbar_expect_tx(bar, (uint32_t)nbv * 48u);
     bulk_g2s(sm.C[buf], Ctab + p * nb + b0, (uint32_t)nbv * 16u, bar);
     bulk_g2s(sm.wx[buf], wx4 + b0, (uint32_t)nbv * 32u, bar);
@@ -325,7 +333,8 @@ __global__ void __launch_bounds__(kAdjThreads, 1)
     const long long p = item / nchunk_e;
     const int g0 = (int)(item % nchunk_e) * kAbChunk;
     const int c = (int)(j % nbc);
-    const int nbv = min(kAbBCH, nb - c * kAbBCH);
+    int nbv = min(kAbBCH, nb - c * kAbBCH);
+    if (!BGW_CHECKED(nbv <= kAbBCH, status, 23)) nbv = 0;
     if (c == 0) {
 #pragma unroll
       for (int k = 0; k < kAbE; ++k) {

@@ -187,6 +187,12 @@ __global__ void __launch_bounds__(kBThreads, KE == 8 ? 1 : 2)
     const int b0 = s.c * BCH;
     const int nbv = max(0, min(BCH, I.nb - b0));
     uint64_t *bar = reinterpret_cast<uint64_t *>(&sm.bar[buf]);
+    if (!BGW_CHECKED(s.i >= 0 && s.i < n && local >= 0 && p < I.P && nvalid > 0 && nvalid <= kCH &&
+                         g0 + nvalid <= I.G && nbv <= BCH,
+                     status, 31)) {
+      mbar_expect_tx(bar, 0);
+      return;
+    }
     mbar_expect_tx(bar, 2u * nvalid * 16u + nbv * 48u);
     bulk_g2s(sm.wt[buf], I.wt + (size_t)p * I.G + g0, nvalid * 16u, bar);
     bulk_g2s(sm.ie[buf], I.ie + (size_t)p * I.G + g0, nvalid * 16u, bar);
@@ -221,8 +227,9 @@ __global__ void __launch_bounds__(kBThreads, KE == 8 ? 1 : 2)
     const BatchInst &I = inst[cur.i];
     const long long local = cur.j - I.item0;
     const int g0 = (int)(local % I.nchunk) * kCH;
-    const int nvalid = min(kCH, I.G - g0);
-    const int nbv = max(0, min(BCH, I.nb - cur.c * BCH));
+    int nvalid = min(kCH, I.G - g0);
+    int nbv = max(0, min(BCH, I.nb - cur.c * BCH));
+    if (!BGW_CHECKED(nvalid <= kCH && nbv <= BCH, status, 32)) nvalid = nbv = 0;
     // MIXED: elements near the chunk's frequencies are summed in FP64.
     if constexpr (MIXED) {
       const RemStep rs = rem_stage<kBThreads, K>(sm.wx[buf], sm.st[buf], nbv, sm.rows, sm.red, sm.xr_lo, sm.xr_hi);

@@ -294,6 +294,7 @@ const char *bgw_status_string(int status) {
     case BGW_ERR_NO_DEVICE: return "no usable CUDA device";
     case BGW_ERR_TIMEOUT: return "device-side wait timed out";
     case BGW_ERR_UNSUPPORTED: return "unsupported option combination";
+    case BGW_ERR_CHECK: return "debug-build bounds check failed";
     default: return "unknown status";
   }
 }

@@ -45,7 +45,10 @@ typedef enum bgw_status {
   BGW_ERR_ALLOC = -4,       /* device or pinned allocation failed        */
   BGW_ERR_NO_DEVICE = -5,   /* no usable CUDA device                     */
   BGW_ERR_TIMEOUT = -6,     /* a bounded device-side wait ran out        */
-  BGW_ERR_UNSUPPORTED = -7  /* option combination not implemented        */
+  BGW_ERR_UNSUPPORTED = -7, /* option combination not implemented        */
+  BGW_ERR_CHECK = -8        /* a bounds check of the debug build failed
+                               (libbgwsigma_check.so, built with
+                               -DBGW_CHECK; never raised otherwise)      */
 } bgw_status;
 
 enum { BGW_MEMORY_HOST = 0, BGW_MEMORY_DEVICE = 1 };
