@@ -879,7 +879,9 @@ int gpp_sx_enqueue(CallEnv *env, int64_t nvband, int64_t P, int64_t G, const int
 // sums S[ngpown] and the per-CTA partials -- lives in one static device
 // array compiled into the library.  The host never dereferences the array's
 // name: on a device's first call the address is fetched with
-// cudaGetSymbolAddress (with that device current) and cached.
+// cudaGetSymbolAddress (with that device current) and cached for the life of
+// the process (it belongs to the primary context; a cudaDeviceReset would
+// invalidate it, which the header documents).
 namespace {
 
 constexpr int64_t kNoAllocMaxNgpown = BGW_NOALLOC_MAX_NGPOWN;

@@ -271,8 +271,11 @@ int bgw_gpp_sigma(int64_t number_bands, int64_t nvband, int64_t ngpown, int64_t 
  *   - The call enqueues on `stream` (cudaStream_t, NULL = default stream)
  *     and synchronises it to read the status.
  *   - A device's first call fetches the array's device address
- *     (cudaGetSymbolAddress) for that device; make that first call before
- *     any stream capture.
+ *     (cudaGetSymbolAddress) for that device and keeps it for the life of
+ *     the process; make that first call before any stream capture.  The
+ *     kept address belongs to the device's primary context: do not use
+ *     this entry point on a device after cudaDeviceReset has destroyed
+ *     that context.
  *   - All calls on a device share the array, which keeps the last call's
  *     contents; the call clears the status words itself.  Calls that overlap
  *     on the GPU (other threads or streams) race on the scratch: serialise

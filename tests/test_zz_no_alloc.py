@@ -42,6 +42,25 @@ def test_noalloc_matches_regular_entry_point_twice_in_a_row(bgw, cuda):
         assert rel_err(got, want) < FP64_RTOL
 
 
+def test_noalloc_warm_calls_allocate_nothing(bgw, cuda):
+    """After one warm-up call (which may load the module and fetch the
+    scratch address), further calls leave the device's free memory and
+    torch's allocator untouched: nothing is allocated or freed."""
+    import torch
+    d = bgw.to_device(I.gpp_seeded(48, 2, 4096, 16, seed=12), cuda)
+    out = torch.zeros(3, dtype=torch.complex128, device=cuda)
+    assert _noalloc(bgw, d, out) == 0
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    alloc0 = torch.cuda.memory_allocated()
+    for _ in range(5):
+        assert _noalloc(bgw, d, out) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert torch.cuda.memory_allocated() == alloc0
+
+
 def test_noalloc_on_a_stream_and_bad_index(bgw, cuda):
     import torch
     g = I.gpp_seeded(16, 2, 1024, 16, seed=8)
