@@ -308,9 +308,11 @@ struct FFSmem {
 };
 
 // One CTA per tile.  4 warps; warp w owns G' columns [16w, 16w + 16) of the
-// tile and all 32 rows: 4 x 2 m8n8 blocks, each a complex accumulator kept
-// as separate real and imaginary DMMA accumulators (4 real MMAs per complex
-// k4 step: Re += Ar Br + Ai (-Bi), Im += Ar Bi + Ai Br).
+// tile and all 32 rows: 4 x 2 m8n8 blocks, each complex block kept as three
+// real DMMA accumulators of Gauss's three-multiplication product (3 real
+// MMAs per complex k4 step instead of 4):
+//   K1 += (Ar + Ai) Br,  K2 += Ar (Bi - Br),  K3 += Ai (Br + Bi),
+//   Re = K1 - K3 = sum Ar Br - Ai Bi,  Im = K1 + K2 = sum Ar Bi + Ai Br.
 // Operands stream global -> shared through a kStages-deep cp.async pipeline
 // (rows gathered by band index, out-of-range rows / k zero-filled); for the
 // COR sum the I_epsR and I_epsA rows are staged separately and R - A is
@@ -379,11 +381,13 @@ __device__ __forceinline__ void contract_tile(FFSmem &sm, const FFTile &t, const
     }
   };
 
-  double cr[4][2][2], ci[4][2][2];
+  double k1[4][2][2], k2[4][2][2], k3[4][2][2];
 #pragma unroll
   for (int m = 0; m < 4; ++m)
 #pragma unroll
-    for (int n = 0; n < 2; ++n) cr[m][n][0] = cr[m][n][1] = ci[m][n][0] = ci[m][n][1] = 0.0;
+    for (int n = 0; n < 2; ++n)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) k1[m][n][j] = k2[m][n][j] = k3[m][n][j] = 0.0;
 
 #pragma unroll
   for (int s = 0; s < kStages - 1; ++s) {
@@ -402,12 +406,13 @@ __device__ __forceinline__ void contract_tile(FFSmem &sm, const FFTile &t, const
     const double2 *sb2 = s.b2 + (warp * 16) * kLds;
 #pragma unroll
     for (int ks = 0; ks < kBK / 4; ++ks) {
-      double ar[4], ai[4], br[2], bi[2], bn[2];
+      double ar[4], ai[4], as[4], br[2], bd[2], bs[2];
 #pragma unroll
       for (int m = 0; m < MC; ++m) {
         const double2 v = sa[(m * 8 + g8) * kLds + ks * 4 + t4];
         ar[m] = v.x;
         ai[m] = v.y;
+        as[m] = v.x + v.y;
       }
 #pragma unroll
       for (int n = 0; n < 2; ++n) {
@@ -418,25 +423,23 @@ __device__ __forceinline__ void contract_tile(FFSmem &sm, const FFTile &t, const
           v.y -= y.y;
         }
         br[n] = v.x;
-        bi[n] = v.y;
-        bn[n] = -v.y;
+        bd[n] = v.y - v.x;
+        bs[n] = v.x + v.y;
       }
-      // Two sweeps over the 4 MC independent accumulators, so that the two
-      // MMAs into one accumulator are 4 MC instructions apart.
+      // Three sweeps, one per Gauss product: each accumulator receives one
+      // MMA per k4 step, 2 MC MMAs after the previous one into it.
 #pragma unroll
       for (int m = 0; m < MC; ++m)
 #pragma unroll
-        for (int n = 0; n < 2; ++n) {
-          dmma_f64(cr[m][n][0], cr[m][n][1], ar[m], br[n]);
-          dmma_f64(ci[m][n][0], ci[m][n][1], ar[m], bi[n]);
-        }
+        for (int n = 0; n < 2; ++n) dmma_f64(k1[m][n][0], k1[m][n][1], as[m], br[n]);
 #pragma unroll
       for (int m = 0; m < MC; ++m)
 #pragma unroll
-        for (int n = 0; n < 2; ++n) {
-          dmma_f64(cr[m][n][0], cr[m][n][1], ai[m], bn[n]);
-          dmma_f64(ci[m][n][0], ci[m][n][1], ai[m], br[n]);
-        }
+        for (int n = 0; n < 2; ++n) dmma_f64(k2[m][n][0], k2[m][n][1], ar[m], bd[n]);
+#pragma unroll
+      for (int m = 0; m < MC; ++m)
+#pragma unroll
+        for (int n = 0; n < 2; ++n) dmma_f64(k3[m][n][0], k3[m][n][1], ai[m], bs[n]);
     }
   }
   cp_async_wait<0>();
@@ -460,7 +463,7 @@ __device__ __forceinline__ void contract_tile(FFSmem &sm, const FFTile &t, const
         const int p = t.p_begin + warp * 16 + n * 8 + 2 * t4 + j;
         if (p >= P) continue;
         const double2 w = W[(size_t)row.band * P + p];
-        const double xr = cr[m][n][j], xi = ci[m][n][j];
+        const double xr = k1[m][n][j] - k3[m][n][j], xi = k1[m][n][j] + k2[m][n][j];
         if (ROWS) {
           rv[m][0] = fma(row.coef, xr * w.x - xi * w.y, rv[m][0]);
           rv[m][1] = fma(row.coef, xr * w.y + xi * w.x, rv[m][1]);
@@ -505,7 +508,7 @@ __device__ __forceinline__ void contract_tile(FFSmem &sm, const FFTile &t, const
   }
 }
 
-__global__ void __launch_bounds__(kFFThreads, 2)
+__global__ void __launch_bounds__(kFFThreads, 3)
     ff_contract_kernel(const FFTile *__restrict__ tiles, const FFRow *__restrict__ rows, int P, int G,
                        const double2 *__restrict__ aqsn, const double2 *__restrict__ R, int r_f0,
                        const double2 *__restrict__ A, int a_f0, const double2 *__restrict__ W,
