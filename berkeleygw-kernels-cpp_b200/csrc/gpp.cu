@@ -111,14 +111,16 @@ __global__ void gpp_wx_kernel(int nb, const double *__restrict__ wx, long long s
 // a frequency x:
 //   dr  = x - wr,  |wdiff|^2 = dr^2 + wi^2,
 //   conj(wdiff) * I_eps = (dr*Ir + a) + i (dr*Ii + b).
-// Elements per thread: 8 (a longer run per band amortises the per-band
-// combination with sch_store1: FP64 53.6 ms at 8 vs 58.0 ms at 4 and 55.8 ms
-// at 6 on the 512-band benchmark).  256 threads per CTA, one CTA per SM
-// (FP64: 210 registers, 153 KB of staging; mixed: 194 KB of staging with
-// the per-band remainder rows).
+// Elements per thread: FP64 8 (a longer run per band amortises the per-band
+// combination with sch_store1: 53.6 ms at 8 vs 58.0 ms at 4 and 55.8 ms at 6
+// on the 512-band benchmark); mixed 12 (more independent work per thread and
+// the per-band multiply over 36 terms; 128-band chunks keep the staging in
+// shared memory).  256 threads per CTA, one CTA per SM (FP64: 210
+// registers, 153 KB of staging; mixed: ~215 registers, 223 KB of staging
+// with the per-band remainder rows).
 template <bool MIXED>
 struct BandCfg {
-  static constexpr int kE = 8;
+  static constexpr int kE = MIXED ? 12 : 8;
   static constexpr int kNT = kThreads;
   static constexpr int kCH = kNT * kE;
 };
@@ -405,15 +407,18 @@ int launch_bandloop(cudaStream_t stream, int max_grid, int nb, int G, const doub
   return BGW_OK;
 }
 
+// Band chunk of the mixed form (the FP64 form stages 256 bands per step).
+constexpr int kMixBCH = 128;
+
 // The instantiation a call's options select: FP64 (guarded or not) or mixed
 // with K = opt.mixed_order hoisted terms.
 int bandloop_per_sm_for(const bgw_options &o, int *per_sm) {
   if (o.precision == BGW_PRECISION_MIXED) {
     switch (o.mixed_order) {
-      case 0: return bandloop_per_sm<256, true, false, 0>(per_sm);
-      case 1: return bandloop_per_sm<256, true, false, 1>(per_sm);
-      case 2: return bandloop_per_sm<256, true, false, 2>(per_sm);
-      default: return bandloop_per_sm<256, true, false, 3>(per_sm);
+      case 0: return bandloop_per_sm<kMixBCH, true, false, 0>(per_sm);
+      case 1: return bandloop_per_sm<kMixBCH, true, false, 1>(per_sm);
+      case 2: return bandloop_per_sm<kMixBCH, true, false, 2>(per_sm);
+      default: return bandloop_per_sm<kMixBCH, true, false, 3>(per_sm);
     }
   }
   if (o.pole_guard > 0.0) return bandloop_per_sm<256, false, true>(per_sm);
@@ -427,16 +432,16 @@ int launch_bandloop_for(const bgw_options &o, cudaStream_t stream, int max_grid,
   if (o.precision == BGW_PRECISION_MIXED) {
     switch (o.mixed_order) {
       case 0:
-        return launch_bandloop<256, true, false, 0>(stream, max_grid, nb, G, wt, ie, st, wx4, P, partials, grid_out,
+        return launch_bandloop<kMixBCH, true, false, 0>(stream, max_grid, nb, G, wt, ie, st, wx4, P, partials, grid_out,
                                                     status, guard2);
       case 1:
-        return launch_bandloop<256, true, false, 1>(stream, max_grid, nb, G, wt, ie, st, wx4, P, partials, grid_out,
+        return launch_bandloop<kMixBCH, true, false, 1>(stream, max_grid, nb, G, wt, ie, st, wx4, P, partials, grid_out,
                                                     status, guard2);
       case 2:
-        return launch_bandloop<256, true, false, 2>(stream, max_grid, nb, G, wt, ie, st, wx4, P, partials, grid_out,
+        return launch_bandloop<kMixBCH, true, false, 2>(stream, max_grid, nb, G, wt, ie, st, wx4, P, partials, grid_out,
                                                     status, guard2);
       default:
-        return launch_bandloop<256, true, false, 3>(stream, max_grid, nb, G, wt, ie, st, wx4, P, partials, grid_out,
+        return launch_bandloop<kMixBCH, true, false, 3>(stream, max_grid, nb, G, wt, ie, st, wx4, P, partials, grid_out,
                                                     status, guard2);
     }
   }

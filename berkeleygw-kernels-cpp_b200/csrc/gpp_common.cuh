@@ -145,10 +145,12 @@ __device__ __forceinline__ void band_sweep(const Elem<double> (&e)[kE], const do
 // pole_guard cut could reach.
 //
 // The remainder's denominators lie in [(1 - tau)^2, (1 + tau)^2], so one
-// reciprocal serves the three frequencies of an element: with d0, d1, d2,
-// R = 1 / (d0 d1 d2), 1/d0 = d1 d2 R, 1/d1 = d0 d2 R, 1/d2 = d0 d1 R (no
-// overflow or underflow can occur in that range).  Two elements are
-// processed per packed f32x2 instruction.
+// reciprocal serves two frequencies of an element: R = 1 / (d0 d1),
+// 1/d0 = d1 R, 1/d1 = d0 R (no overflow or underflow can occur in that
+// range); the third has its own.  Two elements are processed per packed
+// f32x2 instruction.  (An f32x2 FMA occupies both halves of the FMA pipe, so
+// packing saves issue slots, not pipe time; the measured limits are the FMA
+// pipe and dependent-instruction latency, hence two accumulator sets.)
 constexpr double kRemTau = 0.125;
 
 // Per band of a step: (2 delta, 2 delta), (delta^2, delta^2), (delta, delta)
@@ -331,7 +333,7 @@ __device__ __forceinline__ uint32_t rem_elems(RemElems<kE> &e, const double2 *__
 }
 
 // The remainder's band sweep: for each band, T_iw = sum over this thread's
-// elements of (X + delta Y) / |1 + t|^2 (packed FP32, one reciprocal per
+// elements of (X + delta Y) / |1 + t|^2 (packed FP32, two reciprocals per
 // element for the three frequencies), times the band multiplier m; the
 // products are summed in FP32 over groups of kRemGroup bands and each group
 // sum is added to the FP64 accumulators with TwoSum.
@@ -355,34 +357,41 @@ __device__ __forceinline__ void rem_sweep(const RemElems<kE> &e, const RemRow *_
     for (int iw = 0; iw < 3; ++iw) gr[iw] = gi[iw] = make_float2(0.f, 0.f);
     for (int b = b0; b < b1; ++b) {
       const RemRow &R = rows[b];
-      float2 tr[3], ti[3];
+      // Two accumulator sets (even / odd element pairs) shorten the chains of
+      // dependent FMAs.
+      float2 tr[2][3], ti[2][3];
 #pragma unroll
-      for (int iw = 0; iw < 3; ++iw) tr[iw] = ti[iw] = make_float2(0.f, 0.f);
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int iw = 0; iw < 3; ++iw) tr[h][iw] = ti[h][iw] = make_float2(0.f, 0.f);
 #pragma unroll
       for (int q = 0; q < kE / 2; ++q) {
         float2 den[3];
 #pragma unroll
         for (int iw = 0; iw < 3; ++iw) den[iw] = __ffma2_rn(R.dd[iw], e.uu[q], __ffma2_rn(R.d2x[iw], e.ur[q], one));
-        const float2 d12 = __fmul2_rn(den[1], den[2]);
-        const float2 P = __fmul2_rn(den[0], d12);
+        const float2 P = __fmul2_rn(den[0], den[1]);
         const float2 Ri = make_float2(rcp_f32(P.x), rcp_f32(P.y));
-        const float2 t0 = __fmul2_rn(den[0], Ri);
         float2 rc[3];
-        rc[0] = __fmul2_rn(d12, Ri);
-        rc[1] = __fmul2_rn(den[2], t0);
-        rc[2] = __fmul2_rn(den[1], t0);
+        rc[0] = __fmul2_rn(den[1], Ri);
+        rc[1] = __fmul2_rn(den[0], Ri);
+        rc[2] = make_float2(rcp_f32(den[2].x), rcp_f32(den[2].y));
 #pragma unroll
         for (int iw = 0; iw < 3; ++iw) {
           const float2 nr = __ffma2_rn(R.d[iw], e.Yr[q], e.Xr[q]);
           const float2 ni = __ffma2_rn(R.d[iw], e.Yi[q], e.Xi[q]);
-          tr[iw] = __ffma2_rn(nr, rc[iw], tr[iw]);
-          ti[iw] = __ffma2_rn(ni, rc[iw], ti[iw]);
+          tr[q & 1][iw] = __ffma2_rn(nr, rc[iw], tr[q & 1][iw]);
+          ti[q & 1][iw] = __ffma2_rn(ni, rc[iw], ti[q & 1][iw]);
         }
       }
 #pragma unroll
       for (int iw = 0; iw < 3; ++iw) {
-        gr[iw] = __ffma2_rn(R.mr[iw], tr[iw], __ffma2_rn(R.nmi[iw], ti[iw], gr[iw]));
-        gi[iw] = __ffma2_rn(R.mr[iw], ti[iw], __ffma2_rn(R.mi[iw], tr[iw], gi[iw]));
+        tr[0][iw] = __fadd2_rn(tr[0][iw], tr[1][iw]);
+        ti[0][iw] = __fadd2_rn(ti[0][iw], ti[1][iw]);
+      }
+#pragma unroll
+      for (int iw = 0; iw < 3; ++iw) {
+        gr[iw] = __ffma2_rn(R.mr[iw], tr[0][iw], __ffma2_rn(R.nmi[iw], ti[0][iw], gr[iw]));
+        gi[iw] = __ffma2_rn(R.mr[iw], ti[0][iw], __ffma2_rn(R.mi[iw], tr[0][iw], gi[iw]));
       }
     }
 #pragma unroll

@@ -24,7 +24,7 @@ from conftest import FP64_RTOL, rel_err
 pytestmark = pytest.mark.gpu
 
 # 512 bands = 2 band chunks per item; ncouls 4096 = 2 G chunks per row
-# (3 for the mixed form); 300 rows: every CTA of the persistent grid has at
+# (also for the mixed form); 300 rows: every CTA of the persistent grid has at
 # least 4 items, so every CTA reaches step 3.
 DIMS = dict(number_bands=512, nvband=2, ncouls=4096, nodes_per_group=14)
 
