@@ -113,22 +113,25 @@ __global__ void gpp_wx_kernel(int nb, const double *__restrict__ wx, long long s
 //   conj(wdiff) * I_eps = (dr*Ir + a) + i (dr*Ii + b).
 // Elements per thread: FP64 8 (a longer run per band amortises the per-band
 // combination with sch_store1: 53.6 ms at 8 vs 58.0 ms at 4 and 55.8 ms at 6
-// on the 512-band benchmark); mixed 12 (more independent work per thread and
-// the per-band multiply over 36 terms; 128-band chunks keep the staging in
-// shared memory).  256 threads per CTA, one CTA per SM (FP64: 210
-// registers, 153 KB of staging; mixed: ~215 registers, 223 KB of staging
-// with the per-band remainder rows).
+// on the 512-band benchmark); mixed 16 (more independent work per thread,
+// the per-band multiply over 48 terms).  256 threads per CTA, one CTA per
+// SM.  FP64: the step's wtilde / I_eps chunk is staged in shared memory with
+// the band rows (210 registers, 153 KB).  Mixed: the elements are read once
+// per step from global memory (the item's chunk stays in L2 across its band
+// chunks), which leaves the shared memory to 512-band steps: the per-step
+// set-up (band moments, FP64 hoisted terms) is then amortised over every
+// band of a 512-band problem (~123 KB with the remainder rows).
 template <bool MIXED>
 struct BandCfg {
-  static constexpr int kE = MIXED ? 12 : 8;
+  static constexpr int kE = MIXED ? 16 : 8;
   static constexpr int kNT = kThreads;
   static constexpr int kCH = kNT * kE;
 };
 
 template <int BCH, bool MIXED>
 struct BandSmem {
-  double2 wt[2][BandCfg<MIXED>::kCH];
-  double2 ie[2][BandCfg<MIXED>::kCH];
+  double2 wt[2][MIXED ? 1 : BandCfg<MIXED>::kCH];  // FP64 only: staged elements
+  double2 ie[2][MIXED ? 1 : BandCfg<MIXED>::kCH];
   double2 st[2][BCH];
   double4 wx[2][BCH];
   unsigned long long bar[3];  // [2]: never arrived on (stall injection)
@@ -185,7 +188,7 @@ __global__ void __launch_bounds__(BandCfg<MIXED>::kNT, 1)
     const int b0 = c * BCH;
     const int nbv = min(BCH, nb - b0);
     const int buf = (int)(j & 1);
-    uint32_t bytes = 2u * nvalid * 16u + nbv * 16u + nbv * 32u;
+    uint32_t bytes = (MIXED ? 0u : 2u * nvalid * 16u) + nbv * 16u + nbv * 32u;
     uint64_t *bar = reinterpret_cast<uint64_t *>(&sm.bar[buf]);
     // Debug build: the step's source ranges and the staging capacity.
     if (!BGW_CHECKED(item < items && nvalid > 0 && nvalid <= kCH && g0 + nvalid <= G && nbv > 0 && nbv <= BCH &&
@@ -195,8 +198,10 @@ __global__ void __launch_bounds__(BandCfg<MIXED>::kNT, 1)
       return;
     }
     mbar_expect_tx(bar, bytes);
-    bulk_g2s(sm.wt[buf], wtilde + p * G + g0, nvalid * 16u, bar);
-    bulk_g2s(sm.ie[buf], ieps + p * G + g0, nvalid * 16u, bar);
+    if constexpr (!MIXED) {
+      bulk_g2s(sm.wt[buf], wtilde + p * G + g0, nvalid * 16u, bar);
+      bulk_g2s(sm.ie[buf], ieps + p * G + g0, nvalid * 16u, bar);
+    }
     bulk_g2s(sm.st[buf], st + p * nb + b0, nbv * 16u, bar);
     bulk_g2s(sm.wx[buf], wx4 + b0, nbv * 32u, bar);
   };
@@ -230,13 +235,14 @@ __global__ void __launch_bounds__(BandCfg<MIXED>::kNT, 1)
     if (!BGW_CHECKED(nvalid <= kCH && nbv <= BCH, status, 12)) nvalid = nbv = 0;
 
     if constexpr (MIXED) {
+      const long long p = item / nchunks_g;
+      const double2 *wt_g = wtilde + p * G + g0, *ie_g = ieps + p * G + g0;
       const RemStep rs = rem_stage<kThreads, K>(sm.wx[buf], sm.st[buf], nbv, sm.rows, sm.red, sm.xr_lo, sm.xr_hi);
       RemElems<kE> e;
-      const uint32_t near = rem_elems<kE, K>(e, sm.wt[buf], sm.ie[buf], nvalid, kThreads, tid, rs, guard2, acc_r,
-                                             acc_i);
+      const uint32_t near = rem_elems<kE, K>(e, wt_g, ie_g, nvalid, kThreads, tid, rs, guard2, acc_r, acc_i);
       rem_sweep<kE>(e, sm.rows, nbv, acc_r, acc_i, lo_r, lo_i);
-      if (near) near_sweep(near, sm.wt[buf], sm.ie[buf], kThreads, tid, sm.wx[buf], sm.st[buf], nbv, guard2, acc_r,
-                           acc_i, lo_r, lo_i);
+      if (near) near_sweep(near, wt_g, ie_g, kThreads, tid, sm.wx[buf], sm.st[buf], nbv, guard2, acc_r, acc_i, lo_r,
+                           lo_i);
     } else {
       Elem<double> e[kE];
       load_elems<double, kE>(e, sm.wt[buf], sm.ie[buf], nvalid, kThreads, tid);
@@ -408,7 +414,7 @@ int launch_bandloop(cudaStream_t stream, int max_grid, int nb, int G, const doub
 }
 
 // Band chunk of the mixed form (the FP64 form stages 256 bands per step).
-constexpr int kMixBCH = 128;
+constexpr int kMixBCH = 512;
 
 // The instantiation a call's options select: FP64 (guarded or not) or mixed
 // with K = opt.mixed_order hoisted terms.

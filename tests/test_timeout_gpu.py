@@ -23,17 +23,18 @@ from conftest import FP64_RTOL, rel_err
 
 pytestmark = pytest.mark.gpu
 
-# 512 bands = 2 band chunks per item; ncouls 4096 = 2 G chunks per row
-# (also for the mixed form); 300 rows: every CTA of the persistent grid has at
-# least 4 items, so every CTA reaches step 3.
-DIMS = dict(number_bands=512, nvband=2, ncouls=4096, nodes_per_group=14)
+# 512 bands, ncouls 8192, 585 rows: the FP64 form has 2 band chunks x 4 G
+# chunks per row, the mixed form (4096-element chunks, all 512 bands per
+# step) 2 G chunks per row; every CTA of either persistent grid gets at
+# least 4 steps, so every CTA reaches step 3.
+DIMS = dict(number_bands=512, nvband=2, ncouls=8192, nodes_per_group=14)
 
 
 @pytest.fixture(scope="module")
 def gdev(cuda):
     import bgwsigma as bgw
     g = I.gpp_seeded(**DIMS, seed=71)
-    assert g.ngpown >= 290
+    assert g.ngpown >= 585
     return g, bgw.to_device(g, cuda)
 
 
