@@ -609,34 +609,11 @@ def run_ours(args, world, rank, local):
 
 
 def make_batch_device(I, dev, n=64, seed=4321):
-    """The batched workload generated on the GPU (seeded torch generator):
-    ncouls uniform in {4096, 4608, ..., 32768}, number_bands uniform in
-    [128, 512], nodes_per_group 20, the benchmark distributions."""
-    import torch
-    rng = np.random.default_rng(seed)
-    gen = torch.Generator(device=dev)
-    gen.manual_seed(seed)
-    out = []
-    for _ in range(n):
-        G = int(rng.choice(np.arange(4096, 32768 + 1, 512)))
-        nb = int(rng.integers(128, 513))
-        P = G // 20
-
-        def cu(rows, lo, hi):
-            t = torch.rand((rows, G, 2), generator=gen, device=dev, dtype=torch.float64)
-            t.mul_(hi - lo).add_(lo)
-            return torch.view_as_complex(t)
-        wt = torch.rand((P, G, 2), generator=gen, device=dev, dtype=torch.float64)
-        wt[..., 0].mul_(1.5).add_(0.5)
-        wt[..., 1].mul_(0.02).sub_(0.01)
-        indinv = torch.cat([torch.randperm(G, generator=gen, device=dev), torch.tensor([G - 1], device=dev)])
-        out.append(I.GppInputs(
-            number_bands=nb, nvband=2, ncouls=G, ngpown=P,
-            inv_igp_index=(torch.arange(P, device=dev) * 20).to(torch.int32), indinv=indinv.to(torch.int32),
-            wx_array=torch.tensor([9.5, 10.0, 10.5], device=dev, dtype=torch.float64),
-            wtilde_array=torch.view_as_complex(wt), aqsmtemp=cu(nb, -1.0, 1.0), aqsntemp=cu(nb, -1.0, 1.0),
-            I_eps_array=cu(P, -0.5, 0.5), vcoul=1.0 / (1.0 + torch.arange(G, device=dev, dtype=torch.float64))))
-    return out
+    """The batched workload generated on the GPU: shapes from
+    bgwsigma.inputs.batch_shapes (ncouls uniform in {4096, 4608, ..., 32768},
+    number_bands in [128, 512], nodes_per_group 20), values by the library's
+    counter-based fill (bgw_fill_uniform) with the benchmark distributions."""
+    return I.batch_philox(n, seed, device=dev)
 
 
 def bench_batched(bgw, I, dev, sh, stream, dfma_peak, rank):
@@ -646,7 +623,8 @@ def bench_batched(bgw, I, dev, sh, stream, dfma_peak, rank):
     flops = sum(63.0 * g.number_bands * g.ngpown * g.ncouls for g in insts)
     stream_bytes = sum(32.0 * g.ngpown * g.ncouls for g in insts)
     res = {"workload": "64 instances, ncouls uniform in {4096..32768 step 512}, number_bands in [128, 512], "
-                       "nodes_per_group 20; inputs generated on the GPU", "device_bytes": nbytes}
+                       "nodes_per_group 20; inputs generated on the GPU by bgw_fill_uniform (Philox4x64-10)",
+           "device_bytes": nbytes}
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
     def timed(fn, reps):

@@ -230,6 +230,28 @@ def gpp_philox(number_bands: int, nvband: int, ncouls: int, nodes_per_group: int
     return GppInputs(number_bands=nb, nvband=nvband, ncouls=G, ngpown=P, wx_band_stride=0, **small, **big)
 
 
+def batch_shapes(n: int = 64, seed: int = 4321) -> list[tuple[int, int]]:
+    """(number_bands, ncouls) of the batched uneven q-point workload: ncouls
+    uniform in {4096, 4608, ..., 32768}, number_bands uniform in [128, 512]
+    (nodes_per_group 20), drawn from PCG64 in a fixed order."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        G = int(rng.choice(np.arange(4096, 32768 + 1, 512)))
+        nb = int(rng.integers(128, 513))
+        out.append((nb, G))
+    return out
+
+
+def batch_philox(n: int = 64, seed: int = 4321, device=None, only=None) -> list[GppInputs]:
+    """The batched workload's instances (batch_shapes), instance k drawn from
+    gpp_philox with seed + k (on `device`, or on the host).  only: indices of
+    the instances to generate (the others are None)."""
+    shapes = batch_shapes(n, seed)
+    return [gpp_philox(nb, 2, G, 20, seed=seed + k, device=device) if only is None or k in only else None
+            for k, (nb, G) in enumerate(shapes)]
+
+
 # ------------------------------------------------------------------ FF --
 
 def ff_uniform(number_bands: int, nvband: int, ncouls: int, ngpown: int, nFreq: int, nfreqeval: int) -> FFInputs:

@@ -18,8 +18,8 @@
 // prefix of the work list (bgw_gpp_batch_create): FP64 8, 4 or 2 (8: one CTA
 // per SM, the per-band combination amortised over 24 terms); choices are
 // cached per batch signature for the process.  The mixed form (the hoisted
-// expansion of the single-instance band loop, K = mixed_order) runs at 8
-// elements per thread, as the single-instance kernel does.
+// expansion of the single-instance band loop, K = mixed_order) runs at 16
+// elements per thread over 512-band steps, as the single-instance kernel does.
 #include <algorithm>
 #include <climits>
 #include <cmath>
@@ -115,10 +115,12 @@ __global__ void batch_wx_kernel(const BatchInst *__restrict__ inst, int n) {
   }
 }
 
+// The mixed form reads its elements from global memory (as the
+// single-instance mixed band loop does) and stages only the band rows.
 template <int BCH, int KE, bool MIXED>
 struct BatchSmem {
-  double2 wt[2][kBThreads * KE];
-  double2 ie[2][kBThreads * KE];
+  double2 wt[2][MIXED ? 1 : kBThreads * KE];
+  double2 ie[2][MIXED ? 1 : kBThreads * KE];
   double2 st[2][BCH];
   double4 wx[2][BCH];
   unsigned long long bar[3];  // [2]: never arrived on (stall injection)
@@ -144,7 +146,7 @@ __device__ __forceinline__ void flush(double (&acc_r)[3], double (&acc_i)[3], do
 // Band loop over this CTA's range [range[b], range[b+1]) of the global item
 // list.  Steps are (item, band chunk); step s+1 is staged while s computes.
 template <int BCH, int KE, bool MIXED, int K = 3>
-__global__ void __launch_bounds__(kBThreads, KE == 8 ? 1 : 2)
+__global__ void __launch_bounds__(kBThreads, KE >= 8 ? 1 : 2)
     batch_bandloop_kernel(const BatchInst *__restrict__ inst, int n, const long long *__restrict__ range,
                           int max_seg, double *__restrict__ partials, int *status, long long stall) {
   constexpr int kCH = kBThreads * KE;
@@ -193,9 +195,11 @@ __global__ void __launch_bounds__(kBThreads, KE == 8 ? 1 : 2)
       mbar_expect_tx(bar, 0);
       return;
     }
-    mbar_expect_tx(bar, 2u * nvalid * 16u + nbv * 48u);
-    bulk_g2s(sm.wt[buf], I.wt + (size_t)p * I.G + g0, nvalid * 16u, bar);
-    bulk_g2s(sm.ie[buf], I.ie + (size_t)p * I.G + g0, nvalid * 16u, bar);
+    mbar_expect_tx(bar, (MIXED ? 0u : 2u * nvalid * 16u) + nbv * 48u);
+    if constexpr (!MIXED) {
+      bulk_g2s(sm.wt[buf], I.wt + (size_t)p * I.G + g0, nvalid * 16u, bar);
+      bulk_g2s(sm.ie[buf], I.ie + (size_t)p * I.G + g0, nvalid * 16u, bar);
+    }
     if (nbv > 0) {
       bulk_g2s(sm.st[buf], I.tab + (size_t)p * I.nb + b0, nbv * 16u, bar);
       bulk_g2s(sm.wx[buf], I.wx4 + b0, nbv * 32u, bar);
@@ -232,12 +236,13 @@ __global__ void __launch_bounds__(kBThreads, KE == 8 ? 1 : 2)
     if (!BGW_CHECKED(nvalid <= kCH && nbv <= BCH, status, 32)) nvalid = nbv = 0;
     // MIXED: elements near the chunk's frequencies are summed in FP64.
     if constexpr (MIXED) {
+      const double2 *wt_g = I.wt + (size_t)(local / I.nchunk) * I.G + g0;
+      const double2 *ie_g = I.ie + (size_t)(local / I.nchunk) * I.G + g0;
       const RemStep rs = rem_stage<kBThreads, K>(sm.wx[buf], sm.st[buf], nbv, sm.rows, sm.red, sm.xr_lo, sm.xr_hi);
       RemElems<KE> e;
-      const uint32_t near = rem_elems<KE, K>(e, sm.wt[buf], sm.ie[buf], nvalid, kBThreads, tid, rs, 0.0, acc_r,
-                                             acc_i);
+      const uint32_t near = rem_elems<KE, K>(e, wt_g, ie_g, nvalid, kBThreads, tid, rs, 0.0, acc_r, acc_i);
       rem_sweep<KE>(e, sm.rows, nbv, acc_r, acc_i, lo_r, lo_i);
-      if (near) near_sweep(near, sm.wt[buf], sm.ie[buf], kBThreads, tid, sm.wx[buf], sm.st[buf], nbv, 0.0, acc_r,
+      if (near) near_sweep(near, wt_g, ie_g, kBThreads, tid, sm.wx[buf], sm.st[buf], nbv, 0.0, acc_r,
                            acc_i, lo_r, lo_i);
     } else {
       Elem<double> e[KE];
@@ -364,11 +369,17 @@ struct Variant {
   int per_sm;      // resident CTAs per SM
 };
 
+// Band rows per step: FP64 256 (with the staged elements), mixed 512.
+template <bool MIXED>
+constexpr int batch_bch() {
+  return MIXED ? 512 : 256;
+}
+
 template <int KE, bool MIXED, int K = 3>
 int band_variant(Variant *v) {
   v->ke = KE;
-  v->smem = sizeof(BatchSmem<256, KE, MIXED>);
-  auto kfn = batch_bandloop_kernel<256, KE, MIXED, K>;
+  v->smem = sizeof(BatchSmem<batch_bch<MIXED>(), KE, MIXED>);
+  auto kfn = batch_bandloop_kernel<batch_bch<MIXED>(), KE, MIXED, K>;
   BGW_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v->smem));
   BGW_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v->per_sm, kfn, kBThreads, v->smem));
   return v->per_sm >= 1 ? BGW_OK : BGW_ERR_UNSUPPORTED;
@@ -377,8 +388,8 @@ int band_variant(Variant *v) {
 template <int KE, bool MIXED, int K = 3>
 void launch_band(cudaStream_t s, int grid, size_t smem, const BatchInst *inst, int n, const long long *range,
                  int max_seg, double *partials, int *status, long long stall) {
-  batch_bandloop_kernel<256, KE, MIXED, K><<<grid, kBThreads, smem, s>>>(inst, n, range, max_seg, partials, status,
-                                                                         stall);
+  batch_bandloop_kernel<batch_bch<MIXED>(), KE, MIXED, K><<<grid, kBThreads, smem, s>>>(inst, n, range, max_seg,
+                                                                                        partials, status, stall);
 }
 
 std::mutex g_tune_mu;
@@ -418,14 +429,18 @@ namespace {
 // Cuts items [0, limit) into `grid` ranges of equal estimated cost (per item:
 // bands x elements for the band loop, elements for the factored stream, plus
 // a fixed per-item overhead).
-void partition(const std::vector<BatchInst> &inst, bool factored, int kch, long long limit, int grid,
+void partition(const std::vector<BatchInst> &inst, bool factored, int kch, int bch, long long limit, int grid,
                std::vector<long long> *range) {
   const int n = (int)inst.size();
   std::vector<double> cum(n + 1, 0.0), per(n, 0.0);
   for (int i = 0; i < n; ++i) {
     const long long items = (long long)inst[i].P * inst[i].nchunk;
     const double elems = inst[i].nchunk > 0 ? (double)inst[i].G / inst[i].nchunk : 0.0;
-    per[i] = (factored ? elems : elems * std::max(inst[i].nb, 1)) + 0.25 * kch;
+    // The band loop sweeps every slot of a chunk, padding included (an item
+    // costs kch x bands), plus about two bands' worth per staged step; the
+    // factored stream skips the padding.
+    const int nb = std::max(inst[i].nb, 1), steps = (nb + bch - 1) / bch;
+    per[i] = factored ? elems + 0.25 * kch : (double)kch * (nb + 2.0 * steps);
     const long long lim = std::max(0LL, std::min(items, limit - inst[i].item0));
     cum[i + 1] = cum[i] + per[i] * (double)lim;
   }
@@ -492,10 +507,10 @@ int enqueue_batch(bgw_gpp_batch *B, cudaStream_t s, long long stall = -1) {
     batch_wx_kernel<<<std::min(ninst, 1024), 256, 0, s>>>(B->d_inst, ninst);
     BGW_CUDA_TRY(cudaGetLastError());
     if (B->mixed) {
-      auto *fn = B->mixed_order == 0   ? launch_band<8, true, 0>
-                 : B->mixed_order == 1 ? launch_band<8, true, 1>
-                 : B->mixed_order == 2 ? launch_band<8, true, 2>
-                                       : launch_band<8, true, 3>;
+      auto *fn = B->mixed_order == 0   ? launch_band<16, true, 0>
+                 : B->mixed_order == 1 ? launch_band<16, true, 1>
+                 : B->mixed_order == 2 ? launch_band<16, true, 2>
+                                       : launch_band<16, true, 3>;
       fn(s, B->grid, B->smem, B->d_inst, ninst, B->d_range, B->max_seg, B->d_partials, B->d_status, stall);
     } else {
       if (B->ke == 8) launch_band<8, false>(s, B->grid, B->smem, B->d_inst, ninst, B->d_range, B->max_seg,
@@ -599,10 +614,10 @@ extern "C" int bgw_gpp_batch_create(const bgw_gpp_instance *instances, int64_t n
   } else if (mixed) {
     Variant a;
     switch (env.opt.mixed_order) {
-      case 0: BGW_TRY((band_variant<8, true, 0>(&a))); break;
-      case 1: BGW_TRY((band_variant<8, true, 1>(&a))); break;
-      case 2: BGW_TRY((band_variant<8, true, 2>(&a))); break;
-      default: BGW_TRY((band_variant<8, true, 3>(&a))); break;
+      case 0: BGW_TRY((band_variant<16, true, 0>(&a))); break;
+      case 1: BGW_TRY((band_variant<16, true, 1>(&a))); break;
+      case 2: BGW_TRY((band_variant<16, true, 2>(&a))); break;
+      default: BGW_TRY((band_variant<16, true, 3>(&a))); break;
     }
     cands = {a};
   } else {
@@ -637,7 +652,7 @@ extern "C" int bgw_gpp_batch_create(const bgw_gpp_instance *instances, int64_t n
     if (limit < 0 || limit > item) limit = item;
     *grid = (int)std::max<long long>(1, std::min<long long>((long long)ws->sm_count * v.per_sm,
                                                               std::max<long long>(limit, 1)));
-    partition(h, factored, kch, limit, *grid, range);
+    partition(h, factored, kch, mixed ? batch_bch<true>() : batch_bch<false>(), limit, *grid, range);
     assign_slots(h, *range, cta_lo, max_seg);
   };
 

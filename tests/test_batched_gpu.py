@@ -82,3 +82,26 @@ def test_batch_requires_device_memory(bgw, cuda):
     hosts, _ = _batch_inputs(cuda)
     with pytest.raises(ValueError):
         bgw.GppBatch(hosts)
+
+
+def test_64_instance_config_subset_vs_oracle(bgw, oracle, cuda):
+    """The batched workload at its full size (64 uneven q-point instances,
+    ~54 GB generated on the GPU by bgw_fill_uniform): the one persistent
+    launch's results for a subset of the instances -- the smallest, the
+    largest and two others -- match the oracle on the same inputs (the host
+    twin of the fill), FP64 at 1e-12 and mixed at 1e-9."""
+    import torch
+    from bgwsigma import inputs as I
+    shapes = I.batch_shapes()
+    sizes = [nb * G for nb, G in shapes]
+    pick = sorted({int(np.argmin(sizes)), int(np.argmax(sizes)), 17, 42})
+    devs = I.batch_philox(device=cuda)
+    want = {k: oracle.gpp(h, factored=True) for k, h in enumerate(I.batch_philox(only=pick)) if h is not None}
+    for prec, tol in (("fp64", FP64_RTOL), ("mixed", MIXED_RTOL)):
+        b = bgw.GppBatch(devs, algorithm="bandloop", precision=prec)
+        out = b.execute().cpu().numpy()
+        b.close()
+        for k in pick:
+            assert rel_err(out[k], want[k]) < tol, (prec, k, rel_err(out[k], want[k]))
+    del devs
+    torch.cuda.empty_cache()
