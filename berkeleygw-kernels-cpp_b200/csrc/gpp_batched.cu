@@ -429,18 +429,18 @@ namespace {
 // Cuts items [0, limit) into `grid` ranges of equal estimated cost (per item:
 // bands x elements for the band loop, elements for the factored stream, plus
 // a fixed per-item overhead).
-void partition(const std::vector<BatchInst> &inst, bool factored, int kch, int bch, long long limit, int grid,
-               std::vector<long long> *range) {
+void partition(const std::vector<BatchInst> &inst, bool factored, int kch, int bch, double step_bands,
+               long long limit, int grid, std::vector<long long> *range) {
   const int n = (int)inst.size();
   std::vector<double> cum(n + 1, 0.0), per(n, 0.0);
   for (int i = 0; i < n; ++i) {
     const long long items = (long long)inst[i].P * inst[i].nchunk;
     const double elems = inst[i].nchunk > 0 ? (double)inst[i].G / inst[i].nchunk : 0.0;
     // The band loop sweeps every slot of a chunk, padding included (an item
-    // costs kch x bands), plus about two bands' worth per staged step; the
-    // factored stream skips the padding.
+    // costs kch x bands), plus a per-step set-up of step_bands bands' worth;
+    // the factored stream skips the padding.
     const int nb = std::max(inst[i].nb, 1), steps = (nb + bch - 1) / bch;
-    per[i] = factored ? elems + 0.25 * kch : (double)kch * (nb + 2.0 * steps);
+    per[i] = factored ? elems + 0.25 * kch : (double)kch * (nb + step_bands * steps);
     const long long lim = std::max(0LL, std::min(items, limit - inst[i].item0));
     cum[i + 1] = cum[i] + per[i] * (double)lim;
   }
@@ -652,7 +652,11 @@ extern "C" int bgw_gpp_batch_create(const bgw_gpp_instance *instances, int64_t n
     if (limit < 0 || limit > item) limit = item;
     *grid = (int)std::max<long long>(1, std::min<long long>((long long)ws->sm_count * v.per_sm,
                                                               std::max<long long>(limit, 1)));
-    partition(h, factored, kch, mixed ? batch_bch<true>() : batch_bch<false>(), limit, *grid, range);
+    // Per-step set-up in bands' worth (measured on the single-instance
+    // kernels): FP64 staging ~2; mixed band moments and FP64 hoisted terms
+    // ~16 (about a tenth of a 128-band step).
+    partition(h, factored, kch, mixed ? batch_bch<true>() : batch_bch<false>(), mixed ? 16.0 : 2.0, limit, *grid,
+              range);
     assign_slots(h, *range, cta_lo, max_seg);
   };
 
