@@ -212,7 +212,18 @@ class Reference:
         lib.ref_ff_cor.argtypes = [_L, _L, _L, _L, _L, _L, _D, _D, _P, _P, _P, _P, _L, _P, _P, _P, _P, _P, _P]
         lib.ref_ff_cor.restype = None
         lib.ref_num_threads.restype = ctypes.c_int
+        lib.ref_compute_fact.argtypes = [_D, ctypes.c_int, _P, ctypes.c_int, ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_int), ctypes.POINTER(_D), ctypes.POINTER(_D)]
+        lib.ref_compute_fact.restype = None
         self.lib = lib
+
+    def compute_fact(self, wx: float, grid: np.ndarray, loop: int, flag_occ: bool):
+        """(ifreq, fact1, fact2) of the reference's own compute_fact (FF/ff.cpp:103-152)."""
+        g = np.ascontiguousarray(grid, dtype=np.float64)
+        i, f1, f2 = ctypes.c_int(0), _D(0.0), _D(0.0)
+        self.lib.ref_compute_fact(wx, len(g), _p(g), loop, int(flag_occ), ctypes.byref(i), ctypes.byref(f1),
+                                  ctypes.byref(f2))
+        return i.value, f1.value, f2.value
 
     @staticmethod
     def available() -> bool:

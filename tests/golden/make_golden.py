@@ -59,14 +59,16 @@ def main():
             "oracle": {"achs": c2l(orc.achs(f)), "asx": c2l(orc.asx(f)), "cor": c2l(orc.cor(f))},
         }
         print(name, out["ff"][name]["reference"]["achs"][0])
-    # compute_fact probes through the oracle (the reference's compute_fact is
-    # an inline helper of ff.cpp; its effect is pinned by ff_fact_edges).
+    # compute_fact probes through the reference's own compute_fact (an inline
+    # helper of ff.cpp, compiled from ff.cpp by oracle/ref_fact.cpp): every
+    # branch, bracket edges and the grid ends.
     grid = np.linspace(0.0, 2.0, 9)
     probes = []
-    for wx in [0.1, 0.25, 3.0, -0.1, -0.3, 0.0, 1.3, -2.5, 0.6, -0.25, 1.99, 2.0]:
+    for wx in [0.1, 0.25, 3.0, -0.1, -0.3, 0.0, 1.3, -2.5, 0.6, -0.25, 1.99, 2.0, 0.125, -0.125, 1e-9, -1e-9,
+               1.75, -1.75, 2.5, -2.0]:
         for loop in (1, 2):
             for occ in (False, True):
-                probes.append([wx, loop, int(occ), *orc.compute_fact(wx, grid, loop, occ)])
+                probes.append([wx, loop, int(occ), *ref.compute_fact(wx, grid, loop, occ)])
     # Mangled names of the reference kernels (the drop-in shim must export
     # exactly these), read from the objects built from the reference sources.
     import subprocess

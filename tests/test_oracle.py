@@ -89,9 +89,24 @@ def test_compute_fact_quirks(oracle):
 
 
 def test_compute_fact_golden(golden, oracle):
+    """The probe table holds the reference's own compute_fact (FF/ff.cpp:103-152,
+    compiled from ff.cpp by oracle/ref_fact.cpp): every branch and edge, bit for bit."""
     grid = np.array(golden["compute_fact_grid"])
     for wx, loop, occ, i, f1, f2 in golden["compute_fact"]:
         assert oracle.compute_fact(wx, grid, loop, bool(occ)) == (i, f1, f2)
+
+
+def test_compute_fact_live_if_built(oracle):
+    from oracle.oracle import Reference
+    if not Reference.available():
+        pytest.skip("reference build (oracle/_ref) not present on this machine")
+    ref = Reference()
+    rng = np.random.default_rng(12)
+    for grid in (np.linspace(0.0, 2.0, 15), np.sort(rng.uniform(0.0, 3.0, 11))):
+        for wx in rng.uniform(-4.0, 4.0, 200):
+            for loop in (1, 2):
+                for occ in (False, True):
+                    assert oracle.compute_fact(wx, grid, loop, occ) == ref.compute_fact(wx, grid, loop, occ)
 
 
 def test_reference_live_if_built(oracle):
