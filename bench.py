@@ -216,7 +216,9 @@ def run_ours(args, world, rank, local):
     bgw.load()
     dfma_peak, dmma_peak = bgw.measure_fp64_peak(local)
 
-    sharded = world > 1 and not args.replicas
+    # --shard at N = 1 runs the same path with one row block (the gather is
+    # then the rank's own partial): everything of the N > 1 step but NCCL.
+    sharded = (world > 1 or args.shard) and not args.replicas
     if sharded:
         # This rank's G' row block of the one Sigma, generated on its GPU.
         from bgwsigma import shard as SH
@@ -239,7 +241,7 @@ def run_ours(args, world, rank, local):
     def gather(local_out):
         """Sharded: all-gathers the ranks' partial achtemp (NCCL, after this
         rank's kernels on `stream`) and sums them in rank order."""
-        if not sharded:
+        if not sharded or pg is None:
             return local_out
         with torch.cuda.stream(stream):
             pg.all_gather(parts, local_out)
@@ -598,7 +600,9 @@ def run_ours(args, world, rank, local):
                 "scaling": "strong" if sharded else "weak", "vs_baseline": None, "dtype": "f64", "data": data,
                 "config": config_of(world),
                 "execution": (f"G' columns split over {world} GPUs (one NCCL all-gather of the partials per step)"
-                              if sharded else f"{world} independent Sigma evaluation(s), one per GPU"),
+                              if sharded and world > 1 else
+                              "G'-split path with one row block (Philox inputs generated on the GPU; no collective "
+                              "at one rank)" if sharded else f"{world} independent Sigma evaluation(s), one per GPU"),
                 "roofline": roofline, "cpu_baseline": cpu_baseline, "e2e": e2e, "gpu_launches": int(launches),
                 "clocks": clk, "extra": extra}
         print(json.dumps(line), flush=True)
@@ -740,6 +744,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and oracle check")
     ap.add_argument("--replicas", action="store_true",
                     help="with N > 1: one independent Sigma per GPU instead of one Sigma split over G'")
+    ap.add_argument("--shard", action="store_true",
+                    help="run the G'-split path (per-rank Philox inputs, gather) also at N = 1")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-instances extra")
     ap.add_argument("--only", choices=["gpp_bandloop", "gpp_mixed", "gpp_factored", "gpp_adjoint",
                                        "gpp_adjoint_bandloop", "gpp_sigma", "ff", "ff_mixed",
