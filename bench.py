@@ -499,7 +499,8 @@ def run_ours(args, world, rank, local):
             mds.append(pm["device_ms"])
         mk = statistics.mean(mks)
         extra["ff_mixed"] = {
-            "precision": "mixed: 6 int8 digits per operand, levels 2..7 (21 digit pairs), FP64 recombination",
+            "precision": "mixed: 5 balanced int8 digits per operand, levels 2..6 (15 digit pairs), int32 "
+                         "accumulation in tensor memory, FP64 recombination; slices cut inside the tcgen05 kernel",
             "s_per_sigma": statistics.mean(mds) / 1e3, "kernel": pm["main_kernel"], "contraction_ms": mk,
             "speedup_vs_fp64": statistics.mean(dms) / statistics.mean(mds),
             "effective_TFLOPs": pm["flops"] / (mk * 1e-3) / 1e12,
@@ -710,6 +711,7 @@ def run_only(args, local):
         d = bgw.to_device(I.ff_seeded(**dims, seed=1234), dev)
         prec = "mixed" if "mixed" in args.only else "fp64"
         fl = bgw.FLAG_PROFILE | (bgw.FLAG_FF_SLICE_ALL if args.only == "ff_mixed_all" else 0)
+        fl |= bgw.FLAG_FF_STAGED if args.only == "ff_mixed_staged" else 0
         fl |= bgw.FLAG_FF_WX_PER_IW if args.only.startswith("ff_per_iw") else 0
         call = lambda: bgw.ff_sigma(d, precision=prec, flags=fl)  # noqa: E731
     for _ in range(args.warmup):
@@ -749,7 +751,7 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-instances extra")
     ap.add_argument("--only", choices=["gpp_bandloop", "gpp_mixed", "gpp_factored", "gpp_adjoint",
                                        "gpp_adjoint_bandloop", "gpp_sigma", "ff", "ff_mixed",
-                                       "ff_mixed_all", "ff_per_iw", "ff_per_iw_mixed"],
+                                       "ff_mixed_all", "ff_mixed_staged", "ff_per_iw", "ff_per_iw_mixed"],
                     default=None,
                     help="diagnostic: time one kernel path only (for profilers)")
     ap.add_argument("--bands", type=int, default=0, help="with --only: number_bands override")

@@ -36,6 +36,7 @@ GPP_ALGO = {"bandloop": 0, "factored": 1, "auto": 2}
 FLAG_ASYNC = 1
 FLAG_PROFILE = 2
 FLAG_FF_SLICE_ALL = 4
+FLAG_FF_STAGED = 16
 FLAG_FF_WX_PER_IW = 8
 
 # Every extern "C" symbol include/bgw_sigma.h declares.

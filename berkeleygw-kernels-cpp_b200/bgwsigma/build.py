@@ -35,7 +35,7 @@ SHIM_OBJ = LIB_DIR / "bgw_refshim.o"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                      "-Xptxas", "-warn-spills", f"-I{INCLUDE}"]
-CUDA_SOURCES = ["runtime.cu", "gpp.cu", "gpp_adjoint.cu", "gpp_batched.cu", "ff.cu", "ff_mixed.cu", "capi.cu", "peak.cu", "fill.cu"]
+CUDA_SOURCES = ["runtime.cu", "gpp.cu", "gpp_adjoint.cu", "gpp_batched.cu", "ff.cu", "ff_mixed.cu", "ff_fused.cu", "capi.cu", "peak.cu", "fill.cu"]
 
 
 def _nvcc() -> str:

@@ -365,7 +365,16 @@ int ff_call(int64_t nb, int64_t nvband, int64_t nE, int64_t G, int64_t P, int64_
     o_cor = cor;
   }
   const int64_t nb_w = (want_achs || want_cor) ? nb : nvband;
-  if (env->opt.precision == BGW_PRECISION_MIXED)
+  // Mixed precision: the fused kernel (digits cut inside the tensor-core
+  // kernel) unless the plan has per-iw outputs or the staged path is asked
+  // for; the staged path cuts both operands into digit buffers first.
+  const bool staged = plan.per_iw || (env->opt.flags & BGW_FLAG_FF_STAGED);
+  if (env->opt.precision == BGW_PRECISION_MIXED && !staged)
+    BGW_TRY(ff_launch_fused(env, plan, nb_w, nE, G, P, (const int32_t *)d_inv, (const int32_t *)d_ind, indinv_len,
+                            (const double2 *)d_am, (const double2 *)d_an, (const double *)d_vc,
+                            (const double2 *)d_R, r_f0, (const double2 *)d_A, a_f0,
+                            (env->opt.flags & BGW_FLAG_FF_SLICE_ALL) ? 1 : 0, o_achs, o_asx, o_cor));
+  else if (env->opt.precision == BGW_PRECISION_MIXED)
     BGW_TRY(ff_launch_mixed(env, plan, nb, nb_w, nE, G, P, (const int32_t *)d_inv, (const int32_t *)d_ind,
                             indinv_len, (const double2 *)d_am, (const double2 *)d_an, (const double *)d_vc,
                             (const double2 *)d_R, r_f0, (const double2 *)d_A, a_f0, o_achs, o_asx, o_cor));

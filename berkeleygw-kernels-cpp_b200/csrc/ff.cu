@@ -512,9 +512,21 @@ __global__ void __launch_bounds__(kFFThreads, 3)
     ff_contract_kernel(const FFTile *__restrict__ tiles, const FFRow *__restrict__ rows, int P, int G,
                        const double2 *__restrict__ aqsn, const double2 *__restrict__ R, int r_f0,
                        const double2 *__restrict__ A, int a_f0, const double2 *__restrict__ W,
-                       double *__restrict__ partials, int per_row, int nb, int n_rows, int *status) {
+                       double *__restrict__ partials, int per_row, int nb, int n_rows, int *status,
+                       const int *__restrict__ gate, const int *__restrict__ unit_flag) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   FFSmem &sm = *reinterpret_cast<FFSmem *>(smem_raw);
+  // A gated tile (FP64 recomputation of an integer-slice unit) runs only
+  // when that unit flagged a value outside its digit range; otherwise its
+  // partial is zero.
+  if (gate) {
+    const int u = gate[blockIdx.x];
+    if (u >= 0 && unit_flag[u] == 0) {
+      const int n = per_row ? 2 * kTM : 2;
+      for (int i = threadIdx.x; i < n; i += blockDim.x) partials[(size_t)blockIdx.x * n + i] = 0.0;
+      return;
+    }
+  }
   FFTile t = tiles[blockIdx.x];
   // Debug build: the tile's rows, columns and k range lie inside the plan
   // and the arrays (a failing tile contributes zero).
@@ -681,19 +693,21 @@ int ff_fp64_per_sm(int *per_sm) {
 
 int ff_launch_fp64_tiles(cudaStream_t stream, const FFTile *d_tiles, int ntiles, const FFRow *d_rows, int n_rows,
                          int64_t nb, int64_t P, int64_t G, const double2 *an, const double2 *R, int r_f0,
-                         const double2 *A, int a_f0, const double2 *W, double *partials, int *status, bool per_row) {
+                         const double2 *A, int a_f0, const double2 *W, double *partials, int *status, bool per_row,
+                         const int *gate, const int *unit_flag) {
   if (ntiles <= 0) return BGW_OK;
   int per_sm = 0;
   BGW_TRY(ff_fp64_per_sm(&per_sm));
   ff_contract_kernel<<<ntiles, kFFThreads, sizeof(FFSmem), stream>>>(d_tiles, d_rows, (int)P, (int)G, an, R, r_f0,
                                                                       A, a_f0, W, partials, per_row ? 1 : 0, (int)nb,
-                                                                      n_rows, status);
+                                                                      n_rows, status, gate, unit_flag);
   count_launch();
   BGW_CUDA_TRY(cudaGetLastError());
   return BGW_OK;
 }
 
 int ff_fp64_tile_rows() { return kTM; }
+int ff_fp64_tile_cols() { return kTN; }
 
 void ff_fp64_row_ids(const std::vector<FFTile> &tiles, std::vector<int> *row_of) {
   for (const auto &t : tiles)
@@ -795,7 +809,7 @@ int ff_launch(CallEnv *env, const FFPlan &plan, int64_t nb_w, int64_t nE, int64_
     ff_contract_kernel<<<ntiles, kFFThreads, smem, stream>>>(d_tiles, d_rows, (int)P, (int)G, an, R, r_f0, A, a_f0,
                                                              (const double2 *)W, (double *)partials,
                                                              per_row ? 1 : 0, (int)nb_w, (int)plan.rows.size(),
-                                                             env->d_status);
+                                                             env->d_status, nullptr, nullptr);
     count_launch();
     BGW_CUDA_TRY(cudaGetLastError());
   }

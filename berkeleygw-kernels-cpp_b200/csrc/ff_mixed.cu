@@ -598,6 +598,14 @@ void mix_segments(const std::vector<MixGroup> &mg, int PT, int KB, int sm_count,
 
 }  // namespace
 
+int ff_enqueue_out_finalize(cudaStream_t stream, const double *partials, const int *out_of, int n, int nE,
+                            double *achs, double *asx, double *cor) {
+  ff_mix_finalize_kernel<<<1, 256, 0, stream>>>(partials, out_of, n, nE, achs, asx, cor);
+  count_launch();
+  BGW_CUDA_TRY(cudaGetLastError());
+  return BGW_OK;
+}
+
 int ff_launch_mixed(CallEnv *env, const FFPlan &plan, int64_t nb, int64_t nb_w, int64_t nE, int64_t G, int64_t P,
                     const int32_t *inv, const int32_t *indinv, int64_t indinv_len, const double2 *am,
                     const double2 *an, const double *vc, const double2 *R, int r_f0, const double2 *A, int a_f0,

@@ -88,12 +88,19 @@ void ff_fp64_tiles(const std::vector<FFGroup> &groups, int64_t P, int64_t G, int
 // tile at `partials`, or with `per_row` one per tile row (ntiles x
 // ff_fp64_tile_rows(), zero for padding rows).
 // n_rows: rows of the plan; nb: rows of aqsn and W (both bound the debug
-// build's checks, which report through `status`).
+// build's checks, which report through `status`).  gate (optional, one
+// entry per tile): -1 runs the tile; u >= 0 runs it only if unit_flag[u] is
+// nonzero, and writes a zero partial otherwise.
 int ff_launch_fp64_tiles(cudaStream_t stream, const FFTile *d_tiles, int ntiles, const FFRow *d_rows, int n_rows,
                          int64_t nb, int64_t P, int64_t G, const double2 *an, const double2 *R, int r_f0,
                          const double2 *A, int a_f0, const double2 *W, double *partials, int *status,
-                         bool per_row = false);
+                         bool per_row = false, const int *gate = nullptr, const int *unit_flag = nullptr);
 int ff_fp64_tile_rows();
+int ff_fp64_tile_cols();
+// Sums each partial into its output (out_of[i]: 0 achs, 1 asx, 2 cor) in
+// index order; writes achs, asx[nE] and cor[nE] (null skipped).  One block.
+int ff_enqueue_out_finalize(cudaStream_t stream, const double *partials, const int *out_of, int n, int nE,
+                            double *achs, double *asx, double *cor);
 // Plan row of every per-row partial of `tiles` (-1 for padding rows),
 // appended to `row_of`.
 void ff_fp64_row_ids(const std::vector<FFTile> &tiles, std::vector<int> *row_of);
@@ -102,6 +109,15 @@ int ff_fp64_per_sm(int *per_sm);
 int ff_launch_mixed(CallEnv *env, const FFPlan &plan, int64_t nb, int64_t nb_w, int64_t nE, int64_t G, int64_t P,
                     const int32_t *inv, const int32_t *indinv, int64_t indinv_len, const double2 *am,
                     const double2 *an, const double *vc, const double2 *R, int r_f0, const double2 *A, int a_f0,
+                    double *achs_dev, double *asx_dev, double *cor_dev);
+
+// Mixed precision with the fused kernel (ff_fused.cu): the FP64 slices are
+// cut into integer digits inside the tensor-core kernel.  Groups of fewer
+// than `min_rows` rows stay on the FP64 kernel.  Not for per-iw plans.
+int ff_launch_fused(CallEnv *env, const FFPlan &plan, int64_t nb_w, int64_t nE, int64_t G, int64_t P,
+                    const int32_t *inv,
+                    const int32_t *indinv, int64_t indinv_len, const double2 *am, const double2 *an,
+                    const double *vc, const double2 *R, int r_f0, const double2 *A, int a_f0, int min_rows,
                     double *achs_dev, double *asx_dev, double *cor_dev);
 
 // Enqueues a planned FF evaluation.  Device pointers; R / A point at

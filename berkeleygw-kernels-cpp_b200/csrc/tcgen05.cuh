@@ -27,7 +27,8 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t smem_addr, uint32_t lbo, 
 }
 
 // Instruction descriptor of tcgen05.mma .kind::i8: signed A and B, S32
-// accumulator, both operands K-major, dense.
+// accumulator, both operands K-major, dense.  M = 128 takes N % 16 == 0,
+// 16 <= N <= 256.
 __host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
   return (2u << 4)                       // D format: S32
          | (1u << 7)                     // A: signed 8-bit
@@ -84,7 +85,19 @@ __device__ __forceinline__ void ld16(uint32_t taddr, int32_t (&v)[16]) {
         "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
       : "r"(taddr));
 }
+// Warp-wide: 32 lanes x 4 consecutive 32-bit columns.
+__device__ __forceinline__ void ld4(uint32_t taddr, int32_t (&v)[4]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
+               : "r"(taddr));
+}
 __device__ __forceinline__ void wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Orders this thread's earlier generic-proxy shared-memory writes before
+// later async-proxy reads (operands written with st.shared, read by MMAs).
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
 
 // Plain mbarrier arrive (count 1) by this thread.
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {

@@ -71,18 +71,22 @@ enum {
                           work with CUDA events on `stream`; read back with
                           bgw_last_profile() (synchronous calls only).     */
   BGW_FLAG_FF_SLICE_ALL = 4, /* FF with BGW_PRECISION_MIXED: integer-slice
-                          tensor-core products for every band group of more
-                          than 16 rows.  Default: only groups of at least
-                          128 rows (the sums over all bands), where they
-                          beat the FP64 tensor cores; smaller groups stay
-                          FP64.                                            */
-  BGW_FLAG_FF_WX_PER_IW = 8 /* FF asxDtemp / achDtemp_cor: evaluate every
+                          tensor-core products for every band group (staged
+                          path: every group of more than 16 rows).
+                          Default: groups of at least 8 rows (staged path:
+                          128 rows); smaller groups stay FP64.             */
+  BGW_FLAG_FF_WX_PER_IW = 8, /* FF asxDtemp / achDtemp_cor: evaluate every
                           point iw at wx = freqevalmin - ekq[n1] +
                           iw * freqevalstep, giving nfreqeval distinct
                           outputs.  Default (as FF/ff.cpp:245, 337): one
                           wx = freqevalmin - ekq[n1] + freqevalstep for all
                           iw, every output entry equal (the value at iw = 1
                           of this option).                                 */
+  BGW_FLAG_FF_STAGED = 16 /* FF with BGW_PRECISION_MIXED: cut both operands
+                          into digit buffers in HBM before the integer
+                          products (the path BGW_FLAG_FF_WX_PER_IW always
+                          takes).  Default: the frequency slices are cut
+                          inside the tensor-core kernel, read once.        */
 };
 
 typedef struct bgw_options {

@@ -14,9 +14,11 @@ from cases import FF_CASES
 pytestmark = pytest.mark.gpu
 
 MIXED_FF_RTOL = 1e-9
-# 0: integer slices for band groups of >= 128 rows (the default);
-# 4 (FLAG_FF_SLICE_ALL): for every group of more than 16 rows.
-ROUTES = [0, 4]
+# 0: fused kernel (slices cut inside the tensor-core kernel) for band groups
+# of >= 8 rows (the default); 4 (FLAG_FF_SLICE_ALL): for every group;
+# 16 (FLAG_FF_STAGED): digit buffers cut first, groups of >= 128 rows;
+# 20: staged, every group of more than 16 rows.
+ROUTES = [0, 4, 16, 20]
 
 
 @pytest.mark.parametrize("flags", ROUTES)
@@ -101,3 +103,53 @@ def test_bad_index_reported_mixed(bgw, cuda):
     assert e.value.status == -2
     g = I.ff_seeded(40, 2, 128, 16, 4, 2, seed=4)
     assert bgw.ff_sigma(g, precision="mixed", flags=4)[0] is not None
+
+
+def _first_block_small(f, rows, factor):
+    """Scales k < 32 of the given G' rows of every I_epsR / I_epsA slice by
+    `factor`: the fused kernel takes a row's digit scale from the first 32 k
+    of each 2048-k unit, so with factor < 1/2 the later values of those rows
+    do not fit and their units are recomputed in FP64."""
+    f.I_epsR_array = f.I_epsR_array.copy()
+    f.I_epsA_array = f.I_epsA_array.copy()
+    f.I_epsR_array[:, rows, :32] *= factor
+    f.I_epsA_array[:, rows, :32] *= factor
+    return f
+
+
+@pytest.mark.parametrize("flags", [0, 4])
+@pytest.mark.parametrize("rows", [slice(0, 1), slice(100, 300), slice(None)])
+def test_fused_out_of_range_units_recomputed(bgw, oracle, cuda, flags, rows):
+    """Units with a value outside their first-block digit range (one row,
+    a band of rows across two column tiles, every row) give the FP64 result
+    for exactly those units."""
+    f = _first_block_small(I.ff_seeded(90, 2, 3000, 300, 6, 3, seed=21), rows, 1e-3)
+    achs, asx, cor = bgw.ff_sigma(f, precision="mixed", flags=flags)
+    assert rel_err(achs, oracle.achs(f)) < MIXED_FF_RTOL
+    assert rel_err(asx, oracle.asx(f)) < MIXED_FF_RTOL
+    assert rel_err(cor, oracle.cor(f)) < MIXED_FF_RTOL
+
+
+def test_fused_zero_first_block_and_nan(bgw, oracle, cuda):
+    """A row whose first block is zero is recomputed in FP64; a NaN in a
+    slice reaches the output as in the FP64 path."""
+    f = _first_block_small(I.ff_seeded(60, 2, 2500, 140, 5, 2, seed=8), slice(3, 5), 0.0)
+    achs, asx, cor = bgw.ff_sigma(f, precision="mixed")
+    assert rel_err(achs, oracle.achs(f)) < MIXED_FF_RTOL
+    assert rel_err(cor, oracle.cor(f)) < MIXED_FF_RTOL
+    g = I.ff_seeded(60, 2, 2500, 140, 5, 2, seed=8)
+    g.I_epsR_array = g.I_epsR_array.copy()
+    g.I_epsR_array[1, 7, 2100] = np.nan
+    m = bgw.ff_sigma(g, precision="mixed")
+    p = bgw.ff_sigma(g)
+    assert np.isnan(m[0]) == np.isnan(p[0])
+    assert np.array_equal(np.isnan(m[2]), np.isnan(p[2]))
+
+
+def test_fused_matches_staged(bgw, cuda):
+    """The fused and staged integer paths agree to the digit truncation."""
+    f = I.ff_seeded(256, 2, 4096, 384, 8, 4, seed=5)
+    a = bgw.ff_sigma(f, precision="mixed")
+    b = bgw.ff_sigma(f, precision="mixed", flags=bgw.FLAG_FF_STAGED | bgw.FLAG_FF_SLICE_ALL)
+    for x, y in zip(a, b):
+        assert rel_err(x, y) < MIXED_FF_RTOL
