@@ -86,6 +86,7 @@ constexpr int kFHeadroom = 1;                          // bits above the first b
 constexpr int kFBThreads = 256;                        // band-row slicing
 constexpr int kFBK = kFWin / kFBThreads;               // consecutive k per slicing thread
 constexpr int kFuseMinRows = 8;                        // default: smaller groups stay FP64
+constexpr bool kFPair = true;                          // 2-CTA clusters share the slice conversion
 static_assert(kFBK == 8, "a slicing thread writes one 8-byte word per (plane, digit)");
 static_assert((kFM / 4) % kFConvWarps == 0, "every converter warp takes the same tasks per stage");
 constexpr int kFTasks = (kFM / 4) / kFConvWarps;  // tasks (4 rows x 32 k) per converter warp and stage
@@ -110,14 +111,19 @@ struct FuseRow {          // row slot
 };
 struct FuseUnit {         // columns [kFM pt, kFM pt + kFM) x k [k0, k1) of a chunk
   int chunk, pt, k0, k1;
+  int phantom;            // pair member without rows: converts its half of the tile only
+  int pad;
 };
 
 struct __align__(128) FuseSmem {
   int8_t x[kFStages][kFXStage];
   int8_t b[kFStages][kFBStageMax];
   uint64_t bfull[kFStages], xfull[kFStages], empty[kFStages], done;
+  uint64_t xlocal[kFStages];  // a pair: this CTA's half of the stage is written
   uint32_t tmem;
-  int ovf;
+  int ovf;                // a value of this CTA's rows did not fit
+  int ovf_peer;           // ... of the peer's rows (written by the peer)
+  int nrecv;              // stages whose half the peer sent (written by the peer)
   double mult[kFM];       // 2^(38 - E(p))
   double lim[kFM];        // values with |x| >= lim do not fit the digits
   int ex[kFM];            // E(p)
@@ -129,11 +135,13 @@ struct __align__(128) FuseSmem {
 // instead of spinning, so waiting threads leave the issue slots to the
 // converters.  Bounded: BGW_ERR_TIMEOUT after kWaitCycles.
 constexpr uint32_t kSuspendNs = 10000;
+// (Acquire at cluster scope: in 2-CTA pairs the peer's copies and MMA
+// commits complete these phases.)
 __device__ __forceinline__ bool try_wait_sleep(uint64_t *bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
       : "r"(smem_u32(bar)), "r"(parity), "r"(kSuspendNs)
@@ -156,6 +164,38 @@ __device__ __forceinline__ void prefetch_l2(const void *p) {
   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 constexpr int kFPrefetch = 3;  // stages the L2 prefetch runs ahead of the conversion
+// 2-CTA clusters: rank, peer shared-memory addresses, cluster barrier,
+// shared -> peer shared bulk copies completing on the peer's mbarrier, and
+// the MMA commit that arrives on the same mbarrier in both CTAs.
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t peer_addr(const void *p, uint32_t rank) {
+  uint32_t a;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(smem_u32(p)), "r"(rank));
+  return a;
+}
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_s2peer(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   dst),
+               "r"(smem_u32(src)), "r"(bytes), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ void st_peer(uint32_t addr, int v) {
+  asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+__device__ __forceinline__ void commit_pair(uint64_t *bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+          smem_u32(bar)),
+      "h"((uint16_t)3)
+      : "memory");
+}
 // Non-coherent 16-byte global load kept where it is written (asm volatile),
 // so loads issued a stage ahead stay a stage ahead.
 __device__ __forceinline__ double2 ld_nc(const double2 *p) {
@@ -288,6 +328,16 @@ __global__ void __launch_bounds__(kFBThreads)
   }
 }
 
+// PAIR: the grid is made of 2-CTA clusters; the two CTAs hold two chunks
+// (or one chunk and a phantom) of the same X tile and k range.  Each
+// converts half of the tile's 128 rows (CTA rank r: rows [64 r, 64 r + 64))
+// into its own stage buffer; once the half is written (xlocal), the
+// producer thread sends it to the peer's buffer with 20 bulk copies (one
+// per plane and 16-k column group) that complete on the peer's xfull
+// barrier, whose phase also waits for the peer's own half.  Each CTA's MMA
+// commit arrives on the empty barrier of both, so neither overwrites a
+// stage the other still reads.
+template <bool PAIR>
 __global__ void __launch_bounds__(kFThreads, 1)
     ff_fuse_kernel(const FuseUnit *__restrict__ units, const FuseChunk *__restrict__ chunks,
                    const FuseRow *__restrict__ frows, int n_slots, const int8_t *__restrict__ pack,
@@ -296,35 +346,35 @@ __global__ void __launch_bounds__(kFThreads, 1)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   FuseSmem &sm = *reinterpret_cast<FuseSmem *>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = PAIR ? cluster_rank() : 0u, peer = rank ^ 1u;
   const FuseUnit U = units[blockIdx.x];
   const FuseChunk C = chunks[U.chunk];
-  const int nrp = C.nrp;
+  const bool phantom = PAIR && U.phantom != 0;
+  const int nrp = phantom ? 0 : C.nrp;
   // Debug build: the chunk's shape and the unit's k range (a failing unit
-  // contributes zero).
-  if (!BGW_CHECKED(nrp >= 8 && nrp <= kFMaxRows && nrp % 8 == 0 && U.k0 >= 0 && U.k1 > U.k0 && U.k1 <= G &&
-                       U.k1 - U.k0 <= kFWin && U.k0 % kFWin == 0 && C.slot0 >= 0 && C.slot0 + nrp <= n_slots &&
-                       U.pt >= 0 && U.pt * kFM < P,
-                   status, 61)) {
-    if (threadIdx.x == 0) {
-      partials[2 * (size_t)blockIdx.x] = 0.0;
-      partials[2 * (size_t)blockIdx.x + 1] = 0.0;
-      unit_flag[blockIdx.x] = 0;
-    }
-    return;
-  }
+  // does no work and contributes zero).
+  const bool good = BGW_CHECKED((phantom || (nrp >= 8 && nrp <= kFMaxRows && nrp % 8 == 0)) && U.k0 >= 0 &&
+                                    U.k1 > U.k0 && U.k1 <= G && U.k1 - U.k0 <= kFWin && U.k0 % kFWin == 0 &&
+                                    C.slot0 >= 0 && C.slot0 + nrp <= n_slots && U.pt >= 0 && U.pt * kFM < P,
+                                status, 61);
   const int N = 2 * nrp;
-  const int ns = (U.k1 - U.k0 + kFK - 1) / kFK;  // stages
+  const int ns = good ? (U.k1 - U.k0 + kFK - 1) / kFK : 0;  // stages
   const int kb0 = U.k0 / kFK;
   const uint32_t bbytes = (uint32_t)(2 * kFS * N * kFK);  // stacks Sr and Si
+  constexpr int kT = PAIR ? 1 : 2;                         // conversion tasks per warp and stage
+  constexpr uint32_t kHalf = 2 * kFS * 2 * (kFM / 2) * 16;  // bytes of half the rows of a stage
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < kFStages; ++i) {
       mbar_init(&sm.bfull[i], 1);
-      mbar_init(&sm.xfull[i], kFConv);
-      mbar_init(&sm.empty[i], 1);
+      mbar_init(&sm.xfull[i], PAIR ? 1 : kFConv);
+      mbar_init(&sm.xlocal[i], kFConv);
+      mbar_init(&sm.empty[i], PAIR ? 2 : 1);
     }
     mbar_init(&sm.done, 1);
     sm.ovf = 0;
+    sm.ovf_peer = 0;
+    sm.nrecv = 0;
     fence_mbar_init();
   }
   __syncwarp();
@@ -334,22 +384,42 @@ __global__ void __launch_bounds__(kFThreads, 1)
   }
   tc::fence_before();
   __syncthreads();
+  if (PAIR) cluster_sync();  // both CTAs' barriers exist before any remote arrive or copy
   tc::fence_after();
   const uint32_t tmem = sm.tmem;
 
   if (warp == 0) {
-    // ---- band-row digits: one bulk copy per stage.
+    // ---- producer: the band-row digits (one bulk copy per stage) and, in
+    // a pair, this CTA's half of each converted stage to the peer.
     if (lane == 0) {
-      int issued = 0;
+      int issued = 0, nsent = 0;
       for (int j = 0; j < ns; ++j) {
         const int st = j % kFStages;
         if (j >= kFStages && !fwait(&sm.empty[st], ((j / kFStages) - 1) & 1, status)) break;
-        const int8_t *src = pack + C.b_off + (long long)(kb0 + j) * bbytes;
-        // Debug build: the block lies in the packed buffer.
-        if (!BGW_CHECKED(src >= pack && src + bbytes <= pack + pack_bytes, status, 62)) break;
-        mbar_expect_tx(&sm.bfull[st], bbytes);
-        bulk_g2s(sm.b[st], src, bbytes, &sm.bfull[st]);
-        issued = j + 1;
+        if (!phantom) {
+          const int8_t *src = pack + C.b_off + (long long)(kb0 + j) * bbytes;
+          // Debug build: the block lies in the packed buffer.
+          if (!BGW_CHECKED(src >= pack && src + bbytes <= pack + pack_bytes, status, 62)) break;
+          mbar_expect_tx(&sm.bfull[st], bbytes);
+          bulk_g2s(sm.b[st], src, bbytes, &sm.bfull[st]);
+          issued = j + 1;
+        }
+        if (PAIR) {
+          if (!fwait(&sm.xlocal[st], (j / kFStages) & 1, status)) break;
+          // This CTA's arrival on xfull, expecting the peer's half as bytes;
+          // then this half to the peer (the generic writes were made visible
+          // to the async proxy by each converter before xlocal).
+          mbar_expect_tx(&sm.xfull[st], kHalf);
+          const uint32_t pbar = peer_addr(&sm.xfull[st], peer);
+#pragma unroll 1
+          for (int pl = 0; pl < 2 * kFS; ++pl)
+#pragma unroll
+            for (int kg = 0; kg < 2; ++kg) {
+              const int8_t *hs = &sm.x[st][pl * kFXPlane + kg * kFXLbo + rank * (kFM / 2) * 16];
+              bulk_s2peer(peer_addr(hs, peer), hs, (kFM / 2) * 16, pbar);
+            }
+          nsent = j + 1;
+        }
       }
       // Copies still in flight (error paths only) land before the CTA exits.
       for (int t = 0; t < kFStages; ++t) {
@@ -357,6 +427,8 @@ __global__ void __launch_bounds__(kFThreads, 1)
         const int last = (issued - 1) - ((issued - 1 - t) % kFStages);
         (void)fwait(&sm.bfull[t], (last / kFStages) & 1, status);
       }
+      // The peer drains the stages sent to it before it exits.
+      if (PAIR) st_peer(peer_addr(&sm.nrecv, peer), nsent);
     }
     __syncwarp();
   } else if (warp == 1) {
@@ -370,51 +442,54 @@ __global__ void __launch_bounds__(kFThreads, 1)
       for (int j = 0; j < ns; ++j) {
         const int st = j % kFStages;
         const uint32_t par = (uint32_t)((j / kFStages) & 1);
-        if (!fwait(&sm.bfull[st], par, status) || !fwait(&sm.xfull[st], par, status)) break;
+        if ((!phantom && !fwait(&sm.bfull[st], par, status)) || !fwait(&sm.xfull[st], par, status)) break;
         tc::fence_after();
-        const uint32_t xs = xbase + (uint32_t)(st * kFXStage), bs = bbase + (uint32_t)(st * kFBStageMax);
+        if (!phantom) {
+          const uint32_t xs = xbase + (uint32_t)(st * kFXStage), bs = bbase + (uint32_t)(st * kFBStageMax);
 #pragma unroll 1
-        for (int s = 0; s < kFS; ++s) {
-          const uint64_t xr = tc::smem_desc(xs + (uint32_t)(s * kFXPlane), kFXLbo, 128);
-          const uint64_t xi = tc::smem_desc(xs + (uint32_t)((kFS + s) * kFXPlane), kFXLbo, 128);
-          const uint32_t ncol = (uint32_t)((kFS - s) * N);
-          for (uint32_t c0 = 0; c0 < ncol; c0 += 256) {
-            const uint32_t n = min(256u, ncol - c0);
-            const uint32_t idesc = tc::idesc_i8(kFM, (int)n);
-            const uint32_t d = tmem + (uint32_t)(s * N) + c0;
-            const uint64_t br = tc::smem_desc(bs + (c0 / 8) * 128, slbo, 128);
-            const uint64_t bi = tc::smem_desc(bs + sbytes + (c0 / 8) * 128, slbo, 128);
-            tc::mma_i8(d, xr, br, idesc, j > 0 || s > 0);
-            tc::mma_i8(d, xi, bi, idesc, true);
+          for (int s = 0; s < kFS; ++s) {
+            const uint64_t xr = tc::smem_desc(xs + (uint32_t)(s * kFXPlane), kFXLbo, 128);
+            const uint64_t xi = tc::smem_desc(xs + (uint32_t)((kFS + s) * kFXPlane), kFXLbo, 128);
+            const uint32_t ncol = (uint32_t)((kFS - s) * N);
+            for (uint32_t c0 = 0; c0 < ncol; c0 += 256) {
+              const uint32_t n = min(256u, ncol - c0);
+              const uint32_t idesc = tc::idesc_i8(kFM, (int)n);
+              const uint32_t d = tmem + (uint32_t)(s * N) + c0;
+              const uint64_t br = tc::smem_desc(bs + (c0 / 8) * 128, slbo, 128);
+              const uint64_t bi = tc::smem_desc(bs + sbytes + (c0 / 8) * 128, slbo, 128);
+              tc::mma_i8(d, xr, br, idesc, j > 0 || s > 0);
+              tc::mma_i8(d, xi, bi, idesc, true);
+            }
           }
         }
-        tc::commit(&sm.empty[st]);  // stage reusable once these MMAs have read it
+        // Stage reusable once these MMAs (and, in a pair, the peer's) have read it.
+        if (PAIR)
+          commit_pair(&sm.empty[st]);
+        else
+          tc::commit(&sm.empty[st]);
       }
       tc::commit(&sm.done);
     }
     __syncwarp();
   } else {
-    // ---- converters, then the epilogue.  Task (rg, kg) of a stage: rows
-    // [8 rg, 8 rg + 8) x k [16 kg, 16 kg + 16); lane -> row 8 rg + lane / 4,
-    // k 16 kg + 4 (lane % 4) .. + 4, so a warp's digit words are one
-    // contiguous 128-byte core-matrix column per plane.
+    // ---- converters.  Conversion task (4 rows x 32 k): lane -> row
+    // base + lane / 8 and stage k q8 + 8 e (q8 = lane % 8, e < 4), digit
+    // word at stage position 4 q8.
     const int cw = warp - 2, ct = (int)threadIdx.x - 64;
     const int q8 = lane & 7, r4 = lane >> 3;
     const double2 *x0 = C.x0, *x1 = C.x1;
     const int p_base = U.pt * kFM;
-    // Task i of this warp in a stage: rows [4 tr, 4 tr + 4), tr = cw +
-    // kFConvWarps i, all 32 k; lane -> row 4 tr + lane / 8 and stage k
-    // q8 + 8 e (q8 = lane % 8, e < 4), digit word at stage position 4 q8.
-    auto task_row = [&](int i) { return (cw + kFConvWarps * i) * 4 + r4; };
+    // Rows of this CTA's task i (a pair's CTA converts its half of the tile).
+    auto task_row = [&](int i) { return (int)(PAIR ? rank * (kFM / 2) : 0) + (cw + kFConvWarps * i) * 4 + r4; };
     // Stages whose k range lies inside [k0, k1) of a column tile inside
     // [0, P) take the fast path (no clamping, no zeroing); the edges load
     // from clamped addresses and zero the values outside.
     const bool rows_inside = p_base + kFM <= P;
     auto inside = [&](int j) { return rows_inside && U.k0 + (j + 1) * kFK <= U.k1; };
-    auto issue = [&](double2 (&a)[4], double2 (&b)[4], int j, int i) {
+    auto issue = [&](double2 (&a)[4], double2 (&b)[4], int j, int row) {
       const int k = U.k0 + j * kFK + q8;
       if (inside(j)) {
-        const size_t o = (size_t)(p_base + task_row(i)) * (size_t)G + (size_t)k;
+        const size_t o = (size_t)(p_base + row) * (size_t)G + (size_t)k;
 #pragma unroll
         for (int e = 0; e < 4; ++e) a[e] = ld_nc(x0 + o + 8 * e);
         if (x1)
@@ -422,7 +497,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
           for (int e = 0; e < 4; ++e) b[e] = ld_nc(x1 + o + 8 * e);
         return;
       }
-      const int p = min(p_base + task_row(i), P - 1);
+      const int p = min(p_base + row, P - 1);
       const double2 *pa = x0 + (size_t)p * (size_t)G;
 #pragma unroll
       for (int e = 0; e < 4; ++e) a[e] = ld_nc(pa + min(k + 8 * e, U.k1 - 1));
@@ -432,16 +507,17 @@ __global__ void __launch_bounds__(kFThreads, 1)
         for (int e = 0; e < 4; ++e) b[e] = ld_nc(pb + min(k + 8 * e, U.k1 - 1));
       }
     };
-    // L2 prefetch of task (j, i): its 4 rows x 512 bytes of each slice, one
+    // L2 prefetch of a task's 4 rows x 512 bytes of each slice, one
     // 128-byte line per lane (lanes 0-3 of a row: x0, lanes 4-7: x1).
-    auto prefetch = [&](int j, int i) {
+    auto prefetch = [&](int j, int row) {
       const double2 *x = (q8 < 4) ? x0 : x1;
       if (!x) return;
-      const int p = min(p_base + task_row(i), P - 1);
+      const int p = min(p_base + row, P - 1);
       const int k = min(U.k0 + j * kFK + 8 * (q8 & 3), U.k1 - 1);
       prefetch_l2(x + (size_t)p * (size_t)G + k);
     };
-    auto value = [&](const double2 (&a)[4], const double2 (&b)[4], int j, int i, double (&cr)[4], double (&ci)[4]) {
+    auto value = [&](const double2 (&a)[4], const double2 (&b)[4], int j, int row, double (&cr)[4],
+                     double (&ci)[4]) {
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         double2 x = a[e];
@@ -453,7 +529,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
         ci[e] = x.y;
       }
       if (inside(j)) return;
-      const bool rv = p_base + task_row(i) < P;
+      const bool rv = p_base + row < P;
       const int k = U.k0 + j * kFK + q8;
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
@@ -462,28 +538,32 @@ __global__ void __launch_bounds__(kFThreads, 1)
         ci[e] = ok ? ci[e] : 0.0;
       }
     };
-    // Row scales from stage 0 (the unit's first kFK k): largest |re|, |im|.
+    // Row scales of all 128 rows from stage 0 (the unit's first kFK k):
+    // largest |re|, |im| (both CTAs of a pair compute the same values).
+    if (ns > 0) {
 #pragma unroll
-    for (int i = 0; i < kFTasks; ++i) {
-      double2 a[4], b[4];
-      issue(a, b, 0, i);
-      double cr[4], ci[4];
-      value(a, b, 0, i, cr, ci);
-      double m = 0.0;
+      for (int i = 0; i < 2; ++i) {
+        const int row = (cw + kFConvWarps * i) * 4 + r4;
+        double2 a[4], b[4];
+        issue(a, b, 0, row);
+        double cr[4], ci[4];
+        value(a, b, 0, row, cr, ci);
+        double m = 0.0;
 #pragma unroll
-      for (int e = 0; e < 4; ++e) m = fmax(m, fmax(fabs(cr[e]), fabs(ci[e])));
-      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, 1));
-      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, 2));
-      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, 4));
-      if (q8 == 0) sm.rmax[task_row(i)] = m;
+        for (int e = 0; e < 4; ++e) m = fmax(m, fmax(fabs(cr[e]), fabs(ci[e])));
+        m = fmax(m, __shfl_xor_sync(0xffffffffu, m, 1));
+        m = fmax(m, __shfl_xor_sync(0xffffffffu, m, 2));
+        m = fmax(m, __shfl_xor_sync(0xffffffffu, m, 4));
+        if (q8 == 0) sm.rmax[row] = m;
+      }
     }
     // Loads run one task ahead of the conversion, L2 prefetches kFPrefetch
     // stages ahead (so the loads are L2 hits).
     for (int j = 1; j <= kFPrefetch && j < ns; ++j)
 #pragma unroll
-      for (int i = 0; i < kFTasks; ++i) prefetch(j, i);
+      for (int i = 0; i < kT; ++i) prefetch(j, task_row(i));
     double2 ca[4], cb[4];
-    issue(ca, cb, 0, 0);
+    if (ns > 0) issue(ca, cb, 0, task_row(0));
     conv_sync();
     if (ct < kFM) {
       const double m = sm.rmax[ct];
@@ -509,15 +589,15 @@ __global__ void __launch_bounds__(kFThreads, 1)
       const int st = j % kFStages;
       if (j >= kFStages && !fwait(&sm.empty[st], ((j / kFStages) - 1) & 1, status)) break;
 #pragma unroll
-      for (int i = 0; i < kFTasks; ++i) {
-        if (j + kFPrefetch < ns) prefetch(j + kFPrefetch, i);
-        double cr[4], ci[4];
-        value(ca, cb, j, i, cr, ci);
-        if (i + 1 < kFTasks)
-          issue(ca, cb, j, i + 1);
-        else if (j + 1 < ns)
-          issue(ca, cb, j + 1, 0);
+      for (int i = 0; i < kT; ++i) {
         const int row = task_row(i);
+        if (j + kFPrefetch < ns) prefetch(j + kFPrefetch, row);
+        double cr[4], ci[4];
+        value(ca, cb, j, row, cr, ci);
+        if (i + 1 < kT)
+          issue(ca, cb, j, task_row(i + 1));
+        else if (j + 1 < ns)
+          issue(ca, cb, j + 1, task_row(0));
         const double mult = sm.mult[row], lim = sm.lim[row];
         uint32_t wr[kFS], wi[kFS];
         digits4(cr, mult, lim, ovf, wr);
@@ -533,18 +613,39 @@ __global__ void __launch_bounds__(kFThreads, 1)
         }
       }
       tc::fence_proxy_async_smem();
-      tc::mbar_arrive(&sm.xfull[st]);
+      tc::mbar_arrive(PAIR ? &sm.xlocal[st] : &sm.xfull[st]);
     }
     if (ovf) sm.ovf = 1;
-
+    conv_sync();
+    // A pair: the peer learns whether a value of this CTA's rows did not fit.
+    if (PAIR && ct == 0 && sm.ovf) st_peer(peer_addr(&sm.ovf_peer, peer), 1);
+  }
+  // ---- all roles have issued their work; wait for the MMAs.
+  bool dn = true;
+  if (lane == 0 && warp != 1) dn = fwait(&sm.done, 0, status);
+  dn = __shfl_sync(0xffffffffu, (int)dn, 0) != 0;
+  if (PAIR) {
+    cluster_sync();  // the peer's nrecv / ovf_peer are visible, and it issues nothing more
+    // Copies the peer sent into this CTA land before it exits (they have
+    // already, unless a wait ran out).
+    if (threadIdx.x == 64) {
+      const int n = sm.nrecv;
+      for (int t = 0; t < kFStages; ++t) {
+        if (n <= t) continue;
+        const int last = (n - 1) - ((n - 1 - t) % kFStages);
+        (void)fwait(&sm.xfull[t], (last / kFStages) & 1, status);
+      }
+    }
+  } else {
+    __syncthreads();
+  }
+  tc::fence_after();
+  if (warp >= 2) {
     // ---- epilogue.  Warps cw < kFEpiWarps: lane quarter q = warp % 4 (TMEM
     // lanes = G' columns [32 q, 32 q + 32)), half hh = cw / 4 of the rows.
-    bool dn = true;
-    if (lane == 0) dn = fwait(&sm.done, 0, status);
-    dn = __shfl_sync(0xffffffffu, (int)dn, 0) != 0;
-    conv_sync();  // sm.ovf final
-    tc::fence_after();
-    const bool flagged = sm.ovf != 0;
+    const int cw = warp - 2, ct = (int)threadIdx.x - 64;
+    const int p_base = U.pt * kFM;
+    const bool flagged = (sm.ovf | sm.ovf_peer) != 0;
     if (cw < kFEpiWarps) {
       const int q = warp & 3, hh = cw >> 2;
       const int nh = nrp >> 1, j0 = hh * nh;
@@ -613,15 +714,15 @@ __global__ void __launch_bounds__(kFThreads, 1)
       }
       partials[2 * (size_t)blockIdx.x] = pr;
       partials[2 * (size_t)blockIdx.x + 1] = pi;
-      unit_flag[blockIdx.x] = flagged ? 1 : 0;
+      unit_flag[blockIdx.x] = (flagged && !phantom) ? 1 : 0;
     }
   }
   tc::fence_before();
-  __syncthreads();
+  if (PAIR)
+    cluster_sync();  // no remote access targets a CTA that has exited
+  else
+    __syncthreads();
   if (warp == 0) {
-    // Every MMA has completed before the columns are released.
-    if (lane == 0) (void)fwait(&sm.done, 0, status);
-    __syncwarp();
     tc::fence_after();
     tc::dealloc(tmem, 512);
   }
@@ -690,19 +791,24 @@ int ff_launch_fused(CallEnv *env, const FFPlan &plan, int64_t nb_w, int64_t nE, 
   group_chunk0.push_back((int)chunks.size());
   // Units in (group, window, column tile, chunk) order: the chunks of one
   // X tile run side by side (the tile comes from DRAM once, then L2), and
-  // so do the column tiles reading one chunk's digits.
+  // so do the column tiles reading one chunk's digits.  With kFPair the
+  // chunks of an X tile go in twos to 2-CTA clusters (an odd chunk count
+  // leaves a phantom partner that only converts its half of the tile).
   std::vector<FuseUnit> units;
   for (int gi = 0; gi < (int)big.size(); ++gi)
     for (int w = 0; w < NW; ++w)
       for (int pt = 0; pt < PT; ++pt)
-        for (int c = group_chunk0[gi]; c < group_chunk0[gi + 1]; ++c) {
-          FuseUnit u;
-          u.chunk = c;
-          u.pt = pt;
-          u.k0 = w * kFWin;
-          u.k1 = (int)std::min<int64_t>(G, (int64_t)(w + 1) * kFWin);
-          units.push_back(u);
-        }
+        for (int c = group_chunk0[gi]; c < group_chunk0[gi + 1]; c += kFPair ? 2 : 1)
+          for (int m = 0; m < (kFPair ? 2 : 1); ++m) {
+            FuseUnit u;
+            u.phantom = c + m >= group_chunk0[gi + 1] ? 1 : 0;
+            u.chunk = u.phantom ? c : c + m;
+            u.pt = pt;
+            u.k0 = w * kFWin;
+            u.k1 = (int)std::min<int64_t>(G, (int64_t)(w + 1) * kFWin);
+            u.pad = 0;
+            units.push_back(u);
+          }
 
   // FP64 tiles: the small groups (always run), then the recomputation tiles
   // of every unit (gated on its flag).
@@ -717,6 +823,7 @@ int ff_launch_fused(CallEnv *env, const FFPlan &plan, int64_t nb_w, int64_t nE, 
   const int tr = ff_fp64_tile_rows(), tcn = ff_fp64_tile_cols();
   for (int u = 0; u < (int)units.size(); ++u) {
     const FuseUnit &U = units[u];
+    if (U.phantom) continue;
     const FFGroup &g = big[chunk_group[U.chunk]];
     for (int r0 = 0; r0 < chunk_nr[U.chunk]; r0 += tr)
       for (int64_t p0 = (int64_t)U.pt * kFM; p0 < std::min<int64_t>(P, (int64_t)(U.pt + 1) * kFM); p0 += tcn) {
@@ -784,10 +891,23 @@ int ff_launch_fused(CallEnv *env, const FFPlan &plan, int64_t nb_w, int64_t nE, 
     count_launch();
     BGW_CUDA_TRY(cudaGetLastError());
     const int smem = (int)sizeof(FuseSmem);
-    BGW_CUDA_TRY(cudaFuncSetAttribute(ff_fuse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    ff_fuse_kernel<<<(unsigned)nu, kFThreads, smem, stream>>>(
-        (const FuseUnit *)(pb + o_un), d_ch, d_fr, ns, (const int8_t *)pack, off, d_sb, NW, W, (int)P, (int)G,
-        (int)nb_w, part + 2 * (size_t)nft, d_flag, env->d_status);
+    auto kern = ff_fuse_kernel<kFPair>;
+    BGW_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)nu);
+    cfg.blockDim = dim3(kFThreads);
+    cfg.dynamicSmemBytes = (size_t)smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kFPair ? 2 : 1;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    BGW_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, (const FuseUnit *)(pb + o_un), d_ch, d_fr, ns,
+                                    (const int8_t *)pack, off, (const double *)d_sb, NW, (const double2 *)W, (int)P,
+                                    (int)G, (int)nb_w, part + 2 * (size_t)nft, d_flag, env->d_status));
     count_launch();
     BGW_CUDA_TRY(cudaGetLastError());
   }
