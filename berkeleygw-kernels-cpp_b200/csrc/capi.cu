@@ -366,9 +366,9 @@ int ff_call(int64_t nb, int64_t nvband, int64_t nE, int64_t G, int64_t P, int64_
   }
   const int64_t nb_w = (want_achs || want_cor) ? nb : nvband;
   // Mixed precision: the fused kernel (digits cut inside the tensor-core
-  // kernel) unless the plan has per-iw outputs or the staged path is asked
-  // for; the staged path cuts both operands into digit buffers first.
-  const bool staged = plan.per_iw || (env->opt.flags & BGW_FLAG_FF_STAGED);
+  // kernel) unless the staged path is asked for, which cuts both operands
+  // into digit buffers first.
+  const bool staged = (env->opt.flags & BGW_FLAG_FF_STAGED) != 0;
   if (env->opt.precision == BGW_PRECISION_MIXED && !staged)
     BGW_TRY(ff_launch_fused(env, plan, nb_w, nE, G, P, (const int32_t *)d_inv, (const int32_t *)d_ind, indinv_len,
                             (const double2 *)d_am, (const double2 *)d_an, (const double *)d_vc,

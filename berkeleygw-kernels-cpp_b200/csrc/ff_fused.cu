@@ -342,7 +342,8 @@ __global__ void __launch_bounds__(kFThreads, 1)
     ff_fuse_kernel(const FuseUnit *__restrict__ units, const FuseChunk *__restrict__ chunks,
                    const FuseRow *__restrict__ frows, int n_slots, const int8_t *__restrict__ pack,
                    long long pack_bytes, const double *__restrict__ sB, int NW, const double2 *__restrict__ W, int P,
-                   int G, int nb_w, double *__restrict__ partials, int *__restrict__ unit_flag, int *status) {
+                   int G, int nb_w, double *__restrict__ partials, int *__restrict__ unit_flag, int per_row,
+                   int *status) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   FuseSmem &sm = *reinterpret_cast<FuseSmem *>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -698,7 +699,22 @@ __global__ void __launch_bounds__(kFThreads, 1)
       }
     }
     conv_sync();
-    if (ct == 0) {
+    if (per_row) {
+      // One partial per row slot (distinct outputs per iw: the plan's terms
+      // combine them); zero for padding slots and flagged units.
+      if (ct < kFMaxRows) {
+        double pr = 0.0, pi = 0.0;
+        if (!flagged && ct < nrp) {
+          const FuseRow fr = frows[C.slot0 + ct];
+          const double f = fr.coef * sB[(size_t)(C.slot0 + ct) * NW + U.k0 / kFWin];
+          pr = f * (((sm.red[0][ct][0] + sm.red[1][ct][0]) + sm.red[2][ct][0]) + sm.red[3][ct][0]);
+          pi = f * (((sm.red[0][ct][1] + sm.red[1][ct][1]) + sm.red[2][ct][1]) + sm.red[3][ct][1]);
+        }
+        partials[((size_t)blockIdx.x * kFMaxRows + ct) * 2 + 0] = pr;
+        partials[((size_t)blockIdx.x * kFMaxRows + ct) * 2 + 1] = pi;
+      }
+      if (ct == 0) unit_flag[blockIdx.x] = (flagged && !phantom) ? 1 : 0;
+    } else if (ct == 0) {
       double pr = 0.0, pi = 0.0;
       if (!flagged) {
         const int w = U.k0 / kFWin;
@@ -841,11 +857,23 @@ int ff_launch_fused(CallEnv *env, const FFPlan &plan, int64_t nb_w, int64_t nE, 
       }
   }
   const int nft = (int)ft.size(), nu = (int)units.size(), ns = (int)frows.size();
-  // Partials: FP64 tiles first, then one per unit.
-  std::vector<int> out_of(nft + nu);
-  for (int i = 0; i < nft; ++i) out_of[i] = ft[i].out;
-  for (int i = 0; i < nu; ++i) out_of[nft + i] = chunks[units[i].chunk].out;
+  // Partials: FP64 tiles first, then the units'.  One per tile / unit, or
+  // with distinct outputs per iw one per tile row / row slot, combined by the
+  // plan's terms (out_of then holds the plan row of each partial, -1: none).
+  const bool per_row = plan.per_iw;
+  std::vector<int> out_of;
+  if (per_row) {
+    ff_fp64_row_ids(ft, &out_of);
+    for (int i = 0; i < nu; ++i)
+      for (int j = 0; j < kFMaxRows; ++j)
+        out_of.push_back(!units[i].phantom && j < chunk_nr[units[i].chunk] ? chunk_row0[units[i].chunk] + j : -1);
+  } else {
+    out_of.resize(nft + nu);
+    for (int i = 0; i < nft; ++i) out_of[i] = ft[i].out;
+    for (int i = 0; i < nu; ++i) out_of[nft + i] = chunks[units[i].chunk].out;
+  }
   const size_t n_part = out_of.size();
+  const size_t unit_part0 = per_row ? (size_t)nft * ff_fp64_tile_rows() : (size_t)nft;  // first unit partial
 
   // Device buffers: packed band-row digits (TABLE0); plan tables, scales
   // and unit flags in one buffer (PLAN).
@@ -907,16 +935,23 @@ int ff_launch_fused(CallEnv *env, const FFPlan &plan, int64_t nb_w, int64_t nE, 
     cfg.numAttrs = 1;
     BGW_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, (const FuseUnit *)(pb + o_un), d_ch, d_fr, ns,
                                     (const int8_t *)pack, off, (const double *)d_sb, NW, (const double2 *)W, (int)P,
-                                    (int)G, (int)nb_w, part + 2 * (size_t)nft, d_flag, env->d_status));
+                                    (int)G, (int)nb_w, part + 2 * unit_part0, d_flag, per_row ? 1 : 0,
+                                    env->d_status));
     count_launch();
     BGW_CUDA_TRY(cudaGetLastError());
   }
   BGW_TRY(ff_launch_fp64_tiles(stream, (const FFTile *)(pb + o_ft), nft, (const FFRow *)(pb + o_rows),
                                (int)plan.rows.size(), nb_w, P, G, an, R, r_f0, A, a_f0, W, part, env->d_status,
-                               false, (const int *)(pb + o_gate), d_flag));
+                               per_row, (const int *)(pb + o_gate), d_flag));
   BGW_TRY(prof_mark(env, 2));
-  BGW_TRY(ff_enqueue_out_finalize(stream, part, (const int *)(pb + o_out), (int)n_part, (int)nE,
-                                  achs_dev, asx_dev, cor_dev));
+  if (per_row) {
+    FFTermTables tt;
+    ff_build_term_tables(plan, out_of, nE, &tt);
+    BGW_TRY(ff_launch_term_finalize(env, SLOT_TABLE1, tt, part, nE, achs_dev, asx_dev, cor_dev));
+  } else {
+    BGW_TRY(ff_enqueue_out_finalize(stream, part, (const int *)(pb + o_out), (int)n_part, (int)nE, achs_dev, asx_dev,
+                                    cor_dev));
+  }
   {
     double slices = 0.0;
     for (const auto &b : plan.slice_reads) slices += b;

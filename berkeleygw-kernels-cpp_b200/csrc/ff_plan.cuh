@@ -113,7 +113,7 @@ int ff_launch_mixed(CallEnv *env, const FFPlan &plan, int64_t nb, int64_t nb_w, 
 
 // Mixed precision with the fused kernel (ff_fused.cu): the FP64 slices are
 // cut into integer digits inside the tensor-core kernel.  Groups of fewer
-// than `min_rows` rows stay on the FP64 kernel.  Not for per-iw plans.
+// than `min_rows` rows stay on the FP64 kernel.
 int ff_launch_fused(CallEnv *env, const FFPlan &plan, int64_t nb_w, int64_t nE, int64_t G, int64_t P,
                     const int32_t *inv,
                     const int32_t *indinv, int64_t indinv_len, const double2 *am, const double2 *an,

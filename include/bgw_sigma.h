@@ -84,8 +84,7 @@ enum {
                           of this option).                                 */
   BGW_FLAG_FF_STAGED = 16 /* FF with BGW_PRECISION_MIXED: cut both operands
                           into digit buffers in HBM before the integer
-                          products (the path BGW_FLAG_FF_WX_PER_IW always
-                          takes).  Default: the frequency slices are cut
+                          products.  Default: the frequency slices are cut
                           inside the tensor-core kernel, read once.        */
 };
 
