@@ -84,10 +84,9 @@ constexpr int kFXStage = 2 * kFS * kFXPlane;           // Re digits 0-4, Im digi
 constexpr int kFBStageMax = 2 * kFS * 2 * kFMaxRows * kFK;  // stacks Sr, Si x digits x 2 rows x k
 constexpr int kFHeadroom = 1;                          // bits above the first block's largest value
 constexpr int kFBThreads = 256;                        // band-row slicing
-constexpr int kFBK = kFWin / kFBThreads;               // consecutive k per slicing thread
 constexpr int kFuseMinRows = 8;                        // default: smaller groups stay FP64
 constexpr bool kFPair = true;                          // 2-CTA clusters share the slice conversion
-static_assert(kFBK == 8, "a slicing thread writes one 8-byte word per (plane, digit)");
+static_assert(kFBThreads == 256, "band-row slicing: 8 warps, one per row slot of a group");
 static_assert((kFM / 4) % kFConvWarps == 0, "every converter warp takes the same tasks per stage");
 constexpr int kFTasks = (kFM / 4) / kFConvWarps;  // tasks (4 rows x 32 k) per converter warp and stage
 static_assert(kFS * 2 * kFMaxRows <= 512, "the level accumulators fit in tensor memory");
@@ -229,102 +228,120 @@ __device__ __forceinline__ void digits4(const double (&c)[4], double mult, doubl
   w[0] = __byte_perm(__byte_perm(hi[0], hi[1], 0x0040), __byte_perm(hi[2], hi[3], 0x0040), 0x5410);
 }
 
-// One CTA per (row slot, kFWin-k window): the window of aqsn[band] is read
-// once (coalesced, staged through shared memory), its largest |re| / |im|
-// m < 2^e gives the digit scale (2^(e + 2) to sB[slot][w]; NaN when the
-// window holds a non-finite value), and each value's kFS digits go to the
-// chunk's packed block of its 32-k stage: stack Sr (row 2 nrp t + r: ar
-// digit t; row 2 nrp t + nrp + r: ai digit t), then stack Si (-ai, ar),
-// each 10 nrp rows x 32 k in the canonical K-major layout (core matrices of
-// 8 rows x 16 bytes; 16-k column groups 10 nrp x 16 bytes apart).
-// Padding slots and k >= G are written as zero digits.
+// One CTA per (chunk, kFWin-k window, group of 8 row slots), 8 warps.
+// Pass 1: warp r reads row slot r's window of aqsn[band] (coalesced) and its
+// largest |re| / |im| m < 2^e gives the digit scale (2^(e + 2) to
+// sB[slot][w]; NaN when the window holds a non-finite value).  Pass 2 (the
+// window again, from L2): warp w takes the stages w, w + 8, ...; lane ->
+// (row r = lane / 4, u = lane % 4) writes stage positions [8u, 8u + 8)
+// (position 4 q + e holds stage k = q + 8 e, so byte 4 hq + e of its 8
+// takes k = 2u + hq + 8 e) of its row in every digit plane: stack Sr (row
+// 2 nrp t + slot: ar digit t; row 2 nrp t + nrp + slot: ai digit t), then
+// stack Si (-ai, ar), each 10 nrp rows x 32 k in the canonical K-major
+// layout (core matrices of 8 rows x 16 bytes; 16-k column groups 10 nrp x
+// 16 bytes apart).  A warp's 8-byte stores of one plane cover two whole
+// 128-byte lines.  Padding slots and k >= G are written as zero digits.
+struct BSliceTask {  // (chunk, group of 8 row slots)
+  int chunk, group;
+};
 __global__ void __launch_bounds__(kFBThreads)
-    ff_bslice_kernel(const FuseRow *__restrict__ frows, const FuseChunk *__restrict__ chunks, int NW, int G, int KB,
-                     const double2 *__restrict__ aqsn, int nb, int8_t *__restrict__ pack, long long pack_bytes,
-                     double *__restrict__ sB, int *status) {
-  __shared__ double2 stage[kFBThreads * (kFBK + 1)];
-  __shared__ double red[kFBThreads / 32];
+    ff_bslice_kernel(const BSliceTask *__restrict__ tasks, const FuseRow *__restrict__ frows,
+                     const FuseChunk *__restrict__ chunks, int NW, int G, int KB, const double2 *__restrict__ aqsn,
+                     int nb, int8_t *__restrict__ pack, long long pack_bytes, double *__restrict__ sB, int *status) {
+  __shared__ double s_mult[8];
+  __shared__ int s_bad[8];
   const int w = (int)(blockIdx.x % NW);
-  const int slot = (int)(blockIdx.x / NW);
-  const FuseRow fr = frows[slot];
-  const FuseChunk C = chunks[fr.chunk];
-  const int r = slot - C.slot0, nrp = C.nrp;
-  bool valid = fr.coef != 0.0;
-  if (!BGW_CHECKED(!valid || (unsigned)fr.band < (unsigned)nb, status, 63)) valid = false;
-  const double2 *src = aqsn + (size_t)(valid ? fr.band : 0) * (size_t)G;
-  const int kw = w * kFWin;
-  double2 xv[kFBK];
-#pragma unroll
-  for (int j = 0; j < kFBK; ++j) xv[j] = src[min(kw + j * kFBThreads + (int)threadIdx.x, G - 1)];
-  double m = 0.0;
-  int nonfinite = 0;
-#pragma unroll
-  for (int j = 0; j < kFBK; ++j) {
-    const int kk = j * kFBThreads + (int)threadIdx.x;
-    double2 x = xv[j];
-    if (!valid || kw + kk >= G) x = make_double2(0.0, 0.0);
-    const double a = fmax(fabs(x.x), fabs(x.y));
-    nonfinite |= !(a <= DBL_MAX);
-    m = fmax(m, a);
-    stage[kk + (kk >> 3)] = x;
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
-  nonfinite = __syncthreads_or(nonfinite);
-  m = red[0];
-#pragma unroll
-  for (int i = 1; i < kFBThreads / 32; ++i) m = fmax(m, red[i]);
-  int e = 0;
-  if (m > 0.0 && !nonfinite) (void)frexp(m, &e);
-  e = max(e, -960);  // keeps 2^(38 - e) finite; values below 2^-960 lose precision
-  if (threadIdx.x == 0)
-    sB[(size_t)slot * NW + w] = nonfinite ? __longlong_as_double(0x7ff8000000000000LL) : ldexp(1.0, e + 2);
-  const int k0 = kw + (int)threadIdx.x * kFBK;
-  if (k0 >= KB * kFK) return;  // past the packed k range (last window)
-  const double mult = ldexp(1.0, 38 - e);
-  // This thread writes stage positions [8u, 8u + 8) of stage k0 / kFK
-  // (u = k0 / 8 mod 4): position 4 q + e holds stage k = q + 8 e, so byte
-  // 4 hq + e of its 8 takes k = 2u + hq + 8 e.
-  const int u = (k0 / 8) & 3, sk0 = (k0 / kFK) * kFK - kw;  // stage start in the window
-  uint32_t wr[kFS][2], wi[kFS][2], wn[kFS][2];
-  bool ovf = false;
-#pragma unroll
-  for (int hq = 0; hq < 2; ++hq) {
-    double cr[4], ci[4], cn[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int kk = sk0 + 2 * u + hq + 8 * j;
-      const double2 v = stage[kk + (kk >> 3)];
-      cr[j] = nonfinite ? 0.0 : v.x;
-      ci[j] = nonfinite ? 0.0 : v.y;
-      cn[j] = -ci[j];
+  const BSliceTask T = tasks[blockIdx.x / NW];
+  const FuseChunk C = chunks[T.chunk];
+  const int nrp = C.nrp, warp = (int)threadIdx.x >> 5, lane = (int)threadIdx.x & 31;
+  const int kw = w * kFWin, kend = min(G, kw + kFWin);
+  // ---- pass 1: row slot 8 group + warp.
+  {
+    const int slot = C.slot0 + 8 * T.group + warp;
+    const FuseRow fr = frows[slot];
+    bool valid = fr.coef != 0.0;
+    if (!BGW_CHECKED(!valid || (unsigned)fr.band < (unsigned)nb, status, 63)) valid = false;
+    double m = 0.0;
+    int nonfinite = 0;
+    if (valid) {
+      const double2 *src = aqsn + (size_t)fr.band * (size_t)G;
+      for (int k = kw + lane; k < kend; k += 32) {
+        const double2 x = src[k];
+        const double a = fmax(fabs(x.x), fabs(x.y));
+        nonfinite |= !(a <= DBL_MAX);
+        m = fmax(m, a);
+      }
     }
-    uint32_t a[kFS], b[kFS], c[kFS];
-    digits4(cr, mult, INFINITY, ovf, a);
-    digits4(ci, mult, INFINITY, ovf, b);
-    digits4(cn, mult, INFINITY, ovf, c);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      nonfinite |= __shfl_xor_sync(0xffffffffu, nonfinite, o);
+    }
+    int e = 0;
+    if (m > 0.0 && !nonfinite) (void)frexp(m, &e);
+    e = max(e, -960);  // keeps 2^(38 - e) finite; values below 2^-960 lose precision
+    if (lane == 0) {
+      sB[(size_t)slot * NW + w] = nonfinite ? __longlong_as_double(0x7ff8000000000000LL) : ldexp(1.0, e + 2);
+      s_mult[warp] = ldexp(1.0, 38 - e);
+      s_bad[warp] = (!valid || nonfinite) ? 1 : 0;
+    }
+  }
+  __syncthreads();
+  // ---- pass 2.
+  const int r = lane >> 2, u = lane & 3;
+  const int rs = 8 * T.group + r;  // row slot within the chunk
+  const FuseRow fr = frows[C.slot0 + rs];
+  const bool zero = s_bad[r] != 0;
+  const double mult = s_mult[r];
+  const double2 *src = aqsn + (size_t)(zero ? 0 : fr.band) * (size_t)G;
+  const int srows = kFS * 2 * nrp;
+  const long long stack = (long long)srows * kFK;  // bytes of one stack
+  const int nstages = (kend - kw + kFK - 1) / kFK;
+  for (int sl = warp; sl < nstages; sl += kFBThreads / 32) {
+    const int kb = kw / kFK + sl;
+    if (kb >= KB) break;
+    const int k0 = kb * kFK;
+    uint32_t wr[kFS][2], wi[kFS][2], wn[kFS][2];
+    bool ovf = false;
+#pragma unroll
+    for (int hq = 0; hq < 2; ++hq) {
+      double cr[4], ci[4], cn[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int k = k0 + 2 * u + hq + 8 * j;
+        double2 v = make_double2(0.0, 0.0);
+        if (!zero && k < G) v = src[k];
+        cr[j] = v.x;
+        ci[j] = v.y;
+        cn[j] = -v.y;
+      }
+      uint32_t a[kFS], b[kFS], c[kFS];
+      digits4(cr, mult, INFINITY, ovf, a);
+      digits4(ci, mult, INFINITY, ovf, b);
+      digits4(cn, mult, INFINITY, ovf, c);
+#pragma unroll
+      for (int t = 0; t < kFS; ++t) {
+        wr[t][hq] = a[t];
+        wi[t][hq] = b[t];
+        wn[t][hq] = c[t];
+      }
+    }
+    const int kk = 8 * u;  // stage position of this lane's first byte
+    const long long base = C.b_off + (long long)kb * 2 * stack;
+    auto off = [&](int row) {
+      return (long long)((kk >> 4) * (srows * 16) + (row >> 3) * 128 + (row & 7) * 16 + (kk & 15));
+    };
+    // Debug build: the stage's block lies in the packed buffer.
+    if (!BGW_CHECKED(base >= 0 && base + 2 * stack <= pack_bytes, status, 64)) break;
+    int8_t *sr = pack + base, *si = pack + base + stack;
 #pragma unroll
     for (int t = 0; t < kFS; ++t) {
-      wr[t][hq] = a[t];
-      wi[t][hq] = b[t];
-      wn[t][hq] = c[t];
+      const int r0 = 2 * nrp * t + rs, r1 = r0 + nrp;
+      *reinterpret_cast<uint2 *>(sr + off(r0)) = make_uint2(wr[t][0], wr[t][1]);
+      *reinterpret_cast<uint2 *>(sr + off(r1)) = make_uint2(wi[t][0], wi[t][1]);
+      *reinterpret_cast<uint2 *>(si + off(r0)) = make_uint2(wn[t][0], wn[t][1]);
+      *reinterpret_cast<uint2 *>(si + off(r1)) = make_uint2(wr[t][0], wr[t][1]);
     }
-  }
-  const int kb = k0 / kFK, kk = k0 % kFK, srows = kFS * 2 * nrp;
-  const long long stack = (long long)srows * kFK;  // bytes of one stack
-  const long long base = C.b_off + (long long)kb * 2 * stack;
-  auto off = [&](int row) { return (long long)((kk >> 4) * (srows * 16) + (row >> 3) * 128 + (row & 7) * 16 + (kk & 15)); };
-  // Debug build: the stage's block lies in the packed buffer.
-  if (!BGW_CHECKED(base >= 0 && base + 2 * stack <= pack_bytes, status, 64)) return;
-  int8_t *sr = pack + base, *si = pack + base + stack;
-#pragma unroll
-  for (int t = 0; t < kFS; ++t) {
-    const int r0 = 2 * nrp * t + r, r1 = r0 + nrp;
-    *reinterpret_cast<uint2 *>(sr + off(r0)) = make_uint2(wr[t][0], wr[t][1]);
-    *reinterpret_cast<uint2 *>(sr + off(r1)) = make_uint2(wi[t][0], wi[t][1]);
-    *reinterpret_cast<uint2 *>(si + off(r0)) = make_uint2(wn[t][0], wn[t][1]);
-    *reinterpret_cast<uint2 *>(si + off(r1)) = make_uint2(wr[t][0], wr[t][1]);
   }
 }
 
@@ -856,6 +873,10 @@ int ff_launch_fused(CallEnv *env, const FFPlan &plan, int64_t nb_w, int64_t nE, 
         gate.push_back(u);
       }
   }
+  std::vector<BSliceTask> btasks;  // band-row slicing: (chunk, group of 8 row slots)
+  for (int c = 0; c < (int)chunks.size(); ++c)
+    for (int gr = 0; gr < chunks[c].nrp / 8; ++gr) btasks.push_back({c, gr});
+  const int nbt = (int)btasks.size();
   const int nft = (int)ft.size(), nu = (int)units.size(), ns = (int)frows.size();
   // Partials: FP64 tiles first, then the units'.  One per tile / unit, or
   // with distinct outputs per iw one per tile row / row slot, combined by the
@@ -887,7 +908,8 @@ int ff_launch_fused(CallEnv *env, const FFPlan &plan, int64_t nb_w, int64_t nE, 
   const size_t o_fr = o_ch + al(sizeof(FuseChunk) * std::max<size_t>(chunks.size(), 1));
   const size_t o_un = o_fr + al(sizeof(FuseRow) * std::max(ns, 1));
   const size_t o_out = o_un + al(sizeof(FuseUnit) * std::max(nu, 1));
-  const size_t o_sb = o_out + al(sizeof(int) * std::max<size_t>(n_part, 1));
+  const size_t o_bt = o_out + al(sizeof(int) * std::max<size_t>(n_part, 1));
+  const size_t o_sb = o_bt + al(sizeof(BSliceTask) * std::max(nbt, 1));
   const size_t o_flag = o_sb + al(sizeof(double) * std::max<size_t>((size_t)ns * NW, 1));
   const size_t total = o_flag + al(sizeof(int) * std::max(nu, 1));
   std::vector<unsigned char> host(o_sb, 0);  // the device-written tail is not uploaded
@@ -901,6 +923,7 @@ int ff_launch_fused(CallEnv *env, const FFPlan &plan, int64_t nb_w, int64_t nE, 
   put(o_fr, frows.data(), sizeof(FuseRow) * ns);
   put(o_un, units.data(), sizeof(FuseUnit) * nu);
   put(o_out, out_of.data(), sizeof(int) * n_part);
+  put(o_bt, btasks.data(), sizeof(BSliceTask) * nbt);
   BGW_TRY(ws_reserve(ws, SLOT_PLAN, total, &plan_buf));
   BGW_CUDA_TRY(cudaMemcpyAsync(plan_buf, host.data(), o_sb, cudaMemcpyHostToDevice, stream));
   unsigned char *pb = static_cast<unsigned char *>(plan_buf);
@@ -914,8 +937,9 @@ int ff_launch_fused(CallEnv *env, const FFPlan &plan, int64_t nb_w, int64_t nE, 
     const FuseChunk *d_ch = (const FuseChunk *)(pb + o_ch);
     const FuseRow *d_fr = (const FuseRow *)(pb + o_fr);
     double *d_sb = (double *)(pb + o_sb);
-    ff_bslice_kernel<<<(unsigned)((size_t)ns * NW), kFBThreads, 0, stream>>>(
-        d_fr, d_ch, NW, (int)G, KB, an, (int)nb_w, (int8_t *)pack, off, d_sb, env->d_status);
+    ff_bslice_kernel<<<(unsigned)((size_t)nbt * NW), kFBThreads, 0, stream>>>(
+        (const BSliceTask *)(pb + o_bt), d_fr, d_ch, NW, (int)G, KB, an, (int)nb_w, (int8_t *)pack, off, d_sb,
+        env->d_status);
     count_launch();
     BGW_CUDA_TRY(cudaGetLastError());
     const int smem = (int)sizeof(FuseSmem);
