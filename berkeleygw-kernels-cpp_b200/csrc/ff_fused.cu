@@ -3,7 +3,7 @@
 // ff_mixed.cu, FP64 recombination).
 //
 // Roles.  A unit of work is (band-row chunk, 128 G' columns p, k range of
-// one 2048-k window).  The MMA's M side is the frequency slice tile X[p][k]
+// one 4096-k window).  The MMA's M side is the frequency slice tile X[p][k]
 // (I_epsR, I_epsA or their difference, 128 rows), its N side the chunk's
 // band rows a = aqsn[band][k] with real and imaginary parts stacked:
 //   D = Xr [ar; ai]^T + Xi [-ai; ar]^T  =  [Re(X a^T) | Im(X a^T)],
@@ -24,7 +24,7 @@
 // bytes of u minus 128 (byte ^ 0x80) are d_4..d_1 and its signed top byte
 // is d_0.  So x = 2^(E + 2) sum_s d_s 256^-(s + 1) up to 2^(E - 38), and a
 // product of digit levels s + t + 2 = L carries the weight 256^-L.  Every
-// digit product is exact in int32 (|C_L| <= 5 pairs x 2 x 2048 x 2^14).
+// digit product is exact in int32 (|C_L| <= 5 pairs x 2 x 4096 x 2^14).
 //
 // Split.  The band rows are cut by ff_bslice_kernel (exact per-window row
 // scale, the two stacks in the canonical K-major layout, one contiguous
@@ -69,7 +69,7 @@ constexpr int kFM = 128;                               // G' columns per unit (M
 constexpr int kFK = 32;                                // k per stage (one kind::i8 MMA)
 constexpr int kFStages = 3;
 constexpr int kFMaxRows = 48;                          // band rows per chunk (N = 2 rows)
-constexpr int kFWin = 2048;                            // k per unit; band-row scale window
+constexpr int kFWin = 4096;                            // k per unit; band-row scale window
 constexpr int kFConvWarps = 16;                        // 2 tasks each per stage
 constexpr int kFEpiWarps = 8;                          // two per TMEM lane quarter
 constexpr int kFConv = 32 * kFConvWarps;               // converter threads
