@@ -1,6 +1,7 @@
 // ff_fused.cu -- mixed-precision FF sums with the digit split fused into the
-// tensor-core kernel (tcgen05.mma kind::i8, integer Ozaki scheme as in
-// ff_mixed.cu, FP64 recombination).
+// tensor-core kernel (tcgen05.mma kind::i8, integer Ozaki scheme, FP64
+// recombination; ff_mixed.cu holds the staged form, which cuts both
+// operands into digit buffers first).
 //
 // Roles.  A unit of work is (band-row chunk, 128 G' columns p, k range of
 // one 4096-k window).  The MMA's M side is the frequency slice tile X[p][k]
@@ -46,10 +47,12 @@
 // k = q + 8 e (e < 4), so every 16-byte load instruction of a warp covers
 // four whole 128-byte lines, and still writes its four digits as one word.
 //
-// Warps: 0 copies the band-row digit blocks (1-D bulk copies, 3-stage
-// ring), 1 issues the MMAs, 2-9 convert X and, after the last stage, read
-// the accumulators (tcgen05.ld), fold W(band, p) and the scales, and reduce
-// one partial per unit.  Every mbarrier wait is bounded.
+// Warps: 0 is the producer (band-row digit blocks by 1-D bulk copies into a
+// 3-stage ring; in a 2-CTA pair also this CTA's converted half to the
+// peer), 1 issues the MMAs, 2-17 convert X; after the last stage warps 2-9
+// read the accumulators (tcgen05.ld), fold W(band, p) and the scales, and
+// reduce one partial per unit (or per row slot).  Every mbarrier wait is
+// bounded.  The grid is made of 2-CTA clusters (kFPair, see ff_fuse_kernel).
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -70,7 +73,7 @@ constexpr int kFK = 32;                                // k per stage (one kind:
 constexpr int kFStages = 3;
 constexpr int kFMaxRows = 48;                          // band rows per chunk (N = 2 rows)
 constexpr int kFWin = 4096;                            // k per unit; band-row scale window
-constexpr int kFConvWarps = 16;                        // 2 tasks each per stage
+constexpr int kFConvWarps = 16;                        // per stage: 1 task (4 rows x 32 k) each in a pair
 constexpr int kFEpiWarps = 8;                          // two per TMEM lane quarter
 constexpr int kFConv = 32 * kFConvWarps;               // converter threads
 constexpr int kFThreads = 64 + kFConv;
@@ -85,9 +88,11 @@ constexpr int kFBStageMax = 2 * kFS * 2 * kFMaxRows * kFK;  // stacks Sr, Si x d
 constexpr int kFHeadroom = 1;                          // bits above the first block's largest value
 constexpr int kFBThreads = 256;                        // band-row slicing
 constexpr int kFuseMinRows = 8;                        // default: smaller groups stay FP64
-constexpr bool kFPair = true;                          // 2-CTA clusters share the slice conversion
+// 2-CTA clusters share the slice conversion (false: each CTA converts its
+// whole tile, 2 tasks per converter warp; the measured default is true).
+constexpr bool kFPair = true;
 static_assert(kFBThreads == 256, "band-row slicing: 8 warps, one per row slot of a group");
-static_assert((kFM / 4) % kFConvWarps == 0, "every converter warp takes the same tasks per stage");
+static_assert((kFM / 4) % (2 * kFConvWarps) == 0, "every converter warp takes the same tasks per stage");
 constexpr int kFTasks = (kFM / 4) / kFConvWarps;  // tasks (4 rows x 32 k) per converter warp and stage
 static_assert(kFS * 2 * kFMaxRows <= 512, "the level accumulators fit in tensor memory");
 static_assert(kFMaxRows % 8 == 0, "chunks are whole 8-row core-matrix groups");
@@ -379,7 +384,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
   const int ns = good ? (U.k1 - U.k0 + kFK - 1) / kFK : 0;  // stages
   const int kb0 = U.k0 / kFK;
   const uint32_t bbytes = (uint32_t)(2 * kFS * N * kFK);  // stacks Sr and Si
-  constexpr int kT = PAIR ? 1 : 2;                         // conversion tasks per warp and stage
+  constexpr int kT = PAIR ? kFTasks / 2 : kFTasks;         // conversion tasks per warp and stage
   constexpr uint32_t kHalf = 2 * kFS * 2 * (kFM / 2) * 16;  // bytes of half the rows of a stage
 
   if (threadIdx.x == 0) {
