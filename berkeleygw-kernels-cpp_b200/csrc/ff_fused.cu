@@ -412,38 +412,49 @@ __global__ void __launch_bounds__(kFThreads, 1)
   const uint32_t tmem = sm.tmem;
 
   if (warp == 0) {
-    // ---- producer: the band-row digits (one bulk copy per stage) and, in
-    // a pair, this CTA's half of each converted stage to the peer.
-    if (lane == 0) {
-      int issued = 0, nsent = 0;
-      for (int j = 0; j < ns; ++j) {
-        const int st = j % kFStages;
-        if (j >= kFStages && !fwait(&sm.empty[st], ((j / kFStages) - 1) & 1, status)) break;
-        if (!phantom) {
+    // ---- producer: the band-row digits (one bulk copy per stage, lane 0)
+    // and, in a pair, this CTA's half of each converted stage to the peer
+    // (20 copies, one per lane: issued one after the other they took longer
+    // than the stage's MMAs).
+    int issued = 0, nsent = 0;
+    for (int j = 0; j < ns; ++j) {
+      const int st = j % kFStages;
+      int ok = 1;
+      if (lane == 0) {
+        if (j >= kFStages && !fwait(&sm.empty[st], ((j / kFStages) - 1) & 1, status)) {
+          ok = 0;
+        } else if (!phantom) {
           const int8_t *src = pack + C.b_off + (long long)(kb0 + j) * bbytes;
           // Debug build: the block lies in the packed buffer.
-          if (!BGW_CHECKED(src >= pack && src + bbytes <= pack + pack_bytes, status, 62)) break;
-          mbar_expect_tx(&sm.bfull[st], bbytes);
-          bulk_g2s(sm.b[st], src, bbytes, &sm.bfull[st]);
-          issued = j + 1;
-        }
-        if (PAIR) {
-          if (!fwait(&sm.xlocal[st], (j / kFStages) & 1, status)) break;
-          // This CTA's arrival on xfull, expecting the peer's half as bytes;
-          // then this half to the peer (the generic writes were made visible
-          // to the async proxy by each converter before xlocal).
-          mbar_expect_tx(&sm.xfull[st], kHalf);
-          const uint32_t pbar = peer_addr(&sm.xfull[st], peer);
-#pragma unroll 1
-          for (int pl = 0; pl < 2 * kFS; ++pl)
-#pragma unroll
-            for (int kg = 0; kg < 2; ++kg) {
-              const int8_t *hs = &sm.x[st][pl * kFXPlane + kg * kFXLbo + rank * (kFM / 2) * 16];
-              bulk_s2peer(peer_addr(hs, peer), hs, (kFM / 2) * 16, pbar);
-            }
-          nsent = j + 1;
+          if (!BGW_CHECKED(src >= pack && src + bbytes <= pack + pack_bytes, status, 62)) {
+            ok = 0;
+          } else {
+            mbar_expect_tx(&sm.bfull[st], bbytes);
+            bulk_g2s(sm.b[st], src, bbytes, &sm.bfull[st]);
+            issued = j + 1;
+          }
         }
       }
+      if (PAIR) {
+        // Every lane sees this CTA's half written (acquire) before its copy.
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (ok && !fwait(&sm.xlocal[st], (j / kFStages) & 1, status)) ok = 0;
+        ok = __all_sync(0xffffffffu, ok);
+        if (!ok) break;
+        // This CTA's arrival on xfull, expecting the peer's half as bytes.
+        if (lane == 0) mbar_expect_tx(&sm.xfull[st], kHalf);
+        if (lane < 2 * 2 * kFS) {
+          const int pl = lane >> 1, kg = lane & 1;
+          const int8_t *hs = &sm.x[st][pl * kFXPlane + kg * kFXLbo + rank * (kFM / 2) * 16];
+          bulk_s2peer(peer_addr(hs, peer), hs, (kFM / 2) * 16, peer_addr(&sm.xfull[st], peer));
+        }
+        nsent = j + 1;
+      } else {
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) break;
+      }
+    }
+    if (lane == 0) {
       // Copies still in flight (error paths only) land before the CTA exits.
       for (int t = 0; t < kFStages; ++t) {
         if (issued <= t) continue;
