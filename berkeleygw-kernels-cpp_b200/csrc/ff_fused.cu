@@ -124,6 +124,7 @@ struct __align__(128) FuseSmem {
   int8_t b[kFStages][kFBStageMax];
   uint64_t bfull[kFStages], xfull[kFStages], empty[kFStages], done;
   uint64_t xlocal[kFStages];  // a pair: this CTA's half of the stage is written
+  uint64_t never;             // stall injection: nothing arrives on it
   uint32_t tmem;
   int ovf;                // a value of this CTA's rows did not fit
   int ovf_peer;           // ... of the peer's rows (written by the peer)
@@ -152,11 +153,12 @@ __device__ __forceinline__ bool try_wait_sleep(uint64_t *bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-__device__ __forceinline__ bool fwait(uint64_t *bar, uint32_t parity, int *status) {
+__device__ __forceinline__ bool fwait(uint64_t *bar, uint32_t parity, int *status,
+                                      long long budget = kWaitCycles) {
   if (try_wait_sleep(bar, parity)) return true;
   const long long t0 = clock64();
   while (!try_wait_sleep(bar, parity)) {
-    if (clock64() - t0 > kWaitCycles) {
+    if (clock64() - t0 > budget) {
       raise_status(status, BGW_ERR_TIMEOUT, (int)blockIdx.x);
       return false;
     }
@@ -365,7 +367,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
                    const FuseRow *__restrict__ frows, int n_slots, const int8_t *__restrict__ pack,
                    long long pack_bytes, const double *__restrict__ sB, int NW, const double2 *__restrict__ W, int P,
                    int G, int nb_w, double *__restrict__ partials, int *__restrict__ unit_flag, int per_row,
-                   int *status) {
+                   int *status, long long stall) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   FuseSmem &sm = *reinterpret_cast<FuseSmem *>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -385,6 +387,11 @@ __global__ void __launch_bounds__(kFThreads, 1)
   const int kb0 = U.k0 / kFK;
   const uint32_t bbytes = (uint32_t)(2 * kFS * N * kFK);  // stacks Sr and Si
   constexpr int kT = PAIR ? kFTasks / 2 : kFTasks;         // conversion tasks per warp and stage
+  // Stall injection (bgw_debug_inject_stall): at CTA-local stage `stall` the
+  // MMA thread waits on `never` and gives up; every other wait then has the
+  // short budget, so the timeout reaches the rest of the CTA (and of its
+  // pair) within milliseconds, along the same path as a real timeout.
+  const long long budget = stall >= 0 ? kStallCycles : kWaitCycles;
   constexpr uint32_t kHalf = 2 * kFS * 2 * (kFM / 2) * 16;  // bytes of half the rows of a stage
 
   if (threadIdx.x == 0) {
@@ -395,6 +402,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
       mbar_init(&sm.empty[i], PAIR ? 2 : 1);
     }
     mbar_init(&sm.done, 1);
+    mbar_init(&sm.never, 1);
     sm.ovf = 0;
     sm.ovf_peer = 0;
     sm.nrecv = 0;
@@ -421,7 +429,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
       const int st = j % kFStages;
       int ok = 1;
       if (lane == 0) {
-        if (j >= kFStages && !fwait(&sm.empty[st], ((j / kFStages) - 1) & 1, status)) {
+        if (j >= kFStages && !fwait(&sm.empty[st], ((j / kFStages) - 1) & 1, status, budget)) {
           ok = 0;
         } else if (!phantom) {
           const int8_t *src = pack + C.b_off + (long long)(kb0 + j) * bbytes;
@@ -438,7 +446,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
       if (PAIR) {
         // Every lane sees this CTA's half written (acquire) before its copy.
         ok = __shfl_sync(0xffffffffu, ok, 0);
-        if (ok && !fwait(&sm.xlocal[st], (j / kFStages) & 1, status)) ok = 0;
+        if (ok && !fwait(&sm.xlocal[st], (j / kFStages) & 1, status, budget)) ok = 0;
         ok = __all_sync(0xffffffffu, ok);
         if (!ok) break;
         // This CTA's arrival on xfull, expecting the peer's half as bytes.
@@ -459,7 +467,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
       for (int t = 0; t < kFStages; ++t) {
         if (issued <= t) continue;
         const int last = (issued - 1) - ((issued - 1 - t) % kFStages);
-        (void)fwait(&sm.bfull[t], (last / kFStages) & 1, status);
+        (void)fwait(&sm.bfull[t], (last / kFStages) & 1, status, budget);
       }
       // The peer drains the stages sent to it before it exits.
       if (PAIR) st_peer(peer_addr(&sm.nrecv, peer), nsent);
@@ -476,7 +484,8 @@ __global__ void __launch_bounds__(kFThreads, 1)
       for (int j = 0; j < ns; ++j) {
         const int st = j % kFStages;
         const uint32_t par = (uint32_t)((j / kFStages) & 1);
-        if ((!phantom && !fwait(&sm.bfull[st], par, status)) || !fwait(&sm.xfull[st], par, status)) break;
+        if (j == stall && !fwait(&sm.never, 0, status, kStallCycles)) break;
+        if ((!phantom && !fwait(&sm.bfull[st], par, status, budget)) || !fwait(&sm.xfull[st], par, status, budget)) break;
         tc::fence_after();
         if (!phantom) {
           const uint32_t xs = xbase + (uint32_t)(st * kFXStage), bs = bbase + (uint32_t)(st * kFBStageMax);
@@ -621,7 +630,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
     bool ovf = false;
     for (int j = 0; j < ns; ++j) {
       const int st = j % kFStages;
-      if (j >= kFStages && !fwait(&sm.empty[st], ((j / kFStages) - 1) & 1, status)) break;
+      if (j >= kFStages && !fwait(&sm.empty[st], ((j / kFStages) - 1) & 1, status, budget)) break;
 #pragma unroll
       for (int i = 0; i < kT; ++i) {
         const int row = task_row(i);
@@ -656,7 +665,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
   }
   // ---- all roles have issued their work; wait for the MMAs.
   bool dn = true;
-  if (lane == 0 && warp != 1) dn = fwait(&sm.done, 0, status);
+  if (lane == 0 && warp != 1) dn = fwait(&sm.done, 0, status, budget);
   dn = __shfl_sync(0xffffffffu, (int)dn, 0) != 0;
   if (PAIR) {
     cluster_sync();  // the peer's nrecv / ovf_peer are visible, and it issues nothing more
@@ -667,7 +676,7 @@ __global__ void __launch_bounds__(kFThreads, 1)
       for (int t = 0; t < kFStages; ++t) {
         if (n <= t) continue;
         const int last = (n - 1) - ((n - 1 - t) % kFStages);
-        (void)fwait(&sm.xfull[t], (last / kFStages) & 1, status);
+        (void)fwait(&sm.xfull[t], (last / kFStages) & 1, status, budget);
       }
     }
   } else {
@@ -976,7 +985,7 @@ int ff_launch_fused(CallEnv *env, const FFPlan &plan, int64_t nb_w, int64_t nE, 
     BGW_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, (const FuseUnit *)(pb + o_un), d_ch, d_fr, ns,
                                     (const int8_t *)pack, off, (const double *)d_sb, NW, (const double2 *)W, (int)P,
                                     (int)G, (int)nb_w, part + 2 * unit_part0, d_flag, per_row ? 1 : 0,
-                                    env->d_status));
+                                    env->d_status, stall_step()));
     count_launch();
     BGW_CUDA_TRY(cudaGetLastError());
   }

@@ -1,6 +1,7 @@
 """GPU: the timeout path of the kernels that stage their inputs through
-double-buffered bulk copies (GPP band loop FP64 and mixed, both GPP adjoint
-kernels, the batched band loop).
+bulk copies (GPP band loop FP64 and mixed, both GPP adjoint kernels, the
+batched band loop, and the fused FF tensor-core kernel with its 2-CTA
+pairs).
 
 bgw_debug_inject_stall(step) makes the bounded wait of CTA-local step `step`
 wait on a barrier that nothing ever completes, with a ~0.1 ms budget.  The
@@ -111,6 +112,25 @@ def test_batched_timeout_then_recovers(bgw, cuda, step, precision):
     b2 = bgw.GppBatch(insts, algorithm="bandloop", precision=precision)
     assert np.array_equal(b2.execute().cpu().numpy(), before)
     b2.close()
+
+
+@pytest.mark.parametrize("step", [0, 3])
+@pytest.mark.parametrize("flags", [0, 8])
+def test_ff_fused_timeout_then_recovers(bgw, cuda, step, flags):
+    """The fused FF kernel: at the stalled stage the MMA thread of both CTAs
+    of every pair gives up; the pair's converters, producers and the drain
+    then run out of their (short) budgets, every cluster barrier is still
+    reached, and the call reports BGW_ERR_TIMEOUT.  The next call (per-iw
+    outputs too: flags 8) is bitwise equal to one made before."""
+    f = I.ff_seeded(200, 2, 4096, 256, 6, 3, seed=91)
+    d = bgw.to_device(f, cuda)
+
+    def call():
+        return [x.cpu().numpy() for x in bgw.ff_sigma(d, precision="mixed", flags=flags)]
+    before = call()
+    _expect_timeout(bgw, call, step)
+    for a, b in zip(call(), before):
+        assert np.array_equal(a, b)
 
 
 def test_stall_argument_checked(bgw):
