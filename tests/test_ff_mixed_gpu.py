@@ -51,10 +51,11 @@ def test_uniform_closed_forms_mixed(bgw, cuda, flags):
 
 
 # Several 128-row tiles, three 256-column tiles, k not a multiple of 64,
-# column count not a multiple of 256, many frequency groups.
+# column count not a multiple of 256, many frequency groups; fewer k than one
+# 32-k stage, a column tile with 3 real rows, one stage plus one k.
 @pytest.mark.parametrize("flags", ROUTES)
 @pytest.mark.parametrize("dims", [(300, 3, 2000, 600, 9, 4), (129, 1, 333, 257, 5, 3), (17, 0, 300, 256, 3, 1),
-                                  (200, 2, 5000, 96, 6, 2)])
+                                  (200, 2, 5000, 96, 6, 2), (40, 2, 20, 3, 4, 2), (97, 2, 33, 30, 3, 2)])
 def test_ragged_shapes_vs_oracle(bgw, oracle, cuda, dims, flags):
     f = I.ff_seeded(*dims, seed=sum(dims))
     achs, asx, cor = bgw.ff_sigma(f, precision="mixed", flags=flags)
